@@ -1,0 +1,169 @@
+/*
+ * nido_b200.h -- C ABI of the B200-native Louvain engine (libnido_b200.so).
+ *
+ * The reference (sg0/nido) is a monolithic program whose internal operator
+ * API is the GraphGPU class (graph_gpu.hpp:168-247) over the *_cuda launchers
+ * of graph_cuda.hpp.  Each entry point below names the reference interface it
+ * replaces.  Plain pointers and sizes only; every function returns an int
+ * status (NIDO_OK or a negative NIDO_E_* code) and never throws; the message of
+ * the last failure on the calling thread is available from nido_last_error().
+ *
+ * Host buffers are owned by the caller; device buffers are owned by the engine.
+ * Ids crossing the ABI are int64 and weights FP64, as in the reference
+ * (types.hpp:14-22).  On the device, vertex and community ids are int32
+ * (graphs must have fewer than 2^31 vertices; larger ones are rejected with
+ * NIDO_E_TOO_LARGE) and edge offsets int64.
+ */
+#ifndef NIDO_B200_H_
+#define NIDO_B200_H_
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes -------------------------------------------------------- */
+#define NIDO_OK 0
+#define NIDO_E_INVALID -1   /* bad argument */
+#define NIDO_E_CUDA -2      /* CUDA runtime error (message has the CUDA text) */
+#define NIDO_E_NOMEM -3     /* device or host allocation failed / over budget */
+#define NIDO_E_IO -4        /* file could not be opened, read or written */
+#define NIDO_E_TOO_LARGE -5 /* more than 2^31-1 vertices */
+#define NIDO_E_TIMEOUT -6   /* a bounded device wait gave up */
+#define NIDO_E_NODEVICE -7  /* no CUDA device / not an sm_100 device */
+#define NIDO_E_BUSY -8      /* queue full (serving) */
+
+/* tie rules for the best-move argmax */
+#define NIDO_TIE_SMALLEST_ID 0 /* equal gains: smallest community id (default) */
+#define NIDO_TIE_NIDO 1        /* reference rule: 8-lane strided scan + shuffle tree
+                                  (graph_cuda.cu:1493-1526), for parity runs */
+
+typedef struct nido_ctx_s* nido_ctx;
+typedef struct nido_graph_s* nido_graph;
+
+/* Host CSR in the reference's layout (graph.hpp:23-26). */
+typedef struct {
+  int64_t nv;
+  int64_t ne;
+  int64_t* off; /* nv+1 */
+  int64_t* adj; /* ne   */
+  double* w;    /* ne   */
+} nido_csr;
+
+/* Run parameters: the reference's -b/-t/-i options (main.cpp:38-79, defaults
+ * types.hpp:24-38) plus the tie rule. */
+typedef struct {
+  int32_t nbatches;  /* -b, default 2 */
+  int32_t tie_mode;  /* NIDO_TIE_* */
+  double tau;        /* -t, default 1e-6 */
+  int64_t max_iter;  /* -i, default 500 */
+  int32_t verbose;   /* print the reference's per-loop lines to stdout */
+  int32_t reserved;
+} nido_params;
+
+/* Per-run statistics (the reference prints these, louvain_gpu.cpp:43-131). */
+typedef struct {
+  int64_t phases;
+  int64_t total_loops;
+  double final_q;      /* "Final Q" of the last phase */
+  double total_ms;     /* device-event time of the whole run */
+  double move_ms;      /* time inside move-phase kernels */
+  double move_bytes;   /* algorithmic bytes of all move sweeps (16E + 32V per sweep) */
+  double edges_scanned;/* edges visited by move sweeps */
+  int64_t move_launches;
+  int64_t kernel_launches;
+  double q_phase[200];
+  int64_t loops_phase[200];
+  int64_t nv_phase[200];
+  int64_t ne_phase[200];
+} nido_run_stats;
+
+/* ---- library ---------------------------------------------------------------- */
+const char* nido_last_error(void);
+const char* nido_version(void);
+
+/* ---- context: one CUDA device + one stream; one per host thread ----------- */
+/* Replaces GraphGPU's per-device setup (graph_gpu.cpp:33-100). */
+int nido_ctx_create(int device, size_t hbm_budget_bytes, nido_ctx* out);
+int nido_ctx_destroy(nido_ctx ctx);
+int nido_ctx_sync(nido_ctx ctx);
+/* the ctx's cudaStream_t, for callers that order their own work with it */
+int nido_ctx_stream(nido_ctx ctx, void** stream);
+
+/* ---- graphs ----------------------------------------------------------------- */
+/* Upload a CSR and compute k_v and m.  Replaces the GraphGPU constructor
+ * (graph_gpu.cpp:19-185: H2D copies, sum_vertex_weights, compute_mass,
+ * partition_graph_edge_batch).  nbatches sets the -b cuts. */
+int nido_graph_upload(nido_ctx ctx, int64_t nv, int64_t ne, const int64_t* off,
+                      const int64_t* adj, const double* w, int32_t nbatches,
+                      nido_graph* out);
+int nido_graph_free(nido_graph g);
+/* sizes of the current (possibly coarsened) graph */
+int nido_graph_size(nido_graph g, int64_t* nv, int64_t* ne);
+/* download the current CSR (caller sizes from nido_graph_size) */
+int nido_graph_download(nido_graph g, int64_t* off, int64_t* adj, double* w);
+/* batch cut points of the current graph, nbatches+1 entries
+ * (GraphGPU::vertex_per_batch_, graph_gpu.cpp:280-359) */
+int nido_graph_batches(nido_graph g, int64_t* cuts);
+/* k_v (vertexWeights_) and m (mass_) of the current graph */
+int nido_graph_vertex_weights(nido_graph g, double* k, double* m);
+
+/* ---- step-level operators: GraphGPU's public methods (graph_gpu.hpp:172-241) */
+int nido_singleton_partition(nido_graph g);                  /* graph_gpu.cpp:519-536 */
+int nido_set_community_ids(nido_graph g, const int64_t* comm);/* graph_gpu.cpp:433-455 */
+int nido_compute_modularity(nido_graph g, double* q);        /* graph_gpu.cpp:862-905 */
+int nido_louvain_update(nido_graph g, int32_t batch, int32_t tie_mode); /* graph_gpu.cpp:602-624 */
+int nido_update_community_weights(nido_graph g, int32_t batch);/* graph_gpu.cpp:779-791 */
+int nido_update_community_ids(nido_graph g, int32_t batch);  /* graph_gpu.cpp:808-820 */
+int nido_restore_community(nido_graph g);                    /* graph_gpu.cpp:822-842 */
+/* aggregation (graph_gpu.cpp:1382-1545): renumber, compose the clustering,
+ * coarsen in place; *done = 1 when the reference would stop (no merge, or one
+ * community left). */
+int nido_aggregation(nido_graph g, int32_t* done);
+/* state download: commIds_, newCommIds_, commWeights_ (any may be NULL) */
+int nido_get_state(nido_graph g, int64_t* comm, int64_t* newcomm, double* a);
+/* clustering of the ORIGINAL vertices (Clustering::commIds_, clustering.hpp:7-41) */
+int nido_get_clustering(nido_graph g, int64_t* clustering);
+/* Clustering::dump_partition (clustering.cpp:23-46); new_orders may be NULL */
+int nido_dump_partition(nido_graph g, const char* path, const int64_t* new_orders);
+
+/* ---- whole run: LouvainGPU::run (louvain_gpu.cpp:6-139) ------------------------ */
+/* out_comm (nv entries, may be NULL) receives the clustering of the original
+ * vertices; stats may be NULL. */
+int nido_run(nido_graph g, const nido_params* p, int64_t* out_comm, nido_run_stats* stats);
+
+/* ---- colouring for -c (Graph::coloring, graph.cpp:651-797) ---------------------- */
+/* Jones-Plassmann-Luby colouring on the device; colors has nv entries;
+ * returns the number of colours in *ncolors. Proper (no two neighbours share a
+ * colour) and deterministic for a given seed. */
+int nido_color(nido_ctx ctx, const nido_csr* in, uint64_t seed, int64_t* colors,
+               int64_t* ncolors);
+/* relabel by (colour, id) as graph.cpp:714-796: out gets the permuted CSR (its
+ * arrays caller-allocated with the input sizes), new_orders[p] = old id */
+int nido_color_relabel(nido_ctx ctx, const nido_csr* in, const int64_t* colors,
+                       nido_csr* out, int64_t* new_orders);
+
+/* ---- Vite binary files (graph.cpp:425-598) -------------------------------------- */
+int nido_read_vite(const char* path, nido_csr* out); /* arrays malloc'ed */
+int nido_write_vite(const char* path, const nido_csr* g);
+void nido_csr_free(nido_csr* g);
+
+/* ---- seeded synthetic generators (test and benchmark inputs) -------------------- */
+/* weight modes */
+#define NIDO_W_ONE 0       /* all 1.0; duplicate edges dropped */
+#define NIDO_W_UNIFORM 1   /* U[0.5, 1.5]; duplicates merged by summing */
+#define NIDO_W_LOGNORMAL 2 /* lognormal(0, 0.5); duplicates summed */
+#define NIDO_W_INT8 3      /* integers uniform in {1..8}; duplicates summed */
+int nido_gen_planted(int64_t nblocks, int64_t block_size, double avg_degree,
+                     double p_intra, int32_t wmode, uint64_t seed, nido_csr* out);
+int nido_gen_rmat(int64_t nv, int64_t npairs, double a, double b, double c,
+                  int32_t wmode, uint64_t seed, nido_csr* out);
+int nido_gen_sbm(int64_t nv, double alpha, int64_t cmin, int64_t cmax,
+                 double avg_degree, double p_intra, int32_t wmode, int32_t permute,
+                 uint64_t seed, nido_csr* out);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* NIDO_B200_H_ */

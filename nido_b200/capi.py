@@ -1,0 +1,335 @@
+"""ctypes binding of libnido_b200.so (declarations in include/nido_b200.h).
+
+The library is the product; this module only marshals numpy arrays across the
+C ABI.  It refuses to run without the compiled library: there is no Python or
+CPU fallback for any device operation.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "lib", "libnido_b200.so")
+
+NIDO_OK = 0
+NIDO_TIE_SMALLEST_ID = 0
+NIDO_TIE_NIDO = 1
+W_ONE, W_UNIFORM, W_LOGNORMAL, W_INT8 = 0, 1, 2, 3
+
+_i64p = C.POINTER(C.c_int64)
+_f64p = C.POINTER(C.c_double)
+
+
+class NidoError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"nido error {code}: {msg}")
+        self.code = code
+
+
+class _Csr(C.Structure):
+    _fields_ = [("nv", C.c_int64), ("ne", C.c_int64), ("off", _i64p), ("adj", _i64p), ("w", _f64p)]
+
+
+class _Params(C.Structure):
+    _fields_ = [("nbatches", C.c_int32), ("tie_mode", C.c_int32), ("tau", C.c_double),
+                ("max_iter", C.c_int64), ("verbose", C.c_int32), ("reserved", C.c_int32)]
+
+
+class RunStats(C.Structure):
+    _fields_ = [("phases", C.c_int64), ("total_loops", C.c_int64), ("final_q", C.c_double),
+                ("total_ms", C.c_double), ("move_ms", C.c_double), ("move_bytes", C.c_double),
+                ("edges_scanned", C.c_double), ("move_launches", C.c_int64),
+                ("kernel_launches", C.c_int64), ("q_phase", C.c_double * 200),
+                ("loops_phase", C.c_int64 * 200), ("nv_phase", C.c_int64 * 200),
+                ("ne_phase", C.c_int64 * 200)]
+
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """Load the compiled library (raises if it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is missing: build it with `make -C nido_b200/csrc` "
+                              "(or __graft_entry__.build())")
+        L = C.CDLL(LIB_PATH)
+        vp = C.c_void_p
+        sig = {
+            "nido_last_error": (C.c_char_p, []),
+            "nido_version": (C.c_char_p, []),
+            "nido_ctx_create": (C.c_int, [C.c_int, C.c_size_t, C.POINTER(vp)]),
+            "nido_ctx_destroy": (C.c_int, [vp]),
+            "nido_ctx_sync": (C.c_int, [vp]),
+            "nido_ctx_stream": (C.c_int, [vp, C.POINTER(vp)]),
+            "nido_graph_upload": (C.c_int, [vp, C.c_int64, C.c_int64, _i64p, _i64p, _f64p, C.c_int32,
+                                            C.POINTER(vp)]),
+            "nido_graph_free": (C.c_int, [vp]),
+            "nido_graph_size": (C.c_int, [vp, _i64p, _i64p]),
+            "nido_graph_download": (C.c_int, [vp, _i64p, _i64p, _f64p]),
+            "nido_graph_batches": (C.c_int, [vp, _i64p]),
+            "nido_graph_vertex_weights": (C.c_int, [vp, _f64p, _f64p]),
+            "nido_singleton_partition": (C.c_int, [vp]),
+            "nido_set_community_ids": (C.c_int, [vp, _i64p]),
+            "nido_compute_modularity": (C.c_int, [vp, _f64p]),
+            "nido_louvain_update": (C.c_int, [vp, C.c_int32, C.c_int32]),
+            "nido_update_community_weights": (C.c_int, [vp, C.c_int32]),
+            "nido_update_community_ids": (C.c_int, [vp, C.c_int32]),
+            "nido_restore_community": (C.c_int, [vp]),
+            "nido_aggregation": (C.c_int, [vp, C.POINTER(C.c_int32)]),
+            "nido_get_state": (C.c_int, [vp, _i64p, _i64p, _f64p]),
+            "nido_get_clustering": (C.c_int, [vp, _i64p]),
+            "nido_dump_partition": (C.c_int, [vp, C.c_char_p, _i64p]),
+            "nido_run": (C.c_int, [vp, C.POINTER(_Params), _i64p, C.POINTER(RunStats)]),
+            "nido_color": (C.c_int, [vp, C.POINTER(_Csr), C.c_uint64, _i64p, _i64p]),
+            "nido_color_relabel": (C.c_int, [vp, C.POINTER(_Csr), _i64p, C.POINTER(_Csr), _i64p]),
+            "nido_read_vite": (C.c_int, [C.c_char_p, C.POINTER(_Csr)]),
+            "nido_write_vite": (C.c_int, [C.c_char_p, C.POINTER(_Csr)]),
+            "nido_csr_free": (None, [C.POINTER(_Csr)]),
+            "nido_gen_planted": (C.c_int, [C.c_int64, C.c_int64, C.c_double, C.c_double, C.c_int32,
+                                           C.c_uint64, C.POINTER(_Csr)]),
+            "nido_gen_rmat": (C.c_int, [C.c_int64, C.c_int64, C.c_double, C.c_double, C.c_double,
+                                        C.c_int32, C.c_uint64, C.POINTER(_Csr)]),
+            "nido_gen_sbm": (C.c_int, [C.c_int64, C.c_double, C.c_int64, C.c_int64, C.c_double,
+                                       C.c_double, C.c_int32, C.c_int32, C.c_uint64, C.POINTER(_Csr)]),
+        }
+        for name, (res, args) in sig.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def _check(st: int):
+    if st != NIDO_OK:
+        raise NidoError(st, lib().nido_last_error().decode())
+
+
+def _p64(a: np.ndarray):
+    return a.ctypes.data_as(_i64p)
+
+
+def _pf(a: np.ndarray):
+    return a.ctypes.data_as(_f64p)
+
+
+@dataclass
+class Csr:
+    """Host CSR in the reference's layout: int64 offsets and ids, FP64 weights."""
+    off: np.ndarray
+    adj: np.ndarray
+    w: np.ndarray
+
+    @property
+    def nv(self) -> int:
+        return len(self.off) - 1
+
+    @property
+    def ne(self) -> int:
+        return int(self.off[-1])
+
+    def _struct(self) -> _Csr:
+        self.off = np.ascontiguousarray(self.off, dtype=np.int64)
+        self.adj = np.ascontiguousarray(self.adj, dtype=np.int64)
+        self.w = np.ascontiguousarray(self.w, dtype=np.float64)
+        return _Csr(self.nv, self.ne, _p64(self.off), _p64(self.adj), _pf(self.w))
+
+    def degrees(self) -> np.ndarray:
+        return np.diff(self.off)
+
+
+def _take(s: _Csr) -> Csr:
+    nv, ne = s.nv, s.ne
+    off = np.ctypeslib.as_array(s.off, shape=(nv + 1,)).copy()
+    adj = np.ctypeslib.as_array(s.adj, shape=(max(ne, 1),))[:ne].copy()
+    w = np.ctypeslib.as_array(s.w, shape=(max(ne, 1),))[:ne].copy()
+    lib().nido_csr_free(C.byref(s))
+    return Csr(off, adj, w)
+
+
+def gen_planted(nblocks=256, block_size=256, avg_degree=32.0, p_intra=0.8, wmode=W_UNIFORM, seed=1) -> Csr:
+    s = _Csr()
+    _check(lib().nido_gen_planted(nblocks, block_size, avg_degree, p_intra, wmode, seed, C.byref(s)))
+    return _take(s)
+
+
+def gen_rmat(nv, npairs, a=0.57, b=0.19, c=0.19, wmode=W_ONE, seed=2) -> Csr:
+    s = _Csr()
+    _check(lib().nido_gen_rmat(nv, npairs, a, b, c, wmode, seed, C.byref(s)))
+    return _take(s)
+
+
+def gen_sbm(nv, alpha=2.5, cmin=16, cmax=65536, avg_degree=32.0, p_intra=0.7, wmode=W_LOGNORMAL,
+            permute=True, seed=3) -> Csr:
+    s = _Csr()
+    _check(lib().nido_gen_sbm(nv, alpha, cmin, cmax, avg_degree, p_intra, wmode, int(permute), seed,
+                              C.byref(s)))
+    return _take(s)
+
+
+def read_vite(path: str) -> Csr:
+    s = _Csr()
+    _check(lib().nido_read_vite(path.encode(), C.byref(s)))
+    return _take(s)
+
+
+def write_vite(path: str, g: Csr):
+    s = g._struct()
+    _check(lib().nido_write_vite(path.encode(), C.byref(s)))
+
+
+class Context:
+    """One CUDA device and stream (nido_ctx)."""
+
+    def __init__(self, device: int = 0, hbm_budget: int = 0):
+        h = C.c_void_p()
+        _check(lib().nido_ctx_create(device, hbm_budget, C.byref(h)))
+        self.h = h
+
+    def sync(self):
+        _check(lib().nido_ctx_sync(self.h))
+
+    def stream(self) -> int:
+        s = C.c_void_p()
+        _check(lib().nido_ctx_stream(self.h, C.byref(s)))
+        return s.value or 0
+
+    def close(self):
+        if self.h:
+            lib().nido_ctx_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def color(self, g: Csr, seed: int = 1):
+        colors = np.empty(g.nv, dtype=np.int64)
+        nc = C.c_int64()
+        s = g._struct()
+        _check(lib().nido_color(self.h, C.byref(s), seed, _p64(colors), C.byref(nc)))
+        return colors, nc.value
+
+    def color_relabel(self, g: Csr, colors: np.ndarray):
+        colors = np.ascontiguousarray(colors, dtype=np.int64)
+        out = Csr(np.empty(g.nv + 1, np.int64), np.empty(max(g.ne, 1), np.int64),
+                  np.empty(max(g.ne, 1), np.float64))
+        so = _Csr(g.nv, g.ne, _p64(out.off), _p64(out.adj), _pf(out.w))
+        new_orders = np.empty(g.nv, dtype=np.int64)
+        s = g._struct()
+        _check(lib().nido_color_relabel(self.h, C.byref(s), _p64(colors), C.byref(so), _p64(new_orders)))
+        out.adj = out.adj[:g.ne]
+        out.w = out.w[:g.ne]
+        return out, new_orders
+
+
+class Graph:
+    """A graph resident on the device (nido_graph), with GraphGPU's operators."""
+
+    def __init__(self, ctx: Context, g: Csr, nbatches: int = 2):
+        self.ctx = ctx
+        self.nv0 = g.nv
+        self.nbatches = nbatches
+        s = g._struct()
+        h = C.c_void_p()
+        _check(lib().nido_graph_upload(ctx.h, s.nv, s.ne, s.off, s.adj, s.w, nbatches, C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if self.h:
+            lib().nido_graph_free(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def size(self):
+        nv, ne = C.c_int64(), C.c_int64()
+        _check(lib().nido_graph_size(self.h, C.byref(nv), C.byref(ne)))
+        return nv.value, ne.value
+
+    def download(self) -> Csr:
+        nv, ne = self.size()
+        off = np.empty(nv + 1, np.int64)
+        adj = np.empty(max(ne, 1), np.int64)
+        w = np.empty(max(ne, 1), np.float64)
+        _check(lib().nido_graph_download(self.h, _p64(off), _p64(adj), _pf(w)))
+        return Csr(off, adj[:ne], w[:ne])
+
+    def batches(self) -> np.ndarray:
+        cuts = np.empty(self.nbatches + 1, np.int64)
+        _check(lib().nido_graph_batches(self.h, _p64(cuts)))
+        return cuts
+
+    def vertex_weights(self):
+        nv, _ = self.size()
+        k = np.empty(nv, np.float64)
+        m = C.c_double()
+        _check(lib().nido_graph_vertex_weights(self.h, _pf(k), C.byref(m)))
+        return k, m.value
+
+    def singleton_partition(self):
+        _check(lib().nido_singleton_partition(self.h))
+
+    def set_community_ids(self, comm: np.ndarray):
+        comm = np.ascontiguousarray(comm, dtype=np.int64)
+        _check(lib().nido_set_community_ids(self.h, _p64(comm)))
+
+    def compute_modularity(self) -> float:
+        q = C.c_double()
+        _check(lib().nido_compute_modularity(self.h, C.byref(q)))
+        return q.value
+
+    def louvain_update(self, batch: int, tie: int = NIDO_TIE_SMALLEST_ID):
+        _check(lib().nido_louvain_update(self.h, batch, tie))
+
+    def update_community_weights(self, batch: int):
+        _check(lib().nido_update_community_weights(self.h, batch))
+
+    def update_community_ids(self, batch: int):
+        _check(lib().nido_update_community_ids(self.h, batch))
+
+    def restore_community(self):
+        _check(lib().nido_restore_community(self.h))
+
+    def aggregation(self) -> bool:
+        d = C.c_int32()
+        _check(lib().nido_aggregation(self.h, C.byref(d)))
+        return bool(d.value)
+
+    def state(self):
+        nv, _ = self.size()
+        comm = np.empty(nv, np.int64)
+        newc = np.empty(nv, np.int64)
+        a = np.empty(nv, np.float64)
+        _check(lib().nido_get_state(self.h, _p64(comm), _p64(newc), _pf(a)))
+        return comm, newc, a
+
+    def clustering(self) -> np.ndarray:
+        c = np.empty(self.nv0, np.int64)
+        _check(lib().nido_get_clustering(self.h, _p64(c)))
+        return c
+
+    def dump_partition(self, path: str, new_orders: np.ndarray | None = None):
+        p = None if new_orders is None else _p64(np.ascontiguousarray(new_orders, dtype=np.int64))
+        _check(lib().nido_dump_partition(self.h, path.encode(), p))
+
+    def run(self, tau: float = 1e-6, max_iter: int = 500, tie: int = NIDO_TIE_SMALLEST_ID,
+            verbose: bool = False):
+        """LouvainGPU::run; returns (clustering of the input vertices, RunStats)."""
+        p = _Params(self.nbatches, tie, tau, max_iter, int(verbose), 0)
+        out = np.empty(self.nv0, np.int64)
+        st = RunStats()
+        _check(lib().nido_run(self.h, C.byref(p), _p64(out), C.byref(st)))
+        return out, st

@@ -1,0 +1,448 @@
+// coarsen.cu -- aggregation of the reference (GraphGPU::aggregation,
+// graph_gpu.cpp:1382-1545) on the device.
+//
+// 1. Renumber: a used-flag per community id and an exclusive scan give each
+//    community its rank among used ids, i.e. the reference's dense renumber
+//    in ascending old-id order (sort_vertex_by_community_ids,
+//    graph_gpu.cpp:1151-1222).  The clustering of the original vertices is
+//    composed with it (Clustering::update_clustering, clustering.cpp:12-21).
+// 2. Members: a stable radix sort of (new id, vertex) lists each coarse
+//    vertex's members in ascending vertex order; a scan of member degrees
+//    gives the concatenated member-adjacency positions
+//    (shuffle_edge_list, graph_gpu.cpp:1088-1149).
+// 3. Edges: per coarse vertex, neighbours are mapped to new ids and merged
+//    with a hash; the output keeps the first-occurrence order of the
+//    concatenated list (compress_edges, graph_gpu.cpp:1224-1304).
+//    Coarse vertices with at most 256 member edges are handled by one warp
+//    that walks the list in order and folds each weight onto its entry in
+//    edge order, which is the reference's summation order.  Larger ones use a
+//    CTA with atomic first-position tracking and an ordered second pass; their
+//    weight sums are exact for integer weights.
+#include <limits.h>
+
+#include <algorithm>
+
+#include "common.cuh"
+#include "engine.cuh"
+#include "primitives.cuh"
+
+namespace nido {
+namespace {
+
+constexpr int kAggWarpMaxD = 256;   // member edges handled by one warp
+constexpr int kAggCtaMaxCap = 8192; // shared-memory table slots of the CTA tier
+constexpr int kAggThreads = 512;
+
+struct AggArgs {
+  const int64_t* __restrict__ off;
+  const int32_t* __restrict__ adj;
+  const double* __restrict__ w;
+  const int32_t* __restrict__ newid;
+  const uint32_t* __restrict__ member;  // vertices sorted by (new id, id)
+  const int64_t* __restrict__ mo;       // member offsets per coarse vertex
+  const int64_t* __restrict__ medge;    // concatenated-list position of each member
+  int32_t* __restrict__ tadj;           // output, at the coarse vertex's list position
+  double* __restrict__ tw;
+  int64_t* __restrict__ degp;           // coarse degree
+  int64_t nvp;                          // coarse vertex count
+  unsigned long long* err;              // probe-limit failures (never expected)
+};
+
+inline unsigned grid_for(int64_t work, int per_block, int max_blocks) {
+  int64_t b = (work + per_block - 1) / per_block;
+  if (b < 1) b = 1;
+  if (b > max_blocks) b = max_blocks;
+  return (unsigned)b;
+}
+
+__global__ void k_mark_used(const int32_t* __restrict__ comm, int64_t nv, int32_t* __restrict__ used) {
+  for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < nv; v += (int64_t)gridDim.x * blockDim.x)
+    used[comm[v]] = 1;
+}
+
+__global__ void k_newid(const int32_t* __restrict__ comm, const int64_t* __restrict__ cid, int64_t nv,
+                        int32_t* __restrict__ newid, uint32_t* __restrict__ keys, uint32_t* __restrict__ vals) {
+  for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < nv; v += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t x = (int32_t)cid[comm[v]];
+    newid[v] = x;
+    keys[v] = (uint32_t)x;
+    vals[v] = (uint32_t)v;
+  }
+}
+
+__global__ void k_compose(int32_t* __restrict__ clus, int64_t n0, const int32_t* __restrict__ newid) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n0; i += (int64_t)gridDim.x * blockDim.x)
+    clus[i] = newid[clus[i]];
+}
+
+// member offsets from the sorted keys (every id in [0, nvp) occurs) and the
+// member degrees
+__global__ void k_member_bounds(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ member,
+                                int64_t nv, int64_t nvp, const int64_t* __restrict__ off,
+                                int64_t* __restrict__ mo, int64_t* __restrict__ mdeg) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nv; i += (int64_t)gridDim.x * blockDim.x) {
+    if (i == 0 || keys[i] != keys[i - 1]) mo[keys[i]] = i;
+    if (i == 0) mo[nvp] = nv;
+    const uint32_t v = member[i];
+    mdeg[i] = off[v + 1] - off[v];
+  }
+}
+
+// tier of each coarse vertex by its member-edge count D
+__global__ void k_agg_tiers(const int64_t* __restrict__ mo, const int64_t* __restrict__ medge, int64_t nvp,
+                            uint32_t* __restrict__ keys, uint32_t* __restrict__ vals,
+                            int64_t* __restrict__ counts, unsigned long long* __restrict__ maxd) {
+  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < nvp; c += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t D = medge[mo[c + 1]] - medge[mo[c]];
+    const int64_t U = D < nvp ? D : nvp;
+    const uint32_t t = D <= kAggWarpMaxD ? 0u : (2 * U <= kAggCtaMaxCap ? 1u : 2u);
+    keys[c] = t;
+    vals[c] = (uint32_t)c;
+    atomicAdd((unsigned long long*)&counts[t], 1ull);
+    if (t == 2) atomicMax(maxd, (unsigned long long)U);
+  }
+}
+
+__device__ __forceinline__ int64_t find_member(const int64_t* __restrict__ medge, int64_t lo, int64_t hi,
+                                               int64_t P) {
+  while (hi - lo > 1) {
+    const int64_t mid = lo + (hi - lo) / 2;
+    if (medge[mid] <= P) lo = mid; else hi = mid;
+  }
+  return lo;
+}
+
+// Slot of key X, inserting it if absent (*isnew reports the insert); at most
+// mask+1 probes, -1 when the table is full (tables are sized to at least
+// twice the number of keys, so this never happens).
+__device__ __forceinline__ int find_or_insert(int* keys, unsigned mask, int X, bool* isnew) {
+  unsigned h = hash_slot(X, mask);
+  volatile int* vk = keys;
+  *isnew = false;
+  for (unsigned probe = 0; probe <= mask; ++probe) {
+    const int kk = vk[h];
+    if (kk == X) return (int)h;
+    if (kk == -1) {
+      const int old = atomicCAS(&keys[h], -1, X);
+      if (old == -1) { *isnew = true; return (int)h; }
+      if (old == X) return (int)h;
+    }
+    h = (h + 1) & mask;
+  }
+  return -1;
+}
+
+__device__ __forceinline__ int find_slot(const int* keys, unsigned mask, int X) {
+  unsigned h = hash_slot(X, mask);
+  for (unsigned probe = 0; probe <= mask; ++probe) {
+    if (keys[h] == X) return (int)h;
+    h = (h + 1) & mask;
+  }
+  return -1;
+}
+
+__device__ __forceinline__ unsigned cap_for(int64_t D, int64_t nvp) {
+  const int64_t U = D < nvp ? D : nvp;
+  unsigned c = 64;
+  while ((int64_t)c < 2 * U) c <<= 1;
+  return c;
+}
+
+// neighbour of list position P: new id and weight
+__device__ __forceinline__ void load_pos(const AggArgs& q, int64_t m0, int64_t m1, int64_t P, int& X,
+                                         double& wt) {
+  const int64_t i = find_member(q.medge, m0, m1, P);
+  const uint32_t v = q.member[i];
+  const int64_t e = q.off[v] + (P - q.medge[i]);
+  X = q.newid[q.adj[e]];
+  wt = q.w[e];
+}
+
+// Warp tier: one warp per coarse vertex, table in shared memory.
+__global__ void __launch_bounds__(256) k_agg_warp(const int32_t* __restrict__ list, int64_t n, AggArgs q,
+                                                  int capmax) {
+  extern __shared__ double smem[];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  double* vals = smem + (size_t)wid * capmax;
+  int* keys = reinterpret_cast<int*>(smem + (size_t)nwarps * capmax) + (size_t)wid * capmax * 2;
+  int* idxs = keys + capmax;
+  for (int i = lane; i < capmax; i += 32) { keys[i] = -1; vals[i] = 0.; }
+  __syncwarp();
+  const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t task = warp; task < n; task += nw) {
+    const int cp = list[task];
+    const int64_t m0 = q.mo[cp], m1 = q.mo[cp + 1];
+    const int64_t P0 = q.medge[m0], P1 = q.medge[m1];
+    const unsigned cap = min((unsigned)capmax, cap_for(P1 - P0, q.nvp)), mask = cap - 1;
+    int running = 0;
+    for (int64_t base = P0; base < P1; base += 32) {
+      const int64_t P = base + lane;
+      const bool ok = P < P1;
+      int X = -1;
+      double wt = 0.;
+      if (ok) load_pos(q, m0, m1, P, X, wt);
+      const unsigned peers = __match_any_sync(NIDO_FULL_MASK, X);
+      const bool lead = ok && lane == __ffs(peers) - 1;
+      int h = -1;
+      bool isnew = false;
+      if (lead) {
+        h = find_or_insert(keys, mask, X, &isnew);
+        if (h < 0) atomicAdd(q.err, 1ull);
+      }
+      const bool have = h >= 0;
+      const unsigned newmask = __ballot_sync(NIDO_FULL_MASK, have && isnew);
+      if (have && isnew) idxs[h] = running + __popc(newmask & lanemask_lt());
+      running += __popc(newmask);
+      // fold the peers' weights onto the entry in lane (= list) order
+      double acc = have ? vals[h] : 0.;
+      unsigned rem = ok ? peers : 0u;
+      const int maxcnt = __reduce_max_sync(NIDO_FULL_MASK, (unsigned)__popc(rem));
+      for (int it = 0; it < maxcnt; ++it) {
+        const int src = rem ? __ffs(rem) - 1 : lane;
+        const double x = __shfl_sync(NIDO_FULL_MASK, wt, src);
+        if (rem) { acc += x; rem &= rem - 1; }
+      }
+      if (lead) vals[h] = acc;
+      __syncwarp();
+    }
+    for (unsigned i = lane; i < cap; i += 32) {
+      const int kk = keys[i];
+      if (kk >= 0) {
+        q.tadj[P0 + idxs[i]] = kk;
+        q.tw[P0 + idxs[i]] = vals[i];
+      }
+    }
+    if (lane == 0) q.degp[cp] = running;
+    __syncwarp();
+    for (unsigned i = lane; i < cap; i += 32) { keys[i] = -1; vals[i] = 0.; }
+    __syncwarp();
+  }
+}
+
+// CTA tier: one CTA per coarse vertex; pass 1 merges with atomics and keeps
+// the first list position of every new id, pass 2 walks the list in order and
+// emits each id at its first position.
+template <bool kGlobal>
+__global__ void __launch_bounds__(kAggThreads) k_agg_cta(const int32_t* __restrict__ list, int64_t n, AggArgs q,
+                                                         int capmax, int32_t* gkeys, double* gvals,
+                                                         int32_t* gfpos, int64_t gslab) {
+  extern __shared__ double smem[];
+  __shared__ int wsum[kAggThreads / 32];
+  __shared__ int running_s;
+  int *keys, *fpos;
+  double* vals;
+  if (kGlobal) {
+    keys = gkeys + (size_t)blockIdx.x * gslab;
+    fpos = gfpos + (size_t)blockIdx.x * gslab;
+    vals = gvals + (size_t)blockIdx.x * gslab;
+  } else {
+    vals = smem;
+    keys = reinterpret_cast<int*>(smem + capmax);
+    fpos = keys + capmax;
+    for (int i = threadIdx.x; i < capmax; i += blockDim.x) { keys[i] = -1; vals[i] = 0.; fpos[i] = INT_MAX; }
+    __syncthreads();
+  }
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+  for (int64_t task = blockIdx.x; task < n; task += gridDim.x) {
+    const int cp = list[task];
+    const int64_t m0 = q.mo[cp], m1 = q.mo[cp + 1];
+    const int64_t P0 = q.medge[m0], P1 = q.medge[m1];
+    unsigned cap = cap_for(P1 - P0, q.nvp);
+    if (!kGlobal) cap = min(cap, (unsigned)capmax);
+    const unsigned mask = cap - 1;
+    for (int64_t base = P0 + (int64_t)wid * 32; base < P1; base += blockDim.x) {
+      const int64_t P = base + lane;
+      const bool ok = P < P1;
+      int X = -1;
+      double wt = 0.;
+      if (ok) load_pos(q, m0, m1, P, X, wt);
+      const unsigned peers = __match_any_sync(NIDO_FULL_MASK, X);
+      const bool lead = ok && lane == __ffs(peers) - 1;
+      double e = 0.;
+      {
+        unsigned rem = ok ? peers : 0u;
+        const int maxcnt = __reduce_max_sync(NIDO_FULL_MASK, (unsigned)__popc(rem));
+        for (int it = 0; it < maxcnt; ++it) {
+          const int src = rem ? __ffs(rem) - 1 : lane;
+          const double x = __shfl_sync(NIDO_FULL_MASK, wt, src);
+          if (rem) { e += x; rem &= rem - 1; }
+        }
+      }
+      if (lead) {
+        bool isnew;
+        const int h = find_or_insert(keys, mask, X, &isnew);
+        if (h >= 0) {
+          atomicAdd(&vals[h], e);
+          atomicMin(&fpos[h], (int)(P - P0));
+        } else {
+          atomicAdd(q.err, 1ull);
+        }
+      }
+    }
+    if (threadIdx.x == 0) running_s = 0;
+    __syncthreads();
+    for (int64_t base = P0; base < P1; base += blockDim.x) {
+      const int64_t P = base + threadIdx.x;
+      const bool ok = P < P1;
+      int X = -1;
+      double wt = 0.;
+      int h = -1;
+      bool first = false;
+      if (ok) {
+        load_pos(q, m0, m1, P, X, wt);
+        h = find_slot(keys, mask, X);
+        first = h >= 0 && fpos[h] == (int)(P - P0);
+      }
+      const unsigned bal = __ballot_sync(NIDO_FULL_MASK, first);
+      if (lane == 0) wsum[wid] = __popc(bal);
+      __syncthreads();
+      int pre = running_s;
+      for (int i = 0; i < wid; ++i) pre += wsum[i];
+      if (first) {
+        const int idx = pre + __popc(bal & lanemask_lt());
+        q.tadj[P0 + idx] = X;
+        q.tw[P0 + idx] = vals[h];
+      }
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        int t = 0;
+        for (int i = 0; i < nwarp; ++i) t += wsum[i];
+        running_s += t;
+      }
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) q.degp[cp] = running_s;
+    for (unsigned i = threadIdx.x; i < cap; i += blockDim.x) { keys[i] = -1; vals[i] = 0.; fpos[i] = INT_MAX; }
+    __syncthreads();
+  }
+}
+
+// copy each coarse vertex's entries to its final offset
+__global__ void k_compact(int64_t nvp, const int64_t* __restrict__ mo, const int64_t* __restrict__ medge,
+                          const int64_t* __restrict__ coff, const int32_t* __restrict__ tadj,
+                          const double* __restrict__ tw, int32_t* __restrict__ adj, double* __restrict__ w) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t c = warp; c < nvp; c += nw) {
+    const int64_t src = medge[mo[c]], dst = coff[c], len = coff[c + 1] - coff[c];
+    for (int64_t i = lane; i < len; i += 32) {
+      adj[dst + i] = tadj[src + i];
+      w[dst + i] = tw[src + i];
+    }
+  }
+}
+
+}  // namespace
+
+int launch_aggregation(nido_graph_s* g, int* done) {
+  cudaStream_t s = g->ctx->stream;
+  const int64_t nv = g->nv;
+  *done = 1;
+  if (nv == 0) return NIDO_OK;
+  Arena ar(g->scratch, g->scratch_bytes);
+  int32_t* used = ar.take<int32_t>(nv);
+  int64_t* cid = ar.take<int64_t>(nv + 1);
+  int32_t* newid = ar.take<int32_t>(nv);
+  uint32_t* rk = ar.take<uint32_t>(nv);
+  uint32_t* rv = ar.take<uint32_t>(nv);
+  uint32_t* rk2 = ar.take<uint32_t>(nv);
+  uint32_t* rv2 = ar.take<uint32_t>(nv);
+  int64_t* mo = ar.take<int64_t>(nv + 1);
+  int64_t* medge = ar.take<int64_t>(nv + 1);
+  int64_t* degp = ar.take<int64_t>(nv + 1);
+  int64_t* counts = ar.take<int64_t>(4);
+  unsigned long long* maxd = ar.take<unsigned long long>(1);
+  int64_t* temp = ar.take<int64_t>(std::max(radix_temp_elems(nv), scan_temp_elems(nv + 1)));
+  if (!temp) return nido_set_error(NIDO_E_NOMEM, "scratch arena too small (aggregation)");
+  const unsigned gv = grid_for(nv, 256, kSMs * 16);
+  NIDO_CUDA_TRY(cudaMemsetAsync(used, 0, sizeof(int32_t) * nv, s));
+  k_mark_used<<<gv, 256, 0, s>>>(g->comm, nv, used);
+  NIDO_LAUNCH_CHECK();
+  NIDO_TRY(scan_exclusive_i32(used, cid, nv, temp, s));
+  k_newid<<<gv, 256, 0, s>>>(g->comm, cid, nv, newid, rk, rv);
+  NIDO_LAUNCH_CHECK();
+  k_compose<<<grid_for(g->nv0, 256, kSMs * 16), 256, 0, s>>>(g->clus, g->nv0, newid);
+  NIDO_LAUNCH_CHECK();
+  int64_t nvp = 0;
+  NIDO_CUDA_TRY(cudaMemcpyAsync(&nvp, cid + nv, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+  NIDO_CUDA_TRY(cudaStreamSynchronize(s));
+  if (nvp == nv || nvp == 1) return NIDO_OK;  // graph_gpu.cpp:1391-1392
+  *done = 0;
+  int bits = 0;
+  while (((int64_t)1 << bits) < nvp) ++bits;
+  NIDO_TRY(radix_sort_pairs(rk, rv, rk2, rv2, nv, bits, temp, s));
+  k_member_bounds<<<gv, 256, 0, s>>>(rk, rv, nv, nvp, g->off, mo, medge);
+  NIDO_LAUNCH_CHECK();
+  NIDO_TRY(scan_exclusive_i64(medge, medge, nv, temp, s));
+  NIDO_CUDA_TRY(cudaMemsetAsync(counts, 0, sizeof(int64_t) * 4, s));
+  NIDO_CUDA_TRY(cudaMemsetAsync(maxd, 0, sizeof(unsigned long long), s));
+  // coarse-vertex tiers (rk2/rv2 are free after the member sort)
+  uint32_t* tk = rk2;
+  uint32_t* tv = rv2;
+  uint32_t* tk2 = reinterpret_cast<uint32_t*>(used);
+  uint32_t* tv2 = reinterpret_cast<uint32_t*>(degp);  // degp is written only after the tier sort
+  k_agg_tiers<<<grid_for(nvp, 256, kSMs * 16), 256, 0, s>>>(mo, medge, nvp, tk, tv, counts, maxd);
+  NIDO_LAUNCH_CHECK();
+  NIDO_TRY(radix_sort_pairs(tk, tv, tk2, tv2, nvp, 2, temp, s));
+  int64_t cnt[4] = {0, 0, 0, 0};
+  unsigned long long maxu = 0;
+  NIDO_CUDA_TRY(cudaMemcpyAsync(cnt, counts, sizeof(cnt), cudaMemcpyDeviceToHost, s));
+  NIDO_CUDA_TRY(cudaMemcpyAsync(&maxu, maxd, sizeof(maxu), cudaMemcpyDeviceToHost, s));
+  NIDO_CUDA_TRY(cudaStreamSynchronize(s));
+
+  AggArgs q{g->off, g->adj, g->w, newid, rv, mo, medge, g->adj2, g->w2, degp, nvp,
+            reinterpret_cast<unsigned long long*>(g->dcount + 1)};
+  const int32_t* list = reinterpret_cast<const int32_t*>(tv);
+  if (cnt[0] > 0) {
+    const int capmax = 2 * kAggWarpMaxD;
+    const size_t sm = (size_t)8 * capmax * (sizeof(double) + 2 * sizeof(int));
+    NIDO_CUDA_TRY(cudaFuncSetAttribute(k_agg_warp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    k_agg_warp<<<grid_for(cnt[0], 8, kSMs * 8), 256, sm, s>>>(list, cnt[0], q, capmax);
+    NIDO_LAUNCH_CHECK();
+  }
+  if (cnt[1] > 0) {
+    const int capmax = kAggCtaMaxCap;
+    const size_t sm = (size_t)capmax * (sizeof(double) + 2 * sizeof(int));
+    NIDO_CUDA_TRY(cudaFuncSetAttribute(k_agg_cta<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    k_agg_cta<false><<<grid_for(cnt[1], 1, kSMs * 2), kAggThreads, sm, s>>>(list + cnt[0], cnt[1], q, capmax,
+                                                                          nullptr, nullptr, nullptr, 0);
+    NIDO_LAUNCH_CHECK();
+  }
+  if (cnt[2] > 0) {
+    int64_t slab = 64;
+    while (slab < 2 * (int64_t)maxu) slab <<= 1;
+    int64_t slabs = std::min<int64_t>(cnt[2], kSMs);
+    while (slabs > 1 && slabs * slab * 16 > ((int64_t)4 << 30)) slabs /= 2;
+    int32_t *gk = nullptr, *gf = nullptr;
+    double* gvv = nullptr;
+    NIDO_CUDA_TRY(cudaMallocAsync((void**)&gk, sizeof(int32_t) * slabs * slab, s));
+    NIDO_CUDA_TRY(cudaMallocAsync((void**)&gf, sizeof(int32_t) * slabs * slab, s));
+    NIDO_CUDA_TRY(cudaMallocAsync((void**)&gvv, sizeof(double) * slabs * slab, s));
+    NIDO_CUDA_TRY(cudaMemsetAsync(gk, 0xff, sizeof(int32_t) * slabs * slab, s));
+    NIDO_CUDA_TRY(cudaMemsetAsync(gf, 0x7f, sizeof(int32_t) * slabs * slab, s));
+    NIDO_CUDA_TRY(cudaMemsetAsync(gvv, 0, sizeof(double) * slabs * slab, s));
+    k_agg_cta<true><<<(unsigned)slabs, kAggThreads, 0, s>>>(list + cnt[0] + cnt[1], cnt[2], q, 0, gk, gvv, gf, slab);
+    NIDO_LAUNCH_CHECK();
+    NIDO_CUDA_TRY(cudaFreeAsync(gk, s));
+    NIDO_CUDA_TRY(cudaFreeAsync(gf, s));
+    NIDO_CUDA_TRY(cudaFreeAsync(gvv, s));
+  }
+  // coarse offsets into off2, then entries into adj/w (the old lists are dead)
+  NIDO_TRY(scan_exclusive_i64(degp, g->off2, nvp, temp, s));
+  k_compact<<<grid_for(nvp * 32, 256, kSMs * 16), 256, 0, s>>>(nvp, mo, medge, g->off2, g->adj2, g->w2, g->adj, g->w);
+  NIDO_LAUNCH_CHECK();
+  int64_t nep = 0, nerr = 0;
+  NIDO_CUDA_TRY(cudaMemcpyAsync(&nep, g->off2 + nvp, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+  NIDO_CUDA_TRY(cudaMemcpyAsync(&nerr, g->dcount + 1, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+  NIDO_CUDA_TRY(cudaStreamSynchronize(s));
+  if (nerr) return nido_set_error(NIDO_E_CUDA, "hash table overflow in %lld probes", (long long)nerr);
+  std::swap(g->off, g->off2);
+  g->nv = nvp;
+  g->ne = nep;
+  g->bins_valid = false;
+  return NIDO_OK;
+}
+
+}  // namespace nido

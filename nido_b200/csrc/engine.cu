@@ -1,0 +1,518 @@
+// engine.cu -- C ABI of the engine: contexts, graph upload, the step-level
+// operators of the reference's GraphGPU (graph_gpu.hpp:168-247) and the
+// whole-run driver LouvainGPU::run (louvain_gpu.cpp:6-139).
+#include <omp.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <chrono>
+#include <new>
+#include <vector>
+
+#include "common.cuh"
+#include "engine.cuh"
+#include "primitives.cuh"
+
+using nido::Arena;
+
+namespace {
+
+template <typename T>
+int dev_alloc(nido_ctx ctx, T** p, int64_t n) {
+  const size_t bytes = sizeof(T) * (size_t)(n > 0 ? n : 1);
+  if (ctx->budget && ctx->used + bytes > ctx->budget)
+    return nido_set_error(NIDO_E_NOMEM, "HBM budget of %zu bytes exceeded", ctx->budget);
+  cudaError_t e = cudaMalloc((void**)p, bytes);
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    cudaGetLastError();
+    return nido_set_error(NIDO_E_NOMEM, "cudaMalloc(%zu) failed: %s", bytes, cudaGetErrorString(e));
+  }
+  ctx->used += bytes;
+  return NIDO_OK;
+}
+
+void dev_free(nido_ctx ctx, void* p, size_t bytes) {
+  if (p) {
+    cudaFree(p);
+    ctx->used -= std::min(ctx->used, bytes);
+  }
+}
+
+// Narrow int64 neighbour ids to int32 while checking 0 <= id < nv; offsets
+// must be non-decreasing and start at 0.
+__global__ void k_narrow(const int64_t* __restrict__ adj64, int64_t ne, int64_t nv,
+                         int32_t* __restrict__ adj, const int64_t* __restrict__ off,
+                         unsigned long long* __restrict__ bad) {
+  unsigned long long b = 0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < ne;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t x = adj64[i];
+    if (x < 0 || x >= nv) ++b;
+    adj[i] = (int32_t)x;
+  }
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nv;
+       i += (int64_t)gridDim.x * blockDim.x)
+    if (off[i + 1] < off[i]) ++b;
+  if (b) atomicAdd(bad, b);
+}
+
+__global__ void k_iota(int32_t* __restrict__ x, int64_t n) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    x[i] = (int32_t)i;
+}
+
+__global__ void k_widen(const int32_t* __restrict__ x, int64_t n, int64_t* __restrict__ y) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    y[i] = x[i];
+}
+
+// comm ids from int64 with range check; newc gets the same ids
+__global__ void k_set_ids(const int64_t* __restrict__ c64, int64_t nv, int32_t* __restrict__ comm,
+                          int32_t* __restrict__ newc, unsigned long long* __restrict__ bad) {
+  unsigned long long b = 0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nv;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t c = c64[i];
+    if (c < 0 || c >= nv) ++b;
+    const int32_t ci = (c < 0 || c >= nv) ? 0 : (int32_t)c;
+    comm[i] = ci;
+    newc[i] = ci;
+  }
+  if (b) atomicAdd(bad, b);
+}
+
+constexpr unsigned kGrid = 148 * 8;
+
+int size_global_slabs(nido_graph g) {
+  // slabs for the global-memory tier of the move kernel and coarsening
+  if (g->max_degree <= g->ctx->tiers.cta_max) return NIDO_OK;
+  unsigned need = 64;
+  while ((int64_t)need < 2 * g->max_degree) need <<= 1;
+  if ((int64_t)need <= g->gslab) return NIDO_OK;
+  nido_ctx ctx = g->ctx;
+  dev_free(ctx, g->gkeys, sizeof(int32_t) * (size_t)g->gslab * g->gslabs);
+  dev_free(ctx, g->gvals, sizeof(double) * (size_t)g->gslab * g->gslabs);
+  g->gkeys = nullptr; g->gvals = nullptr; g->gslab = 0; g->gslabs = 0;
+  int slabs = nido::kSMs * 2;
+  while (slabs > 8 && (size_t)slabs * need * 12 > ((size_t)2 << 30)) slabs /= 2;
+  NIDO_TRY(dev_alloc(ctx, &g->gkeys, (int64_t)slabs * need));
+  NIDO_TRY(dev_alloc(ctx, &g->gvals, (int64_t)slabs * need));
+  NIDO_CUDA_TRY(cudaMemsetAsync(g->gkeys, 0xff, sizeof(int32_t) * (size_t)slabs * need, ctx->stream));
+  NIDO_CUDA_TRY(cudaMemsetAsync(g->gvals, 0, sizeof(double) * (size_t)slabs * need, ctx->stream));
+  g->gslab = need;
+  g->gslabs = slabs;
+  return NIDO_OK;
+}
+
+int prepare_phase(nido_graph g) {
+  NIDO_TRY(nido::launch_vertex_weights(g));
+  NIDO_TRY(nido::launch_mass(g));
+  g->bins_valid = false;
+  NIDO_TRY(nido::build_batches(g));
+  NIDO_TRY(size_global_slabs(g));
+  return NIDO_OK;
+}
+
+}  // namespace
+
+namespace nido {
+int graph_prepare_phase(nido_graph g) { return prepare_phase(g); }
+}
+
+extern "C" int nido_ctx_create(int device, size_t hbm_budget_bytes, nido_ctx* out) {
+  if (!out) return nido_set_error(NIDO_E_INVALID, "nido_ctx_create: null output");
+  *out = nullptr;
+  int n = 0;
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+    cudaGetLastError();
+    return nido_set_error(NIDO_E_NODEVICE, "no CUDA device available");
+  }
+  if (device < 0 || device >= n) return nido_set_error(NIDO_E_INVALID, "device %d out of range", device);
+  NIDO_CUDA_TRY(cudaSetDevice(device));
+  cudaDeviceProp prop;
+  NIDO_CUDA_TRY(cudaGetDeviceProperties(&prop, device));
+  if (prop.major != 10)
+    return nido_set_error(NIDO_E_NODEVICE, "device %d is sm_%d%d; this build targets sm_100a", device,
+                          prop.major, prop.minor);
+  nido_ctx ctx = new (std::nothrow) nido_ctx_s();
+  if (!ctx) return nido_set_error(NIDO_E_NOMEM, "host allocation failed");
+  ctx->device = device;
+  ctx->budget = hbm_budget_bytes;
+  NIDO_CUDA_TRY(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
+  NIDO_CUDA_TRY(cudaEventCreate(&ctx->ev0));
+  NIDO_CUDA_TRY(cudaEventCreate(&ctx->ev1));
+  *out = ctx;
+  return NIDO_OK;
+}
+
+extern "C" int nido_ctx_destroy(nido_ctx ctx) {
+  if (!ctx) return NIDO_OK;
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  cudaEventDestroy(ctx->ev0);
+  cudaEventDestroy(ctx->ev1);
+  for (cudaEvent_t e : ctx->move_ev) cudaEventDestroy(e);
+  cudaStreamDestroy(ctx->stream);
+  delete ctx;
+  return NIDO_OK;
+}
+
+extern "C" int nido_ctx_sync(nido_ctx ctx) {
+  if (!ctx) return nido_set_error(NIDO_E_INVALID, "null context");
+  NIDO_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
+  return NIDO_OK;
+}
+
+extern "C" int nido_ctx_stream(nido_ctx ctx, void** stream) {
+  if (!ctx || !stream) return nido_set_error(NIDO_E_INVALID, "null argument");
+  *stream = (void*)ctx->stream;
+  return NIDO_OK;
+}
+
+extern "C" int nido_graph_free(nido_graph g) {
+  if (!g) return NIDO_OK;
+  nido_ctx ctx = g->ctx;
+  cudaSetDevice(ctx->device);
+  cudaStreamSynchronize(ctx->stream);
+  const int64_t V = g->cap_v, E = g->cap_e;
+  dev_free(ctx, g->off, 8 * (V + 1)); dev_free(ctx, g->off2, 8 * (V + 1));
+  dev_free(ctx, g->adj, 4 * E); dev_free(ctx, g->adj2, 4 * E);
+  dev_free(ctx, g->w, 8 * E); dev_free(ctx, g->w2, 8 * E);
+  dev_free(ctx, g->k, 8 * V); dev_free(ctx, g->a, 8 * V);
+  dev_free(ctx, g->comm, 4 * V); dev_free(ctx, g->newc, 4 * V);
+  dev_free(ctx, g->clus, 4 * g->nv0); dev_free(ctx, g->perm, 4 * V);
+  dev_free(ctx, g->dm, 64); dev_free(ctx, g->dcount, 64);
+  dev_free(ctx, g->scratch, g->scratch_bytes);
+  dev_free(ctx, g->gkeys, sizeof(int32_t) * (size_t)g->gslab * g->gslabs);
+  dev_free(ctx, g->gvals, sizeof(double) * (size_t)g->gslab * g->gslabs);
+  delete g;
+  return NIDO_OK;
+}
+
+extern "C" int nido_graph_upload(nido_ctx ctx, int64_t nv, int64_t ne, const int64_t* off,
+                                 const int64_t* adj, const double* w, int32_t nbatches,
+                                 nido_graph* out) {
+  if (!ctx || !out || !off || (ne > 0 && (!adj || !w)))
+    return nido_set_error(NIDO_E_INVALID, "nido_graph_upload: null argument");
+  *out = nullptr;
+  if (nv < 0 || ne < 0) return nido_set_error(NIDO_E_INVALID, "negative graph size");
+  if (nv >= ((int64_t)1 << 31) - 1) return nido_set_error(NIDO_E_TOO_LARGE, "%lld vertices exceed 2^31-1", (long long)nv);
+  if (nbatches < 1) return nido_set_error(NIDO_E_INVALID, "nbatches must be >= 1 (got %d)", nbatches);
+  if (off[0] != 0 || off[nv] != ne) return nido_set_error(NIDO_E_INVALID, "offsets must run from 0 to ne");
+  NIDO_CUDA_TRY(cudaSetDevice(ctx->device));
+  nido_graph g = new (std::nothrow) nido_graph_s();
+  if (!g) return nido_set_error(NIDO_E_NOMEM, "host allocation failed");
+  g->ctx = ctx;
+  g->nv0 = g->nv = g->cap_v = nv;
+  g->ne = g->cap_e = ne;
+  g->nbatches = nbatches;
+  const int64_t V = nv, E = ne;
+  int st = NIDO_OK;
+#define ALLOC(p, n) if (st == NIDO_OK) st = dev_alloc(ctx, &g->p, (n))
+  ALLOC(off, V + 1); ALLOC(off2, V + 1);
+  ALLOC(adj, E); ALLOC(adj2, E);
+  ALLOC(w, E); ALLOC(w2, E);
+  ALLOC(k, V); ALLOC(a, V);
+  ALLOC(comm, V); ALLOC(newc, V);
+  ALLOC(clus, V); ALLOC(perm, V);
+  ALLOC(dm, 8); ALLOC(dcount, 8);
+#undef ALLOC
+  // scratch: radix sort / modularity / coarsening temporaries
+  g->scratch_bytes = (size_t)64 * (V + 1) + (size_t)(1 << 20) +
+                     sizeof(int64_t) * (size_t)(nido::radix_temp_elems(V) + nido::scan_temp_elems(E + 1));
+  if (st == NIDO_OK) st = dev_alloc(ctx, &g->scratch, (int64_t)g->scratch_bytes);
+  if (st != NIDO_OK) { nido_graph_free(g); return st; }
+  cudaStream_t s = ctx->stream;
+  // int64 ids travel in the (not yet used) w2 buffer and are narrowed on device
+  int64_t* adj64 = reinterpret_cast<int64_t*>(g->w2);
+  NIDO_CUDA_TRY(cudaMemcpyAsync(g->off, off, 8 * (V + 1), cudaMemcpyHostToDevice, s));
+  if (E > 0) {
+    NIDO_CUDA_TRY(cudaMemcpyAsync(adj64, adj, 8 * E, cudaMemcpyHostToDevice, s));
+    NIDO_CUDA_TRY(cudaMemcpyAsync(g->w, w, 8 * E, cudaMemcpyHostToDevice, s));
+  }
+  unsigned long long* bad = reinterpret_cast<unsigned long long*>(g->dcount);
+  NIDO_CUDA_TRY(cudaMemsetAsync(g->dcount, 0, 8 * sizeof(int64_t), s));
+  k_narrow<<<kGrid, 256, 0, s>>>(adj64, E, V, g->adj, g->off, bad);
+  NIDO_LAUNCH_CHECK();
+  k_iota<<<kGrid, 256, 0, s>>>(g->clus, V);
+  NIDO_LAUNCH_CHECK();
+  unsigned long long nbad = 0;
+  NIDO_CUDA_TRY(cudaMemcpyAsync(&nbad, bad, 8, cudaMemcpyDeviceToHost, s));
+  NIDO_CUDA_TRY(cudaStreamSynchronize(s));
+  if (nbad) {
+    nido_graph_free(g);
+    return nido_set_error(NIDO_E_INVALID, "%llu neighbour ids out of range or decreasing offsets", nbad);
+  }
+  st = prepare_phase(g);
+  if (st == NIDO_OK) st = nido::launch_singleton(g);
+  if (st != NIDO_OK) { nido_graph_free(g); return st; }
+  *out = g;
+  return NIDO_OK;
+}
+
+extern "C" int nido_graph_size(nido_graph g, int64_t* nv, int64_t* ne) {
+  if (!g) return nido_set_error(NIDO_E_INVALID, "null graph");
+  if (nv) *nv = g->nv;
+  if (ne) *ne = g->ne;
+  return NIDO_OK;
+}
+
+extern "C" int nido_graph_download(nido_graph g, int64_t* off, int64_t* adj, double* w) {
+  if (!g) return nido_set_error(NIDO_E_INVALID, "null graph");
+  cudaStream_t s = g->ctx->stream;
+  NIDO_CUDA_TRY(cudaSetDevice(g->ctx->device));
+  if (off) NIDO_CUDA_TRY(cudaMemcpyAsync(off, g->off, 8 * (g->nv + 1), cudaMemcpyDeviceToHost, s));
+  if (w && g->ne) NIDO_CUDA_TRY(cudaMemcpyAsync(w, g->w, 8 * g->ne, cudaMemcpyDeviceToHost, s));
+  if (adj && g->ne) {
+    int64_t* tmp = reinterpret_cast<int64_t*>(g->w2);  // ne doubles, free outside coarsening
+    k_widen<<<kGrid, 256, 0, s>>>(g->adj, g->ne, tmp);
+    NIDO_LAUNCH_CHECK();
+    NIDO_CUDA_TRY(cudaMemcpyAsync(adj, tmp, 8 * g->ne, cudaMemcpyDeviceToHost, s));
+  }
+  NIDO_CUDA_TRY(cudaStreamSynchronize(s));
+  return NIDO_OK;
+}
+
+extern "C" int nido_graph_batches(nido_graph g, int64_t* cuts) {
+  if (!g || !cuts) return nido_set_error(NIDO_E_INVALID, "null argument");
+  if (!g->bins_valid) NIDO_TRY(nido::build_batches(g));
+  std::copy(g->cuts.begin(), g->cuts.end(), cuts);
+  return NIDO_OK;
+}
+
+extern "C" int nido_graph_vertex_weights(nido_graph g, double* k, double* m) {
+  if (!g) return nido_set_error(NIDO_E_INVALID, "null graph");
+  if (k) {
+    NIDO_CUDA_TRY(cudaMemcpyAsync(k, g->k, 8 * g->nv, cudaMemcpyDeviceToHost, g->ctx->stream));
+    NIDO_CUDA_TRY(cudaStreamSynchronize(g->ctx->stream));
+  }
+  if (m) *m = g->m;
+  return NIDO_OK;
+}
+
+extern "C" int nido_singleton_partition(nido_graph g) {
+  if (!g) return nido_set_error(NIDO_E_INVALID, "null graph");
+  return nido::launch_singleton(g);
+}
+
+extern "C" int nido_set_community_ids(nido_graph g, const int64_t* comm) {
+  if (!g || !comm) return nido_set_error(NIDO_E_INVALID, "null argument");
+  cudaStream_t s = g->ctx->stream;
+  Arena ar(g->scratch, g->scratch_bytes);
+  int64_t* c64 = ar.take<int64_t>(g->nv);
+  if (!c64) return nido_set_error(NIDO_E_NOMEM, "scratch arena too small");
+  NIDO_CUDA_TRY(cudaMemcpyAsync(c64, comm, 8 * g->nv, cudaMemcpyHostToDevice, s));
+  unsigned long long* bad = reinterpret_cast<unsigned long long*>(g->dcount);
+  NIDO_CUDA_TRY(cudaMemsetAsync(bad, 0, 8, s));
+  k_set_ids<<<kGrid, 256, 0, s>>>(c64, g->nv, g->comm, g->newc, bad);
+  NIDO_LAUNCH_CHECK();
+  NIDO_TRY(nido::launch_set_comm(g));
+  unsigned long long nbad = 0;
+  NIDO_CUDA_TRY(cudaMemcpyAsync(&nbad, bad, 8, cudaMemcpyDeviceToHost, s));
+  NIDO_CUDA_TRY(cudaStreamSynchronize(s));
+  if (nbad) return nido_set_error(NIDO_E_INVALID, "%llu community ids outside [0, nv)", nbad);
+  return NIDO_OK;
+}
+
+extern "C" int nido_compute_modularity(nido_graph g, double* q) {
+  if (!g || !q) return nido_set_error(NIDO_E_INVALID, "null argument");
+  return nido::launch_modularity(g, q);
+}
+
+extern "C" int nido_louvain_update(nido_graph g, int32_t batch, int32_t tie_mode) {
+  if (!g) return nido_set_error(NIDO_E_INVALID, "null graph");
+  if (tie_mode != NIDO_TIE_SMALLEST_ID && tie_mode != NIDO_TIE_NIDO)
+    return nido_set_error(NIDO_E_INVALID, "unknown tie mode %d", tie_mode);
+  return nido::launch_move(g, batch, tie_mode, nullptr, nullptr);
+}
+
+// The reference updates community degrees and then swaps ids as two calls
+// (graph_gpu.cpp:779-820); the engine fuses them into one kernel, so the
+// degree update performs both and the id update is a no-op kept for API
+// parity.  Calling them in the reference's order gives the reference's state.
+extern "C" int nido_update_community_weights(nido_graph g, int32_t batch) {
+  if (!g) return nido_set_error(NIDO_E_INVALID, "null graph");
+  if (batch < 0 || batch >= g->nbatches) return nido_set_error(NIDO_E_INVALID, "batch out of range");
+  if (!g->bins_valid) NIDO_TRY(nido::build_batches(g));
+  return nido::launch_commit(g, g->cuts[batch], g->cuts[batch + 1]);
+}
+
+extern "C" int nido_update_community_ids(nido_graph g, int32_t batch) {
+  if (!g) return nido_set_error(NIDO_E_INVALID, "null graph");
+  if (batch < 0 || batch >= g->nbatches) return nido_set_error(NIDO_E_INVALID, "batch out of range");
+  return NIDO_OK;
+}
+
+extern "C" int nido_restore_community(nido_graph g) {
+  if (!g) return nido_set_error(NIDO_E_INVALID, "null graph");
+  return nido::launch_commit(g, 0, g->nv);
+}
+
+extern "C" int nido_aggregation(nido_graph g, int32_t* done) {
+  if (!g || !done) return nido_set_error(NIDO_E_INVALID, "null argument");
+  int d = 0;
+  NIDO_TRY(nido::launch_aggregation(g, &d));
+  *done = d;
+  if (!d) NIDO_TRY(prepare_phase(g));
+  return NIDO_OK;
+}
+
+extern "C" int nido_get_state(nido_graph g, int64_t* comm, int64_t* newcomm, double* a) {
+  if (!g) return nido_set_error(NIDO_E_INVALID, "null graph");
+  cudaStream_t s = g->ctx->stream;
+  Arena ar(g->scratch, g->scratch_bytes);
+  int64_t* tmp = ar.take<int64_t>(g->nv);
+  if (!tmp) return nido_set_error(NIDO_E_NOMEM, "scratch arena too small");
+  if (comm) {
+    k_widen<<<kGrid, 256, 0, s>>>(g->comm, g->nv, tmp);
+    NIDO_LAUNCH_CHECK();
+    NIDO_CUDA_TRY(cudaMemcpyAsync(comm, tmp, 8 * g->nv, cudaMemcpyDeviceToHost, s));
+    NIDO_CUDA_TRY(cudaStreamSynchronize(s));
+  }
+  if (newcomm) {
+    k_widen<<<kGrid, 256, 0, s>>>(g->newc, g->nv, tmp);
+    NIDO_LAUNCH_CHECK();
+    NIDO_CUDA_TRY(cudaMemcpyAsync(newcomm, tmp, 8 * g->nv, cudaMemcpyDeviceToHost, s));
+    NIDO_CUDA_TRY(cudaStreamSynchronize(s));
+  }
+  if (a) NIDO_CUDA_TRY(cudaMemcpyAsync(a, g->a, 8 * g->nv, cudaMemcpyDeviceToHost, s));
+  NIDO_CUDA_TRY(cudaStreamSynchronize(s));
+  return NIDO_OK;
+}
+
+extern "C" int nido_get_clustering(nido_graph g, int64_t* clustering) {
+  if (!g || !clustering) return nido_set_error(NIDO_E_INVALID, "null argument");
+  cudaStream_t s = g->ctx->stream;
+  Arena ar(g->scratch, g->scratch_bytes);
+  int64_t* tmp = ar.take<int64_t>(g->nv0);
+  if (!tmp) return nido_set_error(NIDO_E_NOMEM, "scratch arena too small");
+  k_widen<<<kGrid, 256, 0, s>>>(g->clus, g->nv0, tmp);
+  NIDO_LAUNCH_CHECK();
+  NIDO_CUDA_TRY(cudaMemcpyAsync(clustering, tmp, 8 * g->nv0, cudaMemcpyDeviceToHost, s));
+  NIDO_CUDA_TRY(cudaStreamSynchronize(s));
+  return NIDO_OK;
+}
+
+extern "C" int nido_dump_partition(nido_graph g, const char* path, const int64_t* new_orders) {
+  if (!g || !path) return nido_set_error(NIDO_E_INVALID, "null argument");
+  std::vector<int64_t> c(g->nv0);
+  NIDO_TRY(nido_get_clustering(g, c.data()));
+  if (new_orders) {
+    std::vector<int64_t> t(g->nv0);
+    for (int64_t i = 0; i < g->nv0; ++i) t[new_orders[i]] = c[i];
+    c.swap(t);
+  }
+  FILE* f = fopen(path, "wt");
+  if (!f) return nido_set_error(NIDO_E_IO, "cannot open %s", path);
+  std::vector<char> buf;
+  buf.reserve(1 << 20);
+  char line[32];
+  for (int64_t i = 0; i < g->nv0; ++i) {
+    const int n = snprintf(line, sizeof(line), "%lld\n", (long long)c[i]);
+    buf.insert(buf.end(), line, line + n);
+    if (buf.size() > (1u << 20)) { fwrite(buf.data(), 1, buf.size(), f); buf.clear(); }
+  }
+  fwrite(buf.data(), 1, buf.size(), f);
+  if (fclose(f) != 0) return nido_set_error(NIDO_E_IO, "short write to %s", path);
+  return NIDO_OK;
+}
+
+// LouvainGPU::run (louvain_gpu.cpp:28-124): phases of singleton start,
+// iterations of batched moves until dQ <= tau or max_iter, undo of an
+// iteration that lowered Q, and aggregation when the phase gained more
+// than tau.
+extern "C" int nido_run(nido_graph g, const nido_params* p, int64_t* out_comm, nido_run_stats* stats) {
+  if (!g || !p) return nido_set_error(NIDO_E_INVALID, "null argument");
+  if (p->nbatches != g->nbatches)
+    return nido_set_error(NIDO_E_INVALID, "params.nbatches (%d) differs from the graph's (%d)", p->nbatches, g->nbatches);
+  if (p->tie_mode != NIDO_TIE_SMALLEST_ID && p->tie_mode != NIDO_TIE_NIDO)
+    return nido_set_error(NIDO_E_INVALID, "unknown tie mode %d", p->tie_mode);
+  NIDO_CUDA_TRY(cudaSetDevice(g->ctx->device));
+  nido_run_stats st;
+  memset(&st, 0, sizeof(st));
+  cudaStream_t s = g->ctx->stream;
+  cudaEvent_t t0, t1;
+  NIDO_CUDA_TRY(cudaEventCreate(&t0));
+  NIDO_CUDA_TRY(cudaEventCreate(&t1));
+  NIDO_CUDA_TRY(cudaEventRecord(t0, s));
+  const double tau = p->tau;
+  bool done = false;
+  int64_t phases = 0;
+  while (!done && phases < 200) {
+    if (p->verbose) printf("PHASE #%lld: \n", (long long)phases);
+    NIDO_TRY(nido::launch_singleton(g));
+    double Q;
+    NIDO_TRY(nido::launch_modularity(g, &Q));
+    const double Q_old = Q;
+    if (p->verbose) printf("LOOP# \tQ \t\tdQ\n----------------------------------------\n0 \t%g \t0\n", Q);
+    double dQ = NIDO_MAX_FLOAT;
+    int64_t loops = 0;
+    while (tau < dQ && loops < p->max_iter) {
+      std::vector<cudaEvent_t>& ev = g->ctx->move_ev;
+      while (ev.size() < 2 * (size_t)g->nbatches) {
+        cudaEvent_t e;
+        NIDO_CUDA_TRY(cudaEventCreate(&e));
+        ev.push_back(e);
+      }
+      for (int b = 0; b < g->nbatches; ++b) {
+        NIDO_TRY(nido::launch_move(g, b, p->tie_mode, ev[2 * b], ev[2 * b + 1]));
+        NIDO_TRY(nido::launch_commit(g, g->cuts[b], g->cuts[b + 1]));
+      }
+      st.move_launches += g->nbatches;
+      st.edges_scanned += (double)g->ne;
+      st.move_bytes += 16.0 * (double)g->ne + 32.0 * (double)g->nv;
+      double Qtmp;
+      NIDO_TRY(nido::launch_modularity(g, &Qtmp));
+      dQ = Qtmp - Q;
+      ++loops;
+      for (int b = 0; b < g->nbatches; ++b) {  // complete: the Q readback synchronized the stream
+        float ms = 0.f;
+        NIDO_CUDA_TRY(cudaEventElapsedTime(&ms, ev[2 * b], ev[2 * b + 1]));
+        st.move_ms += ms;
+      }
+      if (dQ < 0) NIDO_TRY(nido::launch_commit(g, 0, g->nv));
+      else Q = Qtmp;
+      if (p->verbose) printf("%lld \t%g \t%g\n", (long long)loops, Qtmp, dQ);
+    }
+    if (phases < 200) {
+      st.q_phase[phases] = Q;
+      st.loops_phase[phases] = loops;
+      st.nv_phase[phases] = g->nv;
+      st.ne_phase[phases] = g->ne;
+    }
+    st.total_loops += loops;
+    st.final_q = Q;
+    if (p->verbose) {
+      if (loops >= p->max_iter) printf("Exceed maximum loop number\n");
+      printf("Final Q: %g\n", Q);
+    }
+    if (Q - Q_old > tau) {
+      int d = 0;
+      NIDO_TRY(nido::launch_aggregation(g, &d));
+      done = d != 0;
+      if (!done) NIDO_TRY(prepare_phase(g));
+    } else {
+      done = true;
+    }
+    if (p->verbose) printf("----------------------------------------\n");
+    ++phases;
+  }
+  NIDO_CUDA_TRY(cudaEventRecord(t1, s));
+  NIDO_CUDA_TRY(cudaEventSynchronize(t1));
+  float tot = 0.f;
+  NIDO_CUDA_TRY(cudaEventElapsedTime(&tot, t0, t1));
+  cudaEventDestroy(t0);
+  cudaEventDestroy(t1);
+  st.total_ms = tot;
+  st.phases = phases;
+  int64_t nerr = 0;
+  NIDO_CUDA_TRY(cudaMemcpy(&nerr, g->dcount + 1, sizeof(int64_t), cudaMemcpyDeviceToHost));
+  if (nerr) return nido_set_error(NIDO_E_CUDA, "hash table overflow in %lld probes", (long long)nerr);
+  if (out_comm) NIDO_TRY(nido_get_clustering(g, out_comm));
+  if (stats) *stats = st;
+  return NIDO_OK;
+}

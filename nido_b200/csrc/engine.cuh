@@ -1,0 +1,122 @@
+// engine.cuh -- device state of one graph and the kernel launchers that
+// operate on it.
+//
+// HBM layout of a graph (all arrays resident for the whole run):
+//   off   int64[nv+1]   CSR offsets            adj  int32[ne]  neighbour ids
+//   w     f64[ne]       edge weights           k    f64[nv]    vertex weights k_v
+//   comm  int32[nv]     community ids          newc int32[nv]  move targets / undo ids
+//   a     f64[nv]       community degrees a_c (indexed by community id)
+//   clus  int32[nv0]    clustering of the original vertices
+//   perm  int32[nv]     vertex list ordered by (batch, degree tier, id)
+// plus ping-pong CSR buffers for coarsening and a scratch arena.
+#ifndef NIDO_ENGINE_CUH_
+#define NIDO_ENGINE_CUH_
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <vector>
+
+#include "common.cuh"
+
+// degree tiers of the move / modularity kernels
+enum Tier {
+  kTierG4 = 0,  // d <= 4   : 4-lane group per vertex, registers
+  kTierG8,      // d <= 8   : 8-lane group
+  kTierG16,     // d <= 16  : 16-lane group
+  kTierG32,     // d <= 32  : one warp, registers
+  kTierWarp,    // d <= warp_max : one warp, shared-memory hash
+  kTierCta,     // d <= cta_max  : one CTA, shared-memory hash
+  kTierGlobal,  // larger        : one CTA, hash table in global memory (L2)
+  kNumTiers
+};
+
+struct TierConfig {
+  int warp_max = 256;     // largest degree handled by the warp tier
+  int cta_max = 4096;     // largest degree handled by the CTA shared-memory tier
+  int warps_per_cta = 8;  // CTAs of the warp tier
+  int cta_threads = 512;  // CTAs of the CTA / global tiers
+};
+
+struct nido_ctx_s {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  size_t budget = 0;
+  size_t used = 0;
+  TierConfig tiers;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  std::vector<cudaEvent_t> move_ev;  // 2 per batch, for per-iteration move timing
+};
+
+struct nido_graph_s {
+  nido_ctx ctx = nullptr;
+  int64_t nv0 = 0;           // original vertex count
+  int64_t nv = 0, ne = 0;    // current phase
+  int64_t cap_v = 0, cap_e = 0;
+  int nbatches = 1;
+  bool int_weights = false;  // every weight integral and total below 2^53
+  double m = 0.0;            // host copy of the mass
+
+  int64_t* off = nullptr;
+  int32_t* adj = nullptr;
+  double* w = nullptr;
+  int64_t* off2 = nullptr;
+  int32_t* adj2 = nullptr;
+  double* w2 = nullptr;
+  double* k = nullptr;
+  double* a = nullptr;
+  int32_t* comm = nullptr;
+  int32_t* newc = nullptr;
+  int32_t* clus = nullptr;
+  int32_t* perm = nullptr;
+  double* dm = nullptr;      // device scalars: [0] m, [1] Q, [2..] spare
+  int64_t* dcount = nullptr; // device counters
+  // scratch arena (bytes), carved per operation
+  char* scratch = nullptr;
+  size_t scratch_bytes = 0;
+  // global-memory hash slabs for the largest tier (move and coarsening)
+  int32_t* gkeys = nullptr;
+  double* gvals = nullptr;
+  int64_t gslab = 0;   // slots per CTA slab
+  int gslabs = 0;      // number of slabs
+
+  std::vector<int64_t> cuts;     // host batch cuts (nbatches+1)
+  std::vector<int64_t> tier_off; // host: nbatches*kNumTiers+1 offsets into perm
+  bool bins_valid = false;
+  int64_t max_degree = 0;
+  double host_pinned_dummy = 0;
+};
+
+namespace nido {
+
+// bump allocation inside the graph's scratch arena
+struct Arena {
+  char* base;
+  size_t size;
+  size_t used = 0;
+  Arena(char* b, size_t s) : base(b), size(s) {}
+  template <typename T>
+  T* take(int64_t n) {
+    size_t off = (used + 255) & ~(size_t)255;
+    size_t bytes = sizeof(T) * (size_t)(n > 0 ? n : 1);
+    if (off + bytes > size) return nullptr;
+    used = off + bytes;
+    return reinterpret_cast<T*>(base + off);
+  }
+};
+
+// phase-level kernels (phase.cu)
+int launch_vertex_weights(nido_graph_s* g);             // k_v, nido order
+int launch_mass(nido_graph_s* g);                       // g->m (host) and dm[0]
+int launch_singleton(nido_graph_s* g);
+int launch_set_comm(nido_graph_s* g);                   // a from comm
+int launch_commit(nido_graph_s* g, int64_t v0, int64_t v1);
+int launch_modularity(nido_graph_s* g, double* q);      // host value
+int build_batches(nido_graph_s* g);                     // cuts (host) + tier lists
+// move phase (move.cu)
+// ev_start / ev_end (may be null) are recorded around the tier kernels
+int launch_move(nido_graph_s* g, int batch, int tie, cudaEvent_t ev_start, cudaEvent_t ev_end);
+// coarsening (coarsen.cu)
+int launch_aggregation(nido_graph_s* g, int* done);
+
+}  // namespace nido
+#endif

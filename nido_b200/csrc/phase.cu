@@ -1,0 +1,414 @@
+// phase.cu -- per-phase and per-iteration kernels around the move phase:
+// vertex weights k_v, mass m, singleton start, community-degree commit and
+// restore (FP64 atomics), modularity, and the -b batch cuts with the degree
+// tier lists.
+//
+// k_v, m and Q are reduced in exactly the order of the reference kernels
+// (cited below), so they are bit-identical to the reference given the same
+// inputs; the per-vertex in-community sums inside Q use a fixed order of this
+// engine, which equals the reference's wherever the sums are exact (integer
+// weights).
+#include <algorithm>
+
+#include "common.cuh"
+#include "engine.cuh"
+#include "primitives.cuh"
+
+namespace nido {
+namespace {
+
+constexpr int kThreads = 256;
+
+inline unsigned grid_for(int64_t work, int per_block, int max_blocks = 148 * 16) {
+  int64_t b = (work + per_block - 1) / per_block;
+  if (b < 1) b = 1;
+  if (b > max_blocks) b = max_blocks;
+  return (unsigned)b;
+}
+
+// k_v: one warp per vertex, lane l sums edges l, l+32, ... then a shuffle-down
+// tree (sum_vertex_weights_kernel, graph_cuda.cu:302-346).
+__global__ void k_vertex_weights(const int64_t* __restrict__ off, const double* __restrict__ w,
+                                 int64_t nv, double* __restrict__ k) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t v = warp; v < nv; v += nw) {
+    const int64_t s = off[v], e = off[v + 1];
+    double x = 0.;
+    for (int64_t j = s + lane; j < e; j += 32) x += w[j];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(NIDO_FULL_MASK, x, o);
+    if (lane == 0) k[v] = x;
+  }
+}
+
+// m, first stage: compute_mass_reduce_kernel<32><<<4096,32>>>
+// (graph_cuda.cu:1786-1804).
+__global__ void k_mass_blocks(const double* __restrict__ k, int64_t nv, double* __restrict__ part) {
+  double x = 0.;
+  for (int64_t i = threadIdx.x + 32 * (int64_t)blockIdx.x; i < nv; i += 32 * (int64_t)gridDim.x) x += k[i];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(NIDO_FULL_MASK, x, o);
+  if (threadIdx.x == 0) part[blockIdx.x] = x;
+}
+
+// reduce_vector_kernel<32><<<1,1024>>> (graph_cuda.cu:1806-1835); writes
+// scale * sum to *out.
+__global__ void __launch_bounds__(1024) k_reduce_1024(const double* __restrict__ x, int64_t n,
+                                                      double scale, double* __restrict__ out) {
+  __shared__ double ws[32];
+  double s = 0.;
+  for (int64_t i = threadIdx.x; i < n; i += 1024) s += x[i];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(NIDO_FULL_MASK, s, o);
+  if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    s = ws[threadIdx.x];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(NIDO_FULL_MASK, s, o);
+    if (threadIdx.x == 0) *out = scale * s;
+  }
+}
+
+// singleton_partition_kernel (graph_cuda.cu:410-429)
+__global__ void k_singleton(int64_t nv, const double* __restrict__ k, int32_t* __restrict__ comm,
+                            int32_t* __restrict__ newc, double* __restrict__ a) {
+  for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < nv;
+       v += (int64_t)gridDim.x * blockDim.x) {
+    comm[v] = (int32_t)v;
+    newc[v] = (int32_t)v;
+    a[v] = k[v];
+  }
+}
+
+// compute_community_weights_kernel (graph_cuda.cu:370-390)
+__global__ void k_comm_weights(int64_t nv, const int32_t* __restrict__ comm,
+                               const double* __restrict__ k, double* __restrict__ a) {
+  for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < nv;
+       v += (int64_t)gridDim.x * blockDim.x)
+    atomicAdd(&a[comm[v]], k[v]);
+}
+
+// update_community_weights_kernel + exchange_vector_kernel fused
+// (graph_cuda.cu:1234-1250, 1191-1196): movers subtract k_v from the old
+// community and add it to the new one; then ids swap so newc keeps the old
+// id for restore_community.
+__global__ void k_commit(int64_t v0, int64_t v1, const double* __restrict__ k,
+                         int32_t* __restrict__ comm, int32_t* __restrict__ newc,
+                         double* __restrict__ a, int64_t* __restrict__ moved) {
+  int64_t cnt = 0;
+  for (int64_t v = v0 + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < v1;
+       v += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t src = comm[v], dst = newc[v];
+    if (src != dst) {
+      const double kv = k[v];
+      atomicAdd(&a[src], -kv);
+      atomicAdd(&a[dst], kv);
+      ++cnt;
+    }
+    comm[v] = dst;
+    newc[v] = src;
+  }
+  if (moved) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) cnt += __shfl_down_sync(NIDO_FULL_MASK, cnt, o);
+    if ((threadIdx.x & 31) == 0 && cnt) atomicAdd((unsigned long long*)moved, (unsigned long long)cnt);
+  }
+}
+
+// ---- modularity -------------------------------------------------------------------
+// Stage 1: per-vertex in-community weight (self-loops included), one group of
+// G lanes per vertex; lane l sums edges l, l+G, ... then a fixed tree.
+template <int G>
+__global__ void k_q_self_group(const int32_t* __restrict__ list, int64_t n,
+                               const int64_t* __restrict__ off, const int32_t* __restrict__ adj,
+                               const double* __restrict__ w, const int32_t* __restrict__ comm,
+                               double* __restrict__ selfv) {
+  constexpr int VPW = 32 / G;
+  const int lane = threadIdx.x & 31, gl = lane & (G - 1), gid = lane / G;
+  const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t b = warp * VPW; b < n; b += nw * VPW) {
+    const int64_t idx = b + gid;
+    double x = 0.;
+    int v = 0;
+    if (idx < n) {
+      v = list[idx];
+      const int32_t own = comm[v];
+      const int64_t e = off[v + 1];
+      for (int64_t j = off[v] + gl; j < e; j += G)
+        if (comm[adj[j]] == own) x += w[j];
+    }
+#pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1) x += __shfl_down_sync(NIDO_FULL_MASK, x, o, G);
+    if (gl == 0 && idx < n) selfv[v] = x;
+  }
+}
+
+template <int T>
+__global__ void __launch_bounds__(T) k_q_self_cta(const int32_t* __restrict__ list, int64_t n,
+                                                  const int64_t* __restrict__ off,
+                                                  const int32_t* __restrict__ adj,
+                                                  const double* __restrict__ w,
+                                                  const int32_t* __restrict__ comm,
+                                                  double* __restrict__ selfv) {
+  __shared__ double ws[T / 32];
+  for (int64_t idx = blockIdx.x; idx < n; idx += gridDim.x) {
+    const int v = list[idx];
+    const int32_t own = comm[v];
+    const int64_t e = off[v + 1];
+    double x = 0.;
+    for (int64_t j = off[v] + threadIdx.x; j < e; j += T)
+      if (comm[adj[j]] == own) x += w[j];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(NIDO_FULL_MASK, x, o);
+    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = x;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double s = 0.;
+      for (int i = 0; i < T / 32; ++i) s += ws[i];
+      selfv[v] = s;
+    }
+    __syncthreads();
+  }
+}
+
+// Stage 2: the reference's thread slots and 16-lane groups
+// (compute_modularity_reduce_kernel<128,16>, graph_cuda.cu:2096-2134, grid
+// min(ceil(nv/8), 65535)): slot t takes vertices t, t+S, ...; ac folds
+// fma(a_v, a_v, ac) as nvcc contracts "ac += w*w"; lane 0 of each group
+// writes self/(2m) - ac/(4m*m).
+__global__ void k_q_groups(int64_t nv, int64_t S, int64_t ngroups, const double* __restrict__ selfv,
+                           const double* __restrict__ a, const double* __restrict__ dm,
+                           double* __restrict__ modv) {
+  const int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  const int64_t g = t >> 4;
+  double s = 0., ac = 0.;
+  if (g < ngroups) {
+    for (int64_t v = t; v < nv; v += S) {
+      s += selfv[v];
+      ac = fma(a[v], a[v], ac);
+    }
+  }
+#pragma unroll
+  for (int o = 8; o > 0; o >>= 1) {
+    s += __shfl_down_sync(NIDO_FULL_MASK, s, o, 16);
+    ac += __shfl_down_sync(NIDO_FULL_MASK, ac, o, 16);
+  }
+  if ((t & 15) == 0 && g < ngroups) {
+    const double m = dm[0];
+    double x = __ddiv_rn(s, __dmul_rn(2., m));
+    x = __dsub_rn(x, __ddiv_rn(ac, __dmul_rn(__dmul_rn(4., m), m)));
+    modv[g] = __dadd_rn(0., x);
+  }
+}
+
+// Batch cuts of partition_graph_edge_batch (graph_gpu.cpp:303-339) on one
+// thread, with a binary search per cut instead of the linear scan.
+__global__ void k_batch_cuts(const int64_t* __restrict__ off, int64_t nv, int nb,
+                             int64_t* __restrict__ cuts, int64_t* __restrict__ parts) {
+  if (threadIdx.x != 0 || blockIdx.x != 0) return;
+  const int64_t ave = (off[nv] - off[0]) / nb;
+  int np = 0;
+  parts[np++] = 0;
+  int64_t start = 0;
+  while (np <= nb + 1) {
+    // first i in (start, nv] with off[i] - off[start] > ave
+    const int64_t target = off[start] + ave;
+    int64_t lo = start + 1, hi = nv + 1;
+    while (lo < hi) {
+      const int64_t mid = lo + (hi - lo) / 2;
+      if (off[mid] > target) hi = mid; else lo = mid + 1;
+    }
+    if (lo <= nv) {
+      parts[np++] = lo;
+      start = lo;
+      if (lo == nv) break;
+    } else {
+      parts[np++] = nv;
+      break;
+    }
+  }
+  if (np > nb + 1) {
+    const int64_t nnv = (nv - parts[nb]) / nb;
+    for (int i = 1; i < nb; ++i) parts[i] += nnv;
+    parts[nb] = nv;
+  } else {
+    while (np < nb + 1) parts[np++] = nv;
+  }
+  for (int i = 0; i <= nb; ++i) cuts[i] = parts[i];
+}
+
+__device__ __forceinline__ int tier_of(int64_t d, int warp_max, int cta_max) {
+  if (d <= 4) return kTierG4;
+  if (d <= 8) return kTierG8;
+  if (d <= 16) return kTierG16;
+  if (d <= 32) return kTierG32;
+  if (d <= warp_max) return kTierWarp;
+  if (d <= cta_max) return kTierCta;
+  return kTierGlobal;
+}
+
+// key = tier * nb + batch, so every (tier, batch) range and every tier over
+// all batches is contiguous after the stable sort.
+__global__ void k_tier_keys(const int64_t* __restrict__ off, int64_t nv, const int64_t* __restrict__ cuts,
+                            int nb, int warp_max, int cta_max, uint32_t* __restrict__ keys,
+                            uint32_t* __restrict__ vals, int64_t* __restrict__ counts,
+                            unsigned long long* __restrict__ maxdeg) {
+  for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < nv;
+       v += (int64_t)gridDim.x * blockDim.x) {
+    int lo = 0, hi = nb;  // batch b with cuts[b] <= v < cuts[b+1]
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) / 2;
+      if (cuts[mid] <= v) lo = mid; else hi = mid;
+    }
+    const int64_t d = off[v + 1] - off[v];
+    const uint32_t key = (uint32_t)(tier_of(d, warp_max, cta_max) * nb + lo);
+    keys[v] = key;
+    vals[v] = (uint32_t)v;
+    atomicAdd((unsigned long long*)&counts[key], 1ull);
+    atomicMax(maxdeg, (unsigned long long)d);
+  }
+}
+
+}  // namespace
+
+int launch_vertex_weights(nido_graph_s* g) {
+  if (g->nv == 0) return NIDO_OK;
+  k_vertex_weights<<<grid_for(g->nv * 32, kThreads, 148 * 64), kThreads, 0, g->ctx->stream>>>(
+      g->off, g->w, g->nv, g->k);
+  NIDO_LAUNCH_CHECK();
+  return NIDO_OK;
+}
+
+int launch_mass(nido_graph_s* g) {
+  Arena ar(g->scratch, g->scratch_bytes);
+  double* part = ar.take<double>(4096);
+  if (!part) return nido_set_error(NIDO_E_NOMEM, "scratch arena too small (mass)");
+  k_mass_blocks<<<4096, 32, 0, g->ctx->stream>>>(g->k, g->nv, part);
+  NIDO_LAUNCH_CHECK();
+  k_reduce_1024<<<1, 1024, 0, g->ctx->stream>>>(part, 4096, 0.5, g->dm);
+  NIDO_LAUNCH_CHECK();
+  NIDO_CUDA_TRY(cudaMemcpyAsync(&g->m, g->dm, sizeof(double), cudaMemcpyDeviceToHost, g->ctx->stream));
+  NIDO_CUDA_TRY(cudaStreamSynchronize(g->ctx->stream));
+  return NIDO_OK;
+}
+
+int launch_singleton(nido_graph_s* g) {
+  if (g->nv == 0) return NIDO_OK;
+  k_singleton<<<grid_for(g->nv, kThreads), kThreads, 0, g->ctx->stream>>>(g->nv, g->k, g->comm,
+                                                                          g->newc, g->a);
+  NIDO_LAUNCH_CHECK();
+  return NIDO_OK;
+}
+
+int launch_set_comm(nido_graph_s* g) {
+  NIDO_CUDA_TRY(cudaMemsetAsync(g->a, 0, sizeof(double) * g->nv, g->ctx->stream));
+  if (g->nv == 0) return NIDO_OK;
+  k_comm_weights<<<grid_for(g->nv, kThreads), kThreads, 0, g->ctx->stream>>>(g->nv, g->comm, g->k, g->a);
+  NIDO_LAUNCH_CHECK();
+  return NIDO_OK;
+}
+
+int launch_commit(nido_graph_s* g, int64_t v0, int64_t v1) {
+  if (v1 <= v0) return NIDO_OK;
+  k_commit<<<grid_for(v1 - v0, kThreads), kThreads, 0, g->ctx->stream>>>(v0, v1, g->k, g->comm,
+                                                                         g->newc, g->a, nullptr);
+  NIDO_LAUNCH_CHECK();
+  return NIDO_OK;
+}
+
+int launch_modularity(nido_graph_s* g, double* q) {
+  cudaStream_t s = g->ctx->stream;
+  const int64_t nv = g->nv;
+  if (nv == 0) { *q = 0.; return NIDO_OK; }
+  if (!g->bins_valid) NIDO_TRY(build_batches(g));
+  Arena ar(g->scratch, g->scratch_bytes);
+  double* selfv = ar.take<double>(nv);
+  int64_t grid = (nv + 7) / 8;
+  if (grid > 65535) grid = 65535;
+  const int64_t S = 128 * grid;
+  const int64_t nslots = std::min<int64_t>(S, nv);
+  const int64_t ngroups = (nslots + 15) / 16;
+  double* modv = ar.take<double>(ngroups);
+  if (!selfv || !modv) return nido_set_error(NIDO_E_NOMEM, "scratch arena too small (modularity)");
+  const int nb = g->nbatches;
+  for (int t = 0; t < kNumTiers; ++t) {
+    const int64_t b0 = g->tier_off[(size_t)t * nb], b1 = g->tier_off[(size_t)(t + 1) * nb];
+    const int64_t n = b1 - b0;
+    if (n == 0) continue;
+    const int32_t* list = g->perm + b0;
+    switch (t) {
+      case kTierG4:
+        k_q_self_group<4><<<grid_for(n, kThreads / 4 * 8), kThreads, 0, s>>>(list, n, g->off, g->adj, g->w, g->comm, selfv);
+        break;
+      case kTierG8:
+        k_q_self_group<8><<<grid_for(n, kThreads / 8 * 4), kThreads, 0, s>>>(list, n, g->off, g->adj, g->w, g->comm, selfv);
+        break;
+      case kTierG16:
+        k_q_self_group<16><<<grid_for(n, kThreads / 16 * 2), kThreads, 0, s>>>(list, n, g->off, g->adj, g->w, g->comm, selfv);
+        break;
+      case kTierG32:
+      case kTierWarp:
+        k_q_self_group<32><<<grid_for(n, kThreads / 32), kThreads, 0, s>>>(list, n, g->off, g->adj, g->w, g->comm, selfv);
+        break;
+      default:
+        k_q_self_cta<512><<<grid_for(n, 1, 148 * 4), 512, 0, s>>>(list, n, g->off, g->adj, g->w, g->comm, selfv);
+        break;
+    }
+    NIDO_LAUNCH_CHECK();
+  }
+  const int64_t threads = ngroups * 16;
+  k_q_groups<<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(nv, S, ngroups, selfv, g->a, g->dm, modv);
+  NIDO_LAUNCH_CHECK();
+  k_reduce_1024<<<1, 1024, 0, s>>>(modv, ngroups, 1.0, g->dm + 1);
+  NIDO_LAUNCH_CHECK();
+  NIDO_CUDA_TRY(cudaMemcpyAsync(q, g->dm + 1, sizeof(double), cudaMemcpyDeviceToHost, s));
+  NIDO_CUDA_TRY(cudaStreamSynchronize(s));
+  return NIDO_OK;
+}
+
+int build_batches(nido_graph_s* g) {
+  cudaStream_t s = g->ctx->stream;
+  const int nb = g->nbatches;
+  const int64_t nv = g->nv;
+  Arena ar(g->scratch, g->scratch_bytes);
+  int64_t* dcuts = ar.take<int64_t>(nb + 1);
+  int64_t* dparts = ar.take<int64_t>(nb + 2);
+  const int64_t nkeys = (int64_t)kNumTiers * nb;
+  int64_t* counts = ar.take<int64_t>(nkeys + 1);
+  unsigned long long* maxdeg = ar.take<unsigned long long>(1);
+  uint32_t* keys = ar.take<uint32_t>(nv);
+  uint32_t* keys2 = ar.take<uint32_t>(nv);
+  uint32_t* vals2 = ar.take<uint32_t>(nv);
+  int64_t* rtemp = ar.take<int64_t>(std::max(radix_temp_elems(nv), scan_temp_elems(nkeys)));
+  if (!rtemp) return nido_set_error(NIDO_E_NOMEM, "scratch arena too small (batches)");
+  k_batch_cuts<<<1, 1, 0, s>>>(g->off, nv, nb, dcuts, dparts);
+  NIDO_LAUNCH_CHECK();
+  NIDO_CUDA_TRY(cudaMemsetAsync(counts, 0, sizeof(int64_t) * (nkeys + 1), s));
+  NIDO_CUDA_TRY(cudaMemsetAsync(maxdeg, 0, sizeof(unsigned long long), s));
+  if (nv > 0) {
+    k_tier_keys<<<grid_for(nv, kThreads), kThreads, 0, s>>>(g->off, nv, dcuts, nb, g->ctx->tiers.warp_max,
+                                                           g->ctx->tiers.cta_max, keys, (uint32_t*)g->perm,
+                                                           counts, maxdeg);
+    NIDO_LAUNCH_CHECK();
+    int bits = 0;
+    while (((int64_t)1 << bits) < nkeys) ++bits;
+    NIDO_TRY(radix_sort_pairs(keys, (uint32_t*)g->perm, keys2, vals2, nv, bits, rtemp, s));
+  }
+  NIDO_TRY(scan_exclusive_i64(counts, counts, nkeys, rtemp, s));
+  g->cuts.assign(nb + 1, 0);
+  g->tier_off.assign(nkeys + 1, 0);
+  unsigned long long md = 0;
+  NIDO_CUDA_TRY(cudaMemcpyAsync(g->cuts.data(), dcuts, sizeof(int64_t) * (nb + 1), cudaMemcpyDeviceToHost, s));
+  NIDO_CUDA_TRY(cudaMemcpyAsync(g->tier_off.data(), counts, sizeof(int64_t) * (nkeys + 1), cudaMemcpyDeviceToHost, s));
+  NIDO_CUDA_TRY(cudaMemcpyAsync(&md, maxdeg, sizeof(md), cudaMemcpyDeviceToHost, s));
+  NIDO_CUDA_TRY(cudaStreamSynchronize(s));
+  g->max_degree = (int64_t)md;
+  g->bins_valid = true;
+  return NIDO_OK;
+}
+
+}  // namespace nido
