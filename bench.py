@@ -1,0 +1,340 @@
+#!/usr/bin/env python
+"""Benchmark: whole Louvain runs on one B200 per rank, nido's options.
+
+Default workload (one GPU): "Plain Louvain drop-in on one R-MAT graph":
+R-MAT scale 22 (4,194,304 vertices), edge factor 16, (a,b,c,d) =
+(0.57,0.19,0.19,0.05), symmetrised, self-loops and duplicates removed, weights
+1.0, seed 2, nido defaults -b 2 -t 1e-6 -i 500.  A step is one whole Louvain
+run (all phases, coarsening included) from the graph resident in HBM.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                  [--workload rmat22|planted|sbm]
+
+Prints one JSON line.  `value` is graphs/s over all ranks from CUDA events on
+the engine's stream; `e2e` is the same metric through the public C ABI with
+host buffers (pinned H2D upload of the CSR, run, D2H of the partition inside
+the timed region).  `roofline` covers the move phase (all degree-tier kernels
+of a sweep): algorithmic bytes 16*E + 32*V per sweep (int32 ids, FP64
+weights) over the CUDA-event time of the move kernels.  For N > 1 the ranks
+are independent replicas (no collective on the data path).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+PEAKS_FALLBACK = {"hbm_gbs": 6650.0}
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f), "measured"
+    except OSError:
+        return PEAKS_FALLBACK, "fallback"
+
+
+WORKLOADS = {
+    "rmat22": dict(desc="R-MAT scale 22 (4,194,304 vertices), edge factor 16, (0.57,0.19,0.19,0.05), "
+                        "symmetrised, self-loops and duplicates removed, weights 1.0, seed 2",
+                   nbatches=2, tau=1e-6),
+    "rmat20": dict(desc="R-MAT scale 20 (1,048,576 vertices), edge factor 16, (0.57,0.19,0.19,0.05), "
+                        "symmetrised, self-loops and duplicates removed, weights 1.0, seed 2 (profiling case)",
+                   nbatches=2, tau=1e-6),
+    "planted": dict(desc="planted partition 65,536 vertices (256 blocks of 256), average degree 32, 80% intra, "
+                         "weights U[0.5,1.5], duplicates summed, seed 1", nbatches=1, tau=1e-6),
+    "sbm": dict(desc="SBM 16,777,216 vertices, power-law community sizes (2.5, 16..65,536), average degree 32, "
+                     "70% intra, lognormal(0,0.5) weights, seed 3", nbatches=32, tau=1e-6),
+}
+
+
+def make_graph(capi, name):
+    if name == "rmat22":
+        return capi.gen_rmat(1 << 22, 16 << 22, wmode=capi.W_ONE, seed=2)
+    if name == "rmat20":
+        return capi.gen_rmat(1 << 20, 16 << 20, wmode=capi.W_ONE, seed=2)
+    if name == "planted":
+        return capi.gen_planted(256, 256, 32.0, 0.8, capi.W_UNIFORM, 1)
+    if name == "sbm":
+        return capi.gen_sbm(1 << 24, 2.5, 16, 65536, 32.0, 0.7, capi.W_LOGNORMAL, True, 3)
+    raise SystemExit(f"unknown workload {name}")
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            out, _ = self.proc.communicate(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+            out, _ = self.proc.communicate()
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in out.strip().splitlines():
+            p = [x.strip() for x in line.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                mx = float(p[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, p[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": mx, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def reduce_max(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+SMALL_GRAPH_EDGES = 8_000_000  # whole CPU runs are timed directly below this size
+
+
+def cpu_baseline_sample(G, wl, threads):
+    """The CPU oracle (a port of the reference's algorithm, all host threads)
+    on the same graph.  Small graphs: one whole run.  Large graphs: the first
+    Louvain phase capped at 3 iterations, without coarsening; returns the
+    time and the edges it visited (one modularity sweep before the loop, then
+    one move and one modularity sweep per iteration)."""
+    from oracle import oracle as orc
+    small = G.ne <= SMALL_GRAPH_EDGES
+    t0 = time.perf_counter()
+    _, st = orc.louvain(G.off, G.adj, G.w, nbatches=wl["nbatches"], tau=wl["tau"],
+                        max_loops=500 if small else 3, max_phases=200 if small else 1)
+    el = time.perf_counter() - t0
+    scanned = 0.0
+    for p in range(st.phases):
+        scanned += st.ne_phase[p] * (1 + 2 * st.loops_phase[p])
+    return el, scanned, st, small
+
+
+def run_ours(args, world, rank, local):
+    import torch
+
+    from nido_b200 import capi
+    wl = WORKLOADS[args.workload]
+    torch.cuda.set_device(local)
+    G = make_graph(capi, args.workload)
+    ctx = capi.Context(local)
+    stream = torch.cuda.ExternalStream(ctx.stream())
+    g = capi.Graph(ctx, G, wl["nbatches"])
+    for _ in range(args.warmup):
+        g.run(tau=wl["tau"])
+    barrier(world)
+    torch.cuda.synchronize()
+    ctx.sync()
+    sampler = ClockSampler(local)
+    sampler.start()
+    l0 = capi.lib().nido_launch_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    stats = [g.run(tau=wl["tau"])[1] for _ in range(args.steps)]
+    e1.record(stream)
+    ctx.sync()
+    torch.cuda.synchronize()
+    launches = int(capi.lib().nido_launch_count() - l0)
+    ms = e0.elapsed_time(e1)
+    clocks = sampler.stop()
+    barrier(world)
+    ms_max = reduce_max(ms, world)
+    move_ms = sum(s.move_ms for s in stats)
+    move_bytes = sum(s.move_bytes for s in stats)
+    sweeps = sum(s.total_loops for s in stats)
+    edges_per_run = stats[0].edges_scanned
+    final_q = stats[-1].final_q
+
+    # end to end through the C ABI: pinned host CSR -> upload -> run -> partition
+    for a in (G.off, G.adj, G.w):
+        capi.host_register(a)
+    g.close()
+    h2d = G.off.nbytes + G.adj.nbytes + G.w.nbytes
+    d2h = 8 * G.nv
+    barrier(world)
+    torch.cuda.synchronize()
+    ctx.sync()
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    for _ in range(args.steps):
+        with capi.Graph(ctx, G, wl["nbatches"]) as g2:
+            part, _ = g2.run(tau=wl["tau"])
+    f1.record(stream)
+    ctx.sync()
+    torch.cuda.synchronize()
+    e2e_ms = reduce_max(f0.elapsed_time(f1), world)
+    for a in (G.off, G.adj, G.w):
+        capi.host_unregister(a)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        el, scanned, st, small = cpu_baseline_sample(G, wl, threads)
+        if small:
+            cpu = {"value": 1.0 / el, "unit": "graphs/s", "cores": threads, "kind": "port",
+                   "sample": f"CPU oracle (port of the reference's algorithm), one whole run, {el:.2f} s"}
+        else:
+            run_s = el * edges_per_run / scanned
+            cpu = {"value": 1.0 / run_s, "unit": "graphs/s", "cores": threads, "kind": "port",
+                   "sample": f"CPU oracle (port of the reference's algorithm): first phase, {st.total_loops} "
+                             f"iterations, no coarsening ({el:.1f} s, {scanned:.3g} edges visited), scaled to a "
+                             f"whole run by edges visited ({edges_per_run:.3g} per run, from the GPU run)"}
+    ctx.close()
+    if rank != 0:
+        return None
+    pk, pk_kind = peaks()
+    achieved = move_bytes / (move_ms * 1e-3) / 1e9 if move_ms > 0 else 0.0
+    sec = ms_max * 1e-3
+    return {
+        "metric": "graphs/s", "value": world * args.steps / sec, "unit": "graphs/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "impl": "ours",
+        "config": {"workload": args.workload, "graph": wl["desc"], "nv": G.nv, "ne": G.ne,
+                   "nbatches": wl["nbatches"], "tau": wl["tau"], "ids": "int32 on device",
+                   "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (CSR 12 B/edge)"},
+        "edges_scanned_per_s": world * edges_per_run * args.steps / sec,
+        "move_sweeps_per_run": sweeps / args.steps, "final_q": final_q,
+        "e2e": {"value": world * args.steps / (e2e_ms * 1e-3), "unit": "graphs/s",
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
+                     "frac": achieved / pk["hbm_gbs"], "traffic": None,
+                     "kernel": "move phase (degree-tier kernels of one sweep)",
+                     "peak_kind": pk_kind},
+        "cpu_baseline": cpu,
+        "clocks": clocks,
+        "gpu_launches": launches,
+    }
+
+
+def run_reference(args, world, rank):
+    """The reference's path on the host cores: the CPU oracle (a port of nido's
+    algorithm; nido itself has no CPU implementation), all threads, each step
+    a bounded sample scaled to a whole run."""
+    if rank != 0:
+        return None
+    from nido_b200 import capi
+    from oracle import oracle as orc
+    wl = WORKLOADS[args.workload]
+    G = make_graph(capi, args.workload)
+    threads = os.cpu_count() or 1
+    # warm-up 1: one whole run fixes the edges a run visits (the oracle's
+    # trajectory is the engine's, bit for bit on integer weights)
+    t0 = time.perf_counter()
+    _, full = orc.louvain(G.off, G.adj, G.w, nbatches=wl["nbatches"], tau=wl["tau"])
+    full_s = time.perf_counter() - t0
+    edges_per_run = sum(full.ne_phase[p] * (1 + 2 * full.loops_phase[p]) for p in range(full.phases))
+    samples = []
+    small = False
+    for i in range(args.warmup - 1 + args.steps):
+        el, scanned, st, small = cpu_baseline_sample(G, wl, threads)
+        if i >= args.warmup - 1:
+            samples.append((el, scanned))
+    el = sum(s[0] for s in samples)
+    scanned = sum(s[1] for s in samples)
+    if small:
+        value = len(samples) / el
+        sample = f"CPU oracle (port of the reference's algorithm), {threads} threads, one whole run per step"
+    else:
+        value = scanned / el / edges_per_run
+        sample = (f"CPU oracle (port of the reference's algorithm), {threads} threads; each step the first "
+                  f"Louvain phase capped at 3 iterations without coarsening, scaled by the {edges_per_run:.4g} "
+                  f"edges a whole run visits; one whole run took {full_s:.1f} s")
+    return {
+        "metric": "graphs/s", "value": value, "unit": "graphs/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 / value, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+        "config": {"workload": args.workload, "graph": wl["desc"], "nv": G.nv, "ne": G.ne,
+                   "nbatches": wl["nbatches"], "tau": wl["tau"]},
+        "cpu_baseline": {"value": value, "unit": "graphs/s", "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": "graphs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "full_run_s": full_s, "full_run_q": full.final_q,
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="rmat22")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        raise SystemExit("--warmup must be at least 3")
+    world, rank, local = dist_setup(args)
+    if args.impl == "reference":
+        out = run_reference(args, world, rank)
+    else:
+        out = run_ours(args, world, rank, local)
+    if out is not None:
+        print(json.dumps(out), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -82,6 +82,8 @@ typedef struct {
 /* ---- library ---------------------------------------------------------------- */
 const char* nido_last_error(void);
 const char* nido_version(void);
+/* number of kernels this library has launched in the process (all contexts) */
+uint64_t nido_launch_count(void);
 
 /* ---- context: one CUDA device + one stream; one per host thread ----------- */
 /* Replaces GraphGPU's per-device setup (graph_gpu.cpp:33-100). */
@@ -108,6 +110,16 @@ int nido_graph_download(nido_graph g, int64_t* off, int64_t* adj, double* w);
 int nido_graph_batches(nido_graph g, int64_t* cuts);
 /* k_v (vertexWeights_) and m (mass_) of the current graph */
 int nido_graph_vertex_weights(nido_graph g, double* k, double* m);
+/* Return to the uploaded graph (undo coarsening) with a singleton partition,
+ * from the device-resident original CSR.  The reference has no counterpart:
+ * it re-reads and re-uploads the file (graph_gpu.cpp:19-185). */
+int nido_graph_reset(nido_graph g);
+
+/* Page-lock a caller's host buffer so uploads and downloads run at full
+ * link bandwidth (cudaHostRegister); the reference uses pinned buffers via
+ * CudaMallocHost (cuda_wrapper.hpp:22-25). */
+int nido_host_register(void* ptr, size_t bytes);
+int nido_host_unregister(void* ptr);
 
 /* ---- step-level operators: GraphGPU's public methods (graph_gpu.hpp:172-241) */
 int nido_singleton_partition(nido_graph g);                  /* graph_gpu.cpp:519-536 */
@@ -129,7 +141,8 @@ int nido_get_clustering(nido_graph g, int64_t* clustering);
 int nido_dump_partition(nido_graph g, const char* path, const int64_t* new_orders);
 
 /* ---- whole run: LouvainGPU::run (louvain_gpu.cpp:6-139) ------------------------ */
-/* out_comm (nv entries, may be NULL) receives the clustering of the original
+/* Starts from the uploaded graph (any earlier coarsening is undone first).
+ * out_comm (nv entries, may be NULL) receives the clustering of the original
  * vertices; stats may be NULL. */
 int nido_run(nido_graph g, const nido_params* p, int64_t* out_comm, nido_run_stats* stats);
 

@@ -63,6 +63,7 @@ def lib() -> C.CDLL:
         sig = {
             "nido_last_error": (C.c_char_p, []),
             "nido_version": (C.c_char_p, []),
+            "nido_launch_count": (C.c_uint64, []),
             "nido_ctx_create": (C.c_int, [C.c_int, C.c_size_t, C.POINTER(vp)]),
             "nido_ctx_destroy": (C.c_int, [vp]),
             "nido_ctx_sync": (C.c_int, [vp]),
@@ -74,6 +75,9 @@ def lib() -> C.CDLL:
             "nido_graph_download": (C.c_int, [vp, _i64p, _i64p, _f64p]),
             "nido_graph_batches": (C.c_int, [vp, _i64p]),
             "nido_graph_vertex_weights": (C.c_int, [vp, _f64p, _f64p]),
+            "nido_graph_reset": (C.c_int, [vp]),
+            "nido_host_register": (C.c_int, [vp, C.c_size_t]),
+            "nido_host_unregister": (C.c_int, [vp]),
             "nido_singleton_partition": (C.c_int, [vp]),
             "nido_set_community_ids": (C.c_int, [vp, _i64p]),
             "nido_compute_modularity": (C.c_int, [vp, _f64p]),
@@ -171,6 +175,15 @@ def gen_sbm(nv, alpha=2.5, cmin=16, cmax=65536, avg_degree=32.0, p_intra=0.7, wm
     _check(lib().nido_gen_sbm(nv, alpha, cmin, cmax, avg_degree, p_intra, wmode, int(permute), seed,
                               C.byref(s)))
     return _take(s)
+
+
+def host_register(a: np.ndarray):
+    """Page-lock a numpy array's memory (cudaHostRegister)."""
+    _check(lib().nido_host_register(a.ctypes.data, a.nbytes))
+
+
+def host_unregister(a: np.ndarray):
+    _check(lib().nido_host_unregister(a.ctypes.data))
 
 
 def read_vite(path: str) -> Csr:
@@ -278,6 +291,9 @@ class Graph:
         m = C.c_double()
         _check(lib().nido_graph_vertex_weights(self.h, _pf(k), C.byref(m)))
         return k, m.value
+
+    def reset(self):
+        _check(lib().nido_graph_reset(self.h))
 
     def singleton_partition(self):
         _check(lib().nido_singleton_partition(self.h))

@@ -429,16 +429,21 @@ int launch_aggregation(nido_graph_s* g, int* done) {
     NIDO_CUDA_TRY(cudaFreeAsync(gf, s));
     NIDO_CUDA_TRY(cudaFreeAsync(gvv, s));
   }
-  // coarse offsets into off2, then entries into adj/w (the old lists are dead)
+  // coarse offsets into off2, then the entries into the work CSR (when the
+  // current graph is the work CSR, its lists are dead once pass 1 is done)
   NIDO_TRY(scan_exclusive_i64(degp, g->off2, nvp, temp, s));
-  k_compact<<<grid_for(nvp * 32, 256, kSMs * 16), 256, 0, s>>>(nvp, mo, medge, g->off2, g->adj2, g->w2, g->adj, g->w);
+  k_compact<<<grid_for(nvp * 32, 256, kSMs * 16), 256, 0, s>>>(nvp, mo, medge, g->off2, g->adj2, g->w2, g->adjA, g->wA);
   NIDO_LAUNCH_CHECK();
   int64_t nep = 0, nerr = 0;
   NIDO_CUDA_TRY(cudaMemcpyAsync(&nep, g->off2 + nvp, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
   NIDO_CUDA_TRY(cudaMemcpyAsync(&nerr, g->dcount + 1, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
   NIDO_CUDA_TRY(cudaStreamSynchronize(s));
   if (nerr) return nido_set_error(NIDO_E_CUDA, "hash table overflow in %lld probes", (long long)nerr);
-  std::swap(g->off, g->off2);
+  std::swap(g->offA, g->off2);
+  g->off = g->offA;
+  g->adj = g->adjA;
+  g->w = g->wA;
+  g->coarsened = true;
   g->nv = nvp;
   g->ne = nep;
   g->bins_valid = false;

@@ -26,8 +26,14 @@
     if (s_ != NIDO_OK) return s_; \
   } while (0)
 
-// launch check: reports the launch error (bad configuration) without a sync
-#define NIDO_LAUNCH_CHECK() NIDO_CUDA_TRY(cudaPeekAtLastError())
+// Follows every kernel launch: counts it and reports a launch error (bad
+// configuration) without a sync.
+extern "C" void nido_count_launch(void);
+#define NIDO_LAUNCH_CHECK()                     \
+  do {                                          \
+    nido_count_launch();                        \
+    NIDO_CUDA_TRY(cudaPeekAtLastError());       \
+  } while (0)
 
 namespace nido {
 

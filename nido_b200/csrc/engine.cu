@@ -179,9 +179,10 @@ extern "C" int nido_graph_free(nido_graph g) {
   cudaSetDevice(ctx->device);
   cudaStreamSynchronize(ctx->stream);
   const int64_t V = g->cap_v, E = g->cap_e;
-  dev_free(ctx, g->off, 8 * (V + 1)); dev_free(ctx, g->off2, 8 * (V + 1));
-  dev_free(ctx, g->adj, 4 * E); dev_free(ctx, g->adj2, 4 * E);
-  dev_free(ctx, g->w, 8 * E); dev_free(ctx, g->w2, 8 * E);
+  dev_free(ctx, g->off0, 8 * (V + 1)); dev_free(ctx, g->offA, 8 * (V + 1));
+  dev_free(ctx, g->off2, 8 * (V + 1));
+  dev_free(ctx, g->adj0, 4 * E); dev_free(ctx, g->adjA, 4 * E); dev_free(ctx, g->adj2, 4 * E);
+  dev_free(ctx, g->w0, 8 * E); dev_free(ctx, g->wA, 8 * E); dev_free(ctx, g->w2, 8 * E);
   dev_free(ctx, g->k, 8 * V); dev_free(ctx, g->a, 8 * V);
   dev_free(ctx, g->comm, 4 * V); dev_free(ctx, g->newc, 4 * V);
   dev_free(ctx, g->clus, 4 * g->nv0); dev_free(ctx, g->perm, 4 * V);
@@ -208,14 +209,14 @@ extern "C" int nido_graph_upload(nido_ctx ctx, int64_t nv, int64_t ne, const int
   if (!g) return nido_set_error(NIDO_E_NOMEM, "host allocation failed");
   g->ctx = ctx;
   g->nv0 = g->nv = g->cap_v = nv;
-  g->ne = g->cap_e = ne;
+  g->ne = g->ne0 = g->cap_e = ne;
   g->nbatches = nbatches;
   const int64_t V = nv, E = ne;
   int st = NIDO_OK;
 #define ALLOC(p, n) if (st == NIDO_OK) st = dev_alloc(ctx, &g->p, (n))
-  ALLOC(off, V + 1); ALLOC(off2, V + 1);
-  ALLOC(adj, E); ALLOC(adj2, E);
-  ALLOC(w, E); ALLOC(w2, E);
+  ALLOC(off0, V + 1); ALLOC(offA, V + 1); ALLOC(off2, V + 1);
+  ALLOC(adj0, E); ALLOC(adjA, E); ALLOC(adj2, E);
+  ALLOC(w0, E); ALLOC(wA, E); ALLOC(w2, E);
   ALLOC(k, V); ALLOC(a, V);
   ALLOC(comm, V); ALLOC(newc, V);
   ALLOC(clus, V); ALLOC(perm, V);
@@ -226,6 +227,9 @@ extern "C" int nido_graph_upload(nido_ctx ctx, int64_t nv, int64_t ne, const int
                      sizeof(int64_t) * (size_t)(nido::radix_temp_elems(V) + nido::scan_temp_elems(E + 1));
   if (st == NIDO_OK) st = dev_alloc(ctx, &g->scratch, (int64_t)g->scratch_bytes);
   if (st != NIDO_OK) { nido_graph_free(g); return st; }
+  g->off = g->off0;
+  g->adj = g->adj0;
+  g->w = g->w0;
   cudaStream_t s = ctx->stream;
   // int64 ids travel in the (not yet used) w2 buffer and are narrowed on device
   int64_t* adj64 = reinterpret_cast<int64_t*>(g->w2);
@@ -291,6 +295,41 @@ extern "C" int nido_graph_vertex_weights(nido_graph g, double* k, double* m) {
     NIDO_CUDA_TRY(cudaStreamSynchronize(g->ctx->stream));
   }
   if (m) *m = g->m;
+  return NIDO_OK;
+}
+
+namespace {
+int reset_graph(nido_graph g) {
+  cudaStream_t s = g->ctx->stream;
+  k_iota<<<kGrid, 256, 0, s>>>(g->clus, g->nv0);
+  NIDO_LAUNCH_CHECK();
+  if (!g->coarsened) return NIDO_OK;
+  g->off = g->off0;
+  g->adj = g->adj0;
+  g->w = g->w0;
+  g->nv = g->nv0;
+  g->ne = g->ne0;
+  g->coarsened = false;
+  return prepare_phase(g);
+}
+}  // namespace
+
+extern "C" int nido_graph_reset(nido_graph g) {
+  if (!g) return nido_set_error(NIDO_E_INVALID, "null graph");
+  NIDO_CUDA_TRY(cudaSetDevice(g->ctx->device));
+  NIDO_TRY(reset_graph(g));
+  return nido::launch_singleton(g);
+}
+
+extern "C" int nido_host_register(void* ptr, size_t bytes) {
+  if (!ptr || !bytes) return nido_set_error(NIDO_E_INVALID, "nido_host_register: empty range");
+  NIDO_CUDA_TRY(cudaHostRegister(ptr, bytes, cudaHostRegisterDefault));
+  return NIDO_OK;
+}
+
+extern "C" int nido_host_unregister(void* ptr) {
+  if (!ptr) return nido_set_error(NIDO_E_INVALID, "nido_host_unregister: null pointer");
+  NIDO_CUDA_TRY(cudaHostUnregister(ptr));
   return NIDO_OK;
 }
 
@@ -439,6 +478,8 @@ extern "C" int nido_run(nido_graph g, const nido_params* p, int64_t* out_comm, n
   NIDO_CUDA_TRY(cudaEventCreate(&t0));
   NIDO_CUDA_TRY(cudaEventCreate(&t1));
   NIDO_CUDA_TRY(cudaEventRecord(t0, s));
+  // every run starts from the uploaded graph, as on a fresh GraphGPU
+  NIDO_TRY(reset_graph(g));
   const double tau = p->tau;
   bool done = false;
   int64_t phases = 0;

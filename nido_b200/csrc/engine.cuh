@@ -56,9 +56,21 @@ struct nido_graph_s {
   bool int_weights = false;  // every weight integral and total below 2^53
   double m = 0.0;            // host copy of the mass
 
+  int64_t ne0 = 0;           // original edge count
+  bool coarsened = false;    // current CSR is a coarse graph
+  // current CSR (points at the original or at the work buffers)
   int64_t* off = nullptr;
   int32_t* adj = nullptr;
   double* w = nullptr;
+  // original CSR, never modified: runs restart from it without a host copy
+  int64_t* off0 = nullptr;
+  int32_t* adj0 = nullptr;
+  double* w0 = nullptr;
+  // work CSR that holds coarse graphs
+  int64_t* offA = nullptr;
+  int32_t* adjA = nullptr;
+  double* wA = nullptr;
+  // coarsening temporaries (per-coarse-vertex lists before compaction)
   int64_t* off2 = nullptr;
   int32_t* adj2 = nullptr;
   double* w2 = nullptr;

@@ -427,9 +427,23 @@ extern "C" void orc_color_nido_seq(int64_t nv, const int64_t* off, const int64_t
 // ---------------------------------------------------------------------------
 // Whole run: LouvainGPU::run (louvain_gpu.cpp:28-124) over GraphGPU's state,
 // with aggregation (graph_gpu.cpp:1382-1545) and Clustering (clustering.cpp).
+// max_phases below 200 stops early (used to time bounded samples).
+extern "C" int orc_louvain_capped(int64_t nv0, const int64_t* off0, const int64_t* adj0,
+                                  const double* w0, int nbatches, double tau, int64_t max_loops,
+                                  int tie, int verbose, int max_phases, int64_t* clustering,
+                                  orc_stats* st);
+
 extern "C" int orc_louvain(int64_t nv0, const int64_t* off0, const int64_t* adj0,
                            const double* w0, int nbatches, double tau, int64_t max_loops,
                            int tie, int verbose, int64_t* clustering, orc_stats* st) {
+  return orc_louvain_capped(nv0, off0, adj0, w0, nbatches, tau, max_loops, tie, verbose, 200,
+                            clustering, st);
+}
+
+extern "C" int orc_louvain_capped(int64_t nv0, const int64_t* off0, const int64_t* adj0,
+                                  const double* w0, int nbatches, double tau, int64_t max_loops,
+                                  int tie, int verbose, int max_phases, int64_t* clustering,
+                                  orc_stats* st) {
   if (nbatches < 1) return -1;
   memset(st, 0, sizeof(*st));
   std::vector<int64_t> off(off0, off0 + nv0 + 1), adj(adj0, adj0 + off0[nv0]);
@@ -443,7 +457,7 @@ extern "C" int orc_louvain(int64_t nv0, const int64_t* off0, const int64_t* adj0
   orc_batch_cuts(nv, off.data(), nbatches, cuts.data());
   bool done = false;
   int64_t phases = 0;
-  while (!done && phases < 200) {
+  while (!done && phases < 200 && phases < max_phases) {
     if (verbose) printf("PHASE #%lld: \n", (long long)phases);
     orc_singleton(nv, k.data(), comm.data(), newcomm.data(), a.data());
     double Q = orc_modularity(nv, off.data(), adj.data(), w.data(), comm.data(), a.data(), m);
@@ -470,7 +484,7 @@ extern "C" int orc_louvain(int64_t nv0, const int64_t* off0, const int64_t* adj0
     st->total_loops += loops;
     st->final_q = Q;
     if (verbose) printf("Final Q: %.17g\n", Q);
-    if (Q - Q_old > tau) {
+    if (Q - Q_old > tau && phases + 1 < max_phases) {
       std::vector<int64_t> newid(nv);
       int64_t *coff, *cadj, cne;
       double* cw;

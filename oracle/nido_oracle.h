@@ -108,6 +108,10 @@ typedef struct {
 int orc_louvain(int64_t nv, const int64_t* off, const int64_t* adj, const double* w,
                 int nbatches, double tau, int64_t max_loops, int tie, int verbose,
                 int64_t* clustering, orc_stats* st);
+/* the same, stopping after max_phases phases (bounded timing samples) */
+int orc_louvain_capped(int64_t nv, const int64_t* off, const int64_t* adj, const double* w,
+                       int nbatches, double tau, int64_t max_loops, int tie, int verbose,
+                       int max_phases, int64_t* clustering, orc_stats* st);
 
 /* Plain FP64 modularity of a partition of the original graph (any community
  * ids), summed per vertex in CSR order: used to compare final partitions. */

@@ -58,6 +58,8 @@ def lib() -> C.CDLL:
         L.orc_color_nido_seq.argtypes = [C.c_int64, _i64p, _i64p, _i64p]
         L.orc_louvain.argtypes = [C.c_int64, _i64p, _i64p, _f64p, C.c_int, C.c_double, C.c_int64, C.c_int,
                                   C.c_int, _i64p, C.POINTER(Stats)]
+        L.orc_louvain_capped.argtypes = [C.c_int64, _i64p, _i64p, _f64p, C.c_int, C.c_double, C.c_int64,
+                                         C.c_int, C.c_int, C.c_int, _i64p, C.POINTER(Stats)]
         L.orc_partition_modularity.argtypes = [C.c_int64, _i64p, _i64p, _f64p, _i64p]
         L.orc_partition_modularity.restype = C.c_double
         L.orc_nmi.argtypes = [C.c_int64, _i64p, _i64p]
@@ -178,12 +180,13 @@ def color_nido_seq(off, adj):
     return c
 
 
-def louvain(off, adj, w, nbatches=2, tau=1e-6, max_loops=500, tie=TIE_SMALLEST_ID, verbose=False):
+def louvain(off, adj, w, nbatches=2, tau=1e-6, max_loops=500, tie=TIE_SMALLEST_ID, verbose=False,
+            max_phases=200):
     off, adj, w = _i(off), _i(adj), _f(w)
     cl = np.empty(len(off) - 1, np.int64)
     st = Stats()
-    rc = lib().orc_louvain(len(off) - 1, _p(off), _p(adj), _pf(w), nbatches, tau, max_loops, tie, int(verbose),
-                           _p(cl), C.byref(st))
+    rc = lib().orc_louvain_capped(len(off) - 1, _p(off), _p(adj), _pf(w), nbatches, tau, max_loops, tie,
+                                  int(verbose), max_phases, _p(cl), C.byref(st))
     if rc:
         raise ValueError("orc_louvain failed")
     return cl, st
