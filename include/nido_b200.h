@@ -73,6 +73,11 @@ typedef struct {
   double edges_scanned;/* edges visited by move sweeps */
   int64_t move_launches;
   int64_t kernel_launches;
+  /* host wall time per section (ms): [0] restart from the uploaded graph,
+   * [1] enqueueing moves and commits, [2] modularity including the wait for
+   * the device, [3] aggregation, [4] per-phase preparation after
+   * aggregation, [5] download of the clustering */
+  double host_ms[8];
   double q_phase[200];
   int64_t loops_phase[200];
   int64_t nv_phase[200];

@@ -43,7 +43,7 @@ class RunStats(C.Structure):
     _fields_ = [("phases", C.c_int64), ("total_loops", C.c_int64), ("final_q", C.c_double),
                 ("total_ms", C.c_double), ("move_ms", C.c_double), ("move_bytes", C.c_double),
                 ("edges_scanned", C.c_double), ("move_launches", C.c_int64),
-                ("kernel_launches", C.c_int64), ("q_phase", C.c_double * 200),
+                ("kernel_launches", C.c_int64), ("host_ms", C.c_double * 8), ("q_phase", C.c_double * 200),
                 ("loops_phase", C.c_int64 * 200), ("nv_phase", C.c_int64 * 200),
                 ("ne_phase", C.c_int64 * 200)]
 

@@ -88,18 +88,34 @@ __global__ void k_member_bounds(const uint32_t* __restrict__ keys, const uint32_
   }
 }
 
-// tier of each coarse vertex by its member-edge count D
+// tier of each coarse vertex by its member-edge count D (counts aggregated
+// per warp before the global atomics)
 __global__ void k_agg_tiers(const int64_t* __restrict__ mo, const int64_t* __restrict__ medge, int64_t nvp,
                             uint32_t* __restrict__ keys, uint32_t* __restrict__ vals,
-                            int64_t* __restrict__ counts, unsigned long long* __restrict__ maxd) {
-  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c < nvp; c += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t D = medge[mo[c + 1]] - medge[mo[c]];
-    const int64_t U = D < nvp ? D : nvp;
-    const uint32_t t = D <= kAggWarpMaxD ? 0u : (2 * U <= kAggCtaMaxCap ? 1u : 2u);
-    keys[c] = t;
-    vals[c] = (uint32_t)c;
-    atomicAdd((unsigned long long*)&counts[t], 1ull);
-    if (t == 2) atomicMax(maxd, (unsigned long long)U);
+                            int64_t* __restrict__ counts) {
+  const int lane = threadIdx.x & 31;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t base = blockIdx.x * (int64_t)blockDim.x; base < nvp; base += stride) {
+    const int64_t c = base + threadIdx.x;
+    uint32_t t = 3u;
+    if (c < nvp) {
+      const int64_t D = medge[mo[c + 1]] - medge[mo[c]];
+      const int64_t U = D < nvp ? D : nvp;
+      t = D <= kAggWarpMaxD ? 0u : (2 * U <= kAggCtaMaxCap ? 1u : 2u);
+      keys[c] = t;
+      vals[c] = (uint32_t)c;
+    }
+    const unsigned peers = __match_any_sync(NIDO_FULL_MASK, t);
+    if (t < 3u && lane == __ffs(peers) - 1) atomicAdd((unsigned long long*)&counts[t], (unsigned long long)__popc(peers));
+  }
+}
+
+// member-edge count of the listed coarse vertices (for the segment plan)
+__global__ void k_agg_sizes(const int32_t* __restrict__ list, int64_t n, const int64_t* __restrict__ mo,
+                            const int64_t* __restrict__ medge, int64_t* __restrict__ out) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int c = list[i];
+    out[i] = medge[mo[c + 1]] - medge[mo[c]];
   }
 }
 
@@ -318,6 +334,134 @@ __global__ void __launch_bounds__(kAggThreads) k_agg_cta(const int32_t* __restri
   }
 }
 
+// ---- giant coarse vertices: kAggSeg-position segments on many CTAs ----------
+// Segment items (coarse vertex index in the list, segment) are processed in
+// three passes over per-vertex tables in global memory: insert (atomic sums,
+// first list position per id), count first occurrences per segment, and, after
+// a scan of the counts, emit every id at its first-occurrence rank.
+constexpr int kAggSeg = 4096;
+
+struct SegArgs {
+  const int2* __restrict__ items;
+  const int32_t* __restrict__ cids;     // coarse vertex of each list entry
+  const int64_t* __restrict__ toff;     // table offset of each list entry
+  const int32_t* __restrict__ caps;     // table size of each list entry
+  const int64_t* __restrict__ first;    // first item of each list entry
+  int32_t* keys;
+  double* vals;
+  int32_t* fpos;
+};
+
+__device__ __forceinline__ void seg_range(const AggArgs& q, const SegArgs& a, int2 item, int& cp, int64_t& m0,
+                                          int64_t& m1, int64_t& P0, int64_t& s0, int64_t& s1) {
+  cp = a.cids[item.x];
+  m0 = q.mo[cp];
+  m1 = q.mo[cp + 1];
+  P0 = q.medge[m0];
+  const int64_t P1 = q.medge[m1];
+  s0 = P0 + (int64_t)item.y * kAggSeg;
+  s1 = min(P1, s0 + kAggSeg);
+}
+
+__global__ void __launch_bounds__(256) k_agg_seg_insert(int64_t n, AggArgs q, SegArgs a) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  for (int64_t it = blockIdx.x; it < n; it += gridDim.x) {
+    const int2 item = a.items[it];
+    int cp;
+    int64_t m0, m1, P0, s0, s1;
+    seg_range(q, a, item, cp, m0, m1, P0, s0, s1);
+    int* keys = a.keys + a.toff[item.x];
+    double* vals = a.vals + a.toff[item.x];
+    int* fpos = a.fpos + a.toff[item.x];
+    const unsigned mask = (unsigned)a.caps[item.x] - 1;
+    for (int64_t base = s0 + (int64_t)wid * 32; base < s1; base += blockDim.x) {
+      const int64_t P = base + lane;
+      const bool ok = P < s1;
+      int X = -1;
+      double wt = 0.;
+      if (ok) load_pos(q, m0, m1, P, X, wt);
+      const unsigned peers = __match_any_sync(NIDO_FULL_MASK, X);
+      const bool lead = ok && lane == __ffs(peers) - 1;
+      double e = 0.;
+      unsigned rem = ok ? peers : 0u;
+      const int maxcnt = __reduce_max_sync(NIDO_FULL_MASK, (unsigned)__popc(rem));
+      for (int k = 0; k < maxcnt; ++k) {
+        const int src = rem ? __ffs(rem) - 1 : lane;
+        const double x = __shfl_sync(NIDO_FULL_MASK, wt, src);
+        if (rem) { e += x; rem &= rem - 1; }
+      }
+      if (lead) {
+        bool isnew;
+        const int h = find_or_insert(keys, mask, X, &isnew);
+        if (h >= 0) {
+          atomicAdd(&vals[h], e);
+          atomicMin(&fpos[h], (int)(P - P0));
+        } else {
+          atomicAdd(q.err, 1ull);
+        }
+      }
+    }
+  }
+}
+
+// count (kEmit false) or emit (kEmit true) first occurrences of a segment
+template <bool kEmit>
+__global__ void __launch_bounds__(256) k_agg_seg_scan(int64_t n, AggArgs q, SegArgs a, int64_t* segcnt) {
+  __shared__ int wsum[8];
+  __shared__ int64_t running_s;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  for (int64_t it = blockIdx.x; it < n; it += gridDim.x) {
+    const int2 item = a.items[it];
+    int cp;
+    int64_t m0, m1, P0, s0, s1;
+    seg_range(q, a, item, cp, m0, m1, P0, s0, s1);
+    const int* keys = a.keys + a.toff[item.x];
+    const double* vals = a.vals + a.toff[item.x];
+    const int* fpos = a.fpos + a.toff[item.x];
+    const unsigned mask = (unsigned)a.caps[item.x] - 1;
+    const int64_t base_out = kEmit ? segcnt[it] - segcnt[a.first[item.x]] : 0;
+    if (threadIdx.x == 0) running_s = 0;
+    __syncthreads();
+    for (int64_t base = s0; base < s1; base += blockDim.x) {
+      const int64_t P = base + threadIdx.x;
+      int X = -1;
+      double wt = 0.;
+      int h = -1;
+      bool firstocc = false;
+      if (P < s1) {
+        load_pos(q, m0, m1, P, X, wt);
+        h = find_slot(keys, mask, X);
+        firstocc = h >= 0 && fpos[h] == (int)(P - P0);
+      }
+      const unsigned bal = __ballot_sync(NIDO_FULL_MASK, firstocc);
+      if (lane == 0) wsum[wid] = __popc(bal);
+      __syncthreads();
+      if (kEmit && firstocc) {
+        int64_t idx = base_out + running_s + __popc(bal & lanemask_lt());
+        for (int i = 0; i < wid; ++i) idx += wsum[i];
+        q.tadj[P0 + idx] = X;
+        q.tw[P0 + idx] = vals[h];
+      }
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        int t = 0;
+        for (int i = 0; i < (int)(blockDim.x >> 5); ++i) t += wsum[i];
+        running_s += t;
+      }
+      __syncthreads();
+    }
+    if (!kEmit && threadIdx.x == 0) segcnt[it] = running_s;
+    __syncthreads();
+  }
+}
+
+// degree of each giant coarse vertex from the scanned segment counts
+__global__ void k_agg_seg_deg(int64_t nlist, const int32_t* __restrict__ cids, const int64_t* __restrict__ first,
+                              const int64_t* __restrict__ segoff, int64_t* __restrict__ degp) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nlist; i += (int64_t)gridDim.x * blockDim.x)
+    degp[cids[i]] = segoff[first[i + 1]] - segoff[first[i]];
+}
+
 // copy each coarse vertex's entries to its final offset
 __global__ void k_compact(int64_t nvp, const int64_t* __restrict__ mo, const int64_t* __restrict__ medge,
                           const int64_t* __restrict__ coff, const int32_t* __restrict__ tadj,
@@ -353,7 +497,6 @@ int launch_aggregation(nido_graph_s* g, int* done) {
   int64_t* medge = ar.take<int64_t>(nv + 1);
   int64_t* degp = ar.take<int64_t>(nv + 1);
   int64_t* counts = ar.take<int64_t>(4);
-  unsigned long long* maxd = ar.take<unsigned long long>(1);
   int64_t* temp = ar.take<int64_t>(std::max(radix_temp_elems(nv), scan_temp_elems(nv + 1)));
   if (!temp) return nido_set_error(NIDO_E_NOMEM, "scratch arena too small (aggregation)");
   const unsigned gv = grid_for(nv, 256, kSMs * 16);
@@ -377,19 +520,16 @@ int launch_aggregation(nido_graph_s* g, int* done) {
   NIDO_LAUNCH_CHECK();
   NIDO_TRY(scan_exclusive_i64(medge, medge, nv, temp, s));
   NIDO_CUDA_TRY(cudaMemsetAsync(counts, 0, sizeof(int64_t) * 4, s));
-  NIDO_CUDA_TRY(cudaMemsetAsync(maxd, 0, sizeof(unsigned long long), s));
   // coarse-vertex tiers (rk2/rv2 are free after the member sort)
   uint32_t* tk = rk2;
   uint32_t* tv = rv2;
   uint32_t* tk2 = reinterpret_cast<uint32_t*>(used);
   uint32_t* tv2 = reinterpret_cast<uint32_t*>(degp);  // degp is written only after the tier sort
-  k_agg_tiers<<<grid_for(nvp, 256, kSMs * 16), 256, 0, s>>>(mo, medge, nvp, tk, tv, counts, maxd);
+  k_agg_tiers<<<grid_for(nvp, 256, kSMs * 16), 256, 0, s>>>(mo, medge, nvp, tk, tv, counts);
   NIDO_LAUNCH_CHECK();
   NIDO_TRY(radix_sort_pairs(tk, tv, tk2, tv2, nvp, 2, temp, s));
   int64_t cnt[4] = {0, 0, 0, 0};
-  unsigned long long maxu = 0;
   NIDO_CUDA_TRY(cudaMemcpyAsync(cnt, counts, sizeof(cnt), cudaMemcpyDeviceToHost, s));
-  NIDO_CUDA_TRY(cudaMemcpyAsync(&maxu, maxd, sizeof(maxu), cudaMemcpyDeviceToHost, s));
   NIDO_CUDA_TRY(cudaStreamSynchronize(s));
 
   AggArgs q{g->off, g->adj, g->w, newid, rv, mo, medge, g->adj2, g->w2, degp, nvp,
@@ -411,23 +551,71 @@ int launch_aggregation(nido_graph_s* g, int* done) {
     NIDO_LAUNCH_CHECK();
   }
   if (cnt[2] > 0) {
-    int64_t slab = 64;
-    while (slab < 2 * (int64_t)maxu) slab <<= 1;
-    int64_t slabs = std::min<int64_t>(cnt[2], kSMs);
-    while (slabs > 1 && slabs * slab * 16 > ((int64_t)4 << 30)) slabs /= 2;
-    int32_t *gk = nullptr, *gf = nullptr;
-    double* gvv = nullptr;
-    NIDO_CUDA_TRY(cudaMallocAsync((void**)&gk, sizeof(int32_t) * slabs * slab, s));
-    NIDO_CUDA_TRY(cudaMallocAsync((void**)&gf, sizeof(int32_t) * slabs * slab, s));
-    NIDO_CUDA_TRY(cudaMallocAsync((void**)&gvv, sizeof(double) * slabs * slab, s));
-    NIDO_CUDA_TRY(cudaMemsetAsync(gk, 0xff, sizeof(int32_t) * slabs * slab, s));
-    NIDO_CUDA_TRY(cudaMemsetAsync(gf, 0x7f, sizeof(int32_t) * slabs * slab, s));
-    NIDO_CUDA_TRY(cudaMemsetAsync(gvv, 0, sizeof(double) * slabs * slab, s));
-    k_agg_cta<true><<<(unsigned)slabs, kAggThreads, 0, s>>>(list + cnt[0] + cnt[1], cnt[2], q, 0, gk, gvv, gf, slab);
+    // plan: per giant coarse vertex a table of >= 2*min(D, nvp) slots and
+    // ceil(D / kAggSeg) segment items
+    const int64_t n2 = cnt[2];
+    const int32_t* list2 = list + cnt[0] + cnt[1];
+    int64_t* dsz = ar.take<int64_t>(n2);
+    if (!dsz) return nido_set_error(NIDO_E_NOMEM, "scratch arena too small (aggregation plan)");
+    k_agg_sizes<<<grid_for(n2, 256, kSMs * 4), 256, 0, s>>>(list2, n2, mo, medge, dsz);
     NIDO_LAUNCH_CHECK();
-    NIDO_CUDA_TRY(cudaFreeAsync(gk, s));
-    NIDO_CUDA_TRY(cudaFreeAsync(gf, s));
-    NIDO_CUDA_TRY(cudaFreeAsync(gvv, s));
+    std::vector<int64_t> D(n2);
+    std::vector<int32_t> cids(n2), caps(n2);
+    NIDO_CUDA_TRY(cudaMemcpyAsync(D.data(), dsz, sizeof(int64_t) * n2, cudaMemcpyDeviceToHost, s));
+    NIDO_CUDA_TRY(cudaMemcpyAsync(cids.data(), list2, sizeof(int32_t) * n2, cudaMemcpyDeviceToHost, s));
+    NIDO_CUDA_TRY(cudaStreamSynchronize(s));
+    std::vector<int64_t> toff(n2), first(n2 + 1);
+    std::vector<int2> items;
+    int64_t slots = 0;
+    for (int64_t i = 0; i < n2; ++i) {
+      const int64_t u = std::min<int64_t>(D[i], nvp);
+      int64_t cap = 64;
+      while (cap < 2 * u) cap <<= 1;
+      caps[i] = (int32_t)cap;
+      toff[i] = slots;
+      slots += cap;
+      first[i] = (int64_t)items.size();
+      for (int64_t sg = 0; sg * kAggSeg < D[i]; ++sg) items.push_back(make_int2((int)i, (int)sg));
+    }
+    first[n2] = (int64_t)items.size();
+    const int64_t ni = (int64_t)items.size();
+    char* buf = nullptr;
+    const size_t bytes = sizeof(int2) * ni + sizeof(int32_t) * 2 * n2 + sizeof(int64_t) * (2 * n2 + 1) +
+                         sizeof(int64_t) * (ni + 1) + sizeof(int64_t) * scan_temp_elems(ni) +
+                         (sizeof(int32_t) * 2 + sizeof(double)) * slots + 8 * 256;
+    NIDO_CUDA_TRY(cudaMallocAsync((void**)&buf, bytes, s));
+    Arena pa(buf, bytes);
+    int2* ditems = pa.take<int2>(ni);
+    int32_t* dcids = pa.take<int32_t>(n2);
+    int32_t* dcaps = pa.take<int32_t>(n2);
+    int64_t* dtoff = pa.take<int64_t>(n2);
+    int64_t* dfirst = pa.take<int64_t>(n2 + 1);
+    int64_t* segcnt = pa.take<int64_t>(ni + 1);
+    int64_t* stemp = pa.take<int64_t>(scan_temp_elems(ni));
+    int32_t* tkeys = pa.take<int32_t>(slots);
+    int32_t* tfpos = pa.take<int32_t>(slots);
+    double* tvals = pa.take<double>(slots);
+    NIDO_CUDA_TRY(cudaMemcpyAsync(ditems, items.data(), sizeof(int2) * ni, cudaMemcpyHostToDevice, s));
+    NIDO_CUDA_TRY(cudaMemcpyAsync(dcids, cids.data(), sizeof(int32_t) * n2, cudaMemcpyHostToDevice, s));
+    NIDO_CUDA_TRY(cudaMemcpyAsync(dcaps, caps.data(), sizeof(int32_t) * n2, cudaMemcpyHostToDevice, s));
+    NIDO_CUDA_TRY(cudaMemcpyAsync(dtoff, toff.data(), sizeof(int64_t) * n2, cudaMemcpyHostToDevice, s));
+    NIDO_CUDA_TRY(cudaMemcpyAsync(dfirst, first.data(), sizeof(int64_t) * (n2 + 1), cudaMemcpyHostToDevice, s));
+    NIDO_CUDA_TRY(cudaMemsetAsync(tkeys, 0xff, sizeof(int32_t) * slots, s));
+    NIDO_CUDA_TRY(cudaMemsetAsync(tfpos, 0x7f, sizeof(int32_t) * slots, s));
+    NIDO_CUDA_TRY(cudaMemsetAsync(tvals, 0, sizeof(double) * slots, s));
+    SegArgs sa{ditems, dcids, dtoff, dcaps, dfirst, tkeys, tvals, tfpos};
+    const unsigned gi = grid_for(ni, 1, kSMs * 8);
+    k_agg_seg_insert<<<gi, 256, 0, s>>>(ni, q, sa);
+    NIDO_LAUNCH_CHECK();
+    k_agg_seg_scan<false><<<gi, 256, 0, s>>>(ni, q, sa, segcnt);
+    NIDO_LAUNCH_CHECK();
+    NIDO_TRY(scan_exclusive_i64(segcnt, segcnt, ni, stemp, s));
+    k_agg_seg_scan<true><<<gi, 256, 0, s>>>(ni, q, sa, segcnt);
+    NIDO_LAUNCH_CHECK();
+    k_agg_seg_deg<<<grid_for(n2, 256, kSMs * 4), 256, 0, s>>>(n2, dcids, dfirst, segcnt, degp);
+    NIDO_LAUNCH_CHECK();
+    NIDO_CUDA_TRY(cudaStreamSynchronize(s));  // the host plan vectors go out of scope
+    NIDO_CUDA_TRY(cudaFreeAsync(buf, s));
   }
   // coarse offsets into off2, then the entries into the work CSR (when the
   // current graph is the work CSR, its lists are dead once pass 1 is done)

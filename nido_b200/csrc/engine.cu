@@ -87,33 +87,11 @@ __global__ void k_set_ids(const int64_t* __restrict__ c64, int64_t nv, int32_t* 
 
 constexpr unsigned kGrid = 148 * 8;
 
-int size_global_slabs(nido_graph g) {
-  // slabs for the global-memory tier of the move kernel and coarsening
-  if (g->max_degree <= g->ctx->tiers.cta_max) return NIDO_OK;
-  unsigned need = 64;
-  while ((int64_t)need < 2 * g->max_degree) need <<= 1;
-  if ((int64_t)need <= g->gslab) return NIDO_OK;
-  nido_ctx ctx = g->ctx;
-  dev_free(ctx, g->gkeys, sizeof(int32_t) * (size_t)g->gslab * g->gslabs);
-  dev_free(ctx, g->gvals, sizeof(double) * (size_t)g->gslab * g->gslabs);
-  g->gkeys = nullptr; g->gvals = nullptr; g->gslab = 0; g->gslabs = 0;
-  int slabs = nido::kSMs * 2;
-  while (slabs > 8 && (size_t)slabs * need * 12 > ((size_t)2 << 30)) slabs /= 2;
-  NIDO_TRY(dev_alloc(ctx, &g->gkeys, (int64_t)slabs * need));
-  NIDO_TRY(dev_alloc(ctx, &g->gvals, (int64_t)slabs * need));
-  NIDO_CUDA_TRY(cudaMemsetAsync(g->gkeys, 0xff, sizeof(int32_t) * (size_t)slabs * need, ctx->stream));
-  NIDO_CUDA_TRY(cudaMemsetAsync(g->gvals, 0, sizeof(double) * (size_t)slabs * need, ctx->stream));
-  g->gslab = need;
-  g->gslabs = slabs;
-  return NIDO_OK;
-}
-
 int prepare_phase(nido_graph g) {
   NIDO_TRY(nido::launch_vertex_weights(g));
   NIDO_TRY(nido::launch_mass(g));
   g->bins_valid = false;
   NIDO_TRY(nido::build_batches(g));
-  NIDO_TRY(size_global_slabs(g));
   return NIDO_OK;
 }
 
@@ -138,6 +116,7 @@ extern "C" int nido_ctx_create(int device, size_t hbm_budget_bytes, nido_ctx* ou
   if (prop.major != 10)
     return nido_set_error(NIDO_E_NODEVICE, "device %d is sm_%d%d; this build targets sm_100a", device,
                           prop.major, prop.minor);
+  NIDO_TRY(nido::move_init_attributes());
   nido_ctx ctx = new (std::nothrow) nido_ctx_s();
   if (!ctx) return nido_set_error(NIDO_E_NOMEM, "host allocation failed");
   ctx->device = device;
@@ -188,8 +167,10 @@ extern "C" int nido_graph_free(nido_graph g) {
   dev_free(ctx, g->clus, 4 * g->nv0); dev_free(ctx, g->perm, 4 * V);
   dev_free(ctx, g->dm, 64); dev_free(ctx, g->dcount, 64);
   dev_free(ctx, g->scratch, g->scratch_bytes);
-  dev_free(ctx, g->gkeys, sizeof(int32_t) * (size_t)g->gslab * g->gslabs);
-  dev_free(ctx, g->gvals, sizeof(double) * (size_t)g->gslab * g->gslabs);
+  // hub-tier buffers are sized per phase outside the budget accounting
+  for (void* p : {(void*)g->gkeys, (void*)g->gvals, (void*)g->hub_items, (void*)g->hub_v, (void*)g->hub_capv,
+                  (void*)g->hub_nseg, (void*)g->hub_toff, (void*)g->hub_done})
+    if (p) cudaFree(p);
   delete g;
   return NIDO_OK;
 }
@@ -477,9 +458,20 @@ extern "C" int nido_run(nido_graph g, const nido_params* p, int64_t* out_comm, n
   cudaEvent_t t0, t1;
   NIDO_CUDA_TRY(cudaEventCreate(&t0));
   NIDO_CUDA_TRY(cudaEventCreate(&t1));
+  auto now_ms = [] {
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
+  };
+  const uint64_t launches0 = nido_launch_count();
+  double tm = now_ms();
+  auto lap = [&](int slot) {
+    const double t = now_ms();
+    st.host_ms[slot] += t - tm;
+    tm = t;
+  };
   NIDO_CUDA_TRY(cudaEventRecord(t0, s));
   // every run starts from the uploaded graph, as on a fresh GraphGPU
   NIDO_TRY(reset_graph(g));
+  lap(0);
   const double tau = p->tau;
   bool done = false;
   int64_t phases = 0;
@@ -488,6 +480,7 @@ extern "C" int nido_run(nido_graph g, const nido_params* p, int64_t* out_comm, n
     NIDO_TRY(nido::launch_singleton(g));
     double Q;
     NIDO_TRY(nido::launch_modularity(g, &Q));
+    lap(2);
     const double Q_old = Q;
     if (p->verbose) printf("LOOP# \tQ \t\tdQ\n----------------------------------------\n0 \t%g \t0\n", Q);
     double dQ = NIDO_MAX_FLOAT;
@@ -506,8 +499,10 @@ extern "C" int nido_run(nido_graph g, const nido_params* p, int64_t* out_comm, n
       st.move_launches += g->nbatches;
       st.edges_scanned += (double)g->ne;
       st.move_bytes += 16.0 * (double)g->ne + 32.0 * (double)g->nv;
+      lap(1);
       double Qtmp;
       NIDO_TRY(nido::launch_modularity(g, &Qtmp));
+      lap(2);
       dQ = Qtmp - Q;
       ++loops;
       for (int b = 0; b < g->nbatches; ++b) {  // complete: the Q readback synchronized the stream
@@ -533,9 +528,12 @@ extern "C" int nido_run(nido_graph g, const nido_params* p, int64_t* out_comm, n
     }
     if (Q - Q_old > tau) {
       int d = 0;
+      lap(1);
       NIDO_TRY(nido::launch_aggregation(g, &d));
+      lap(3);
       done = d != 0;
       if (!done) NIDO_TRY(prepare_phase(g));
+      lap(4);
     } else {
       done = true;
     }
@@ -553,7 +551,10 @@ extern "C" int nido_run(nido_graph g, const nido_params* p, int64_t* out_comm, n
   int64_t nerr = 0;
   NIDO_CUDA_TRY(cudaMemcpy(&nerr, g->dcount + 1, sizeof(int64_t), cudaMemcpyDeviceToHost));
   if (nerr) return nido_set_error(NIDO_E_CUDA, "hash table overflow in %lld probes", (long long)nerr);
+  lap(1);
   if (out_comm) NIDO_TRY(nido_get_clustering(g, out_comm));
+  lap(5);
+  st.kernel_launches = (int64_t)(nido_launch_count() - launches0);
   if (stats) *stats = st;
   return NIDO_OK;
 }

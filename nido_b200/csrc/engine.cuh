@@ -24,25 +24,23 @@ enum Tier {
   kTierG8,      // d <= 8   : 8-lane group
   kTierG16,     // d <= 16  : 16-lane group
   kTierG32,     // d <= 32  : one warp, registers
-  kTierWarp,    // d <= warp_max : one warp, shared-memory hash
-  kTierCta,     // d <= cta_max  : one CTA, shared-memory hash
-  kTierGlobal,  // larger        : one CTA, hash table in global memory (L2)
+  kTierWarp,    // d <= 256  : one warp, shared-memory hash (512 slots)
+  kTierCtaS,    // d <= 1024 : one 128-thread CTA, shared-memory hash (2048 slots)
+  kTierCtaL,    // d <= 2048 : one 256-thread CTA, shared-memory hash (4096 slots)
+  kTierHub,     // larger    : 2048-edge segments on many CTAs, hash in global memory (L2)
   kNumTiers
 };
 
-struct TierConfig {
-  int warp_max = 256;     // largest degree handled by the warp tier
-  int cta_max = 4096;     // largest degree handled by the CTA shared-memory tier
-  int warps_per_cta = 8;  // CTAs of the warp tier
-  int cta_threads = 512;  // CTAs of the CTA / global tiers
-};
+// degree bounds of the tiers (the shared-memory table sizes are fixed by them)
+constexpr int kWarpMaxDeg = 256;
+constexpr int kCtaSMaxDeg = 1024;
+constexpr int kCtaLMaxDeg = 2048;
 
 struct nido_ctx_s {
   int device = 0;
   cudaStream_t stream = nullptr;
   size_t budget = 0;
   size_t used = 0;
-  TierConfig tiers;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   std::vector<cudaEvent_t> move_ev;  // 2 per batch, for per-iteration move timing
 };
@@ -85,11 +83,21 @@ struct nido_graph_s {
   // scratch arena (bytes), carved per operation
   char* scratch = nullptr;
   size_t scratch_bytes = 0;
-  // global-memory hash slabs for the largest tier (move and coarsening)
+  // hub tier of the move phase: per-hub tables in global memory (gslab slots
+  // in all) and (hub, segment) work items, planned once per phase
   int32_t* gkeys = nullptr;
   double* gvals = nullptr;
-  int64_t gslab = 0;   // slots per CTA slab
-  int gslabs = 0;      // number of slabs
+  int64_t gslab = 0;
+  int2* hub_items = nullptr;
+  int32_t* hub_v = nullptr;
+  int32_t* hub_capv = nullptr;
+  int32_t* hub_nseg = nullptr;
+  int64_t* hub_toff = nullptr;
+  int32_t* hub_done = nullptr;
+  int64_t hub_cap_items = 0, hub_cap_hubs_v = 0, hub_cap_hubs_c = 0, hub_cap_hubs_s = 0,
+          hub_cap_hubs_t = 0, hub_cap_hubs_d = 0;
+  int64_t nhubs = 0;
+  std::vector<int64_t> hub_item_off;  // items per batch
 
   std::vector<int64_t> cuts;     // host batch cuts (nbatches+1)
   std::vector<int64_t> tier_off; // host: nbatches*kNumTiers+1 offsets into perm
@@ -127,6 +135,8 @@ int build_batches(nido_graph_s* g);                     // cuts (host) + tier li
 // move phase (move.cu)
 // ev_start / ev_end (may be null) are recorded around the tier kernels
 int launch_move(nido_graph_s* g, int batch, int tie, cudaEvent_t ev_start, cudaEvent_t ev_end);
+int plan_hubs(nido_graph_s* g);          // per phase, after the tier lists
+int move_init_attributes();              // once per device
 // coarsening (coarsen.cu)
 int launch_aggregation(nido_graph_s* g, int* done);
 

@@ -169,29 +169,43 @@ __global__ void __launch_bounds__(256) k_move_group(const int32_t* __restrict__ 
   }
 }
 
-// Insert (c, e) into an open-addressing table.  Tables owned by one warp
-// (kAtomicVals false) see distinct keys from the warp's leaders, so the value
-// update needs no atomic.  Tables hold at least twice as many slots as the
-// vertex has edges, so a free slot always exists; the probe count is still
-// bounded by the table size, and a full table is reported through *err.
+
+// ---- hash tables --------------------------------------------------------------
+// Open addressing over a power-of-two slot array.  New keys are appended to an
+// occupied-slot list so that evaluation and clearing cost O(unique keys).
+// Tables hold at least twice as many slots as the vertex has edges, so a free
+// slot always exists; probing is still bounded by the table size, and a full
+// table is reported through *err.
+struct Table {
+  int* keys;
+  double* vals;
+  int* occ;
+  int* nocc;
+  unsigned mask;
+};
+
 template <bool kAtomicVals>
-__device__ __forceinline__ void table_add(int* keys, double* vals, unsigned mask, int c, double e,
-                                          unsigned long long* err) {
-  unsigned h = hash_slot(c, mask);
-  volatile int* vk = keys;
-  for (unsigned probe = 0; probe <= mask; ++probe) {
+__device__ __forceinline__ void table_add(const Table& t, int c, double e, unsigned long long* err) {
+  unsigned h = hash_slot(c, t.mask);
+  volatile int* vk = t.keys;
+  for (unsigned probe = 0; probe <= t.mask; ++probe) {
     const int kk = vk[h];
     bool hit = kk == c;
     if (!hit && kk == -1) {
-      const int old = atomicCAS(&keys[h], -1, c);
-      hit = (old == -1 || old == c);
+      const int old = atomicCAS(&t.keys[h], -1, c);
+      if (old == -1) {
+        if (t.occ) t.occ[atomicAdd(t.nocc, 1)] = (int)h;
+        hit = true;
+      } else {
+        hit = old == c;
+      }
     }
     if (hit) {
-      if (kAtomicVals) atomicAdd(&vals[h], e);
-      else vals[h] += e;
+      if (kAtomicVals) atomicAdd(&t.vals[h], e);
+      else t.vals[h] += e;
       return;
     }
-    h = (h + 1) & mask;
+    h = (h + 1) & t.mask;
   }
   atomicAdd(err, 1ull);
 }
@@ -202,77 +216,122 @@ __device__ __forceinline__ unsigned next_pow2_cap(int64_t d) {
   return c;
 }
 
-// ---- degree <= warp_max: one warp per vertex, shared-memory hash ---------------
-__global__ void __launch_bounds__(256) k_move_warp(const int32_t* __restrict__ list, int64_t n,
-                                                   MoveArgs p, int capmax) {
+// Accumulate the edges [s, eend) of vertex v, one 32-edge chunk per warp step
+// starting at `first` and advancing by `stride` edges.  Every lane of the warp
+// takes part.
+template <bool kAtomicVals>
+__device__ __forceinline__ void accumulate_edges(const MoveArgs& p, int v, int64_t first, int64_t eend,
+                                                 int64_t stride, const Table& t) {
+  const int lane = threadIdx.x & 31;
+  for (int64_t base = first; base < eend; base += stride) {
+    const int64_t j = base + lane;
+    const bool ok = j < eend;
+    int c = -1;
+    double wt = 0.;
+    if (ok) {
+      const int u = p.adj[j];
+      c = p.comm[u];
+      wt = (u == v) ? 0. : p.w[j];
+    }
+    const unsigned peers = __match_any_sync(NIDO_FULL_MASK, c);
+    const bool lead = ok && lane == __ffs(peers) - 1;
+    const double e = fold_peers(peers, ok, wt);
+    if (lead) table_add<kAtomicVals>(t, c, e, p.err);
+    if (!kAtomicVals) __syncwarp();
+  }
+}
+
+// Scan entries i = t0, t0+step, ... of the occupied list (or of all slots when
+// occ is null): e_own and the best (gain, tie key, community) of this thread.
+__device__ __forceinline__ void scan_entries(const MoveArgs& p, const Table& t, int n, int t0, int step,
+                                             int own, double ki, bool cg, double& eown, double& g,
+                                             unsigned long long& tk, int& cand) {
+  for (int i = t0; i < n; i += step) {
+    const int slot = t.occ ? t.occ[i] : i;
+    const int cc = cg ? __ldcg(&t.keys[slot]) : t.keys[slot];
+    if (cc < 0) continue;
+    const double val = cg ? __ldcg(&t.vals[slot]) : t.vals[slot];
+    if (cc == own) {
+      eown = val;
+    } else {
+      const double gg = gain_of(val, ki, p.a[cc], p.m);
+      if (better(gg, (unsigned)cc, g, tk)) { g = gg; tk = (unsigned)cc; cand = cc; }
+    }
+  }
+}
+
+// The reference's tie rule over the same entries: among communities whose
+// gain equals gm, the smallest (bitrev3(rank mod 8), rank), where rank counts
+// the vertex's neighbour communities with a smaller id.
+__device__ __forceinline__ void nido_tie_entries(const MoveArgs& p, const Table& t, int n, int t0, int step,
+                                                 int own, double ki, double gm, bool cg, double& g,
+                                                 unsigned long long& tk, int& cand) {
+  g = -NIDO_MAX_FLOAT; tk = kNoKey; cand = -1;
+  for (int i = t0; i < n; i += step) {
+    const int slot = t.occ ? t.occ[i] : i;
+    const int cc = cg ? __ldcg(&t.keys[slot]) : t.keys[slot];
+    if (cc < 0 || cc == own) continue;
+    const double val = cg ? __ldcg(&t.vals[slot]) : t.vals[slot];
+    if (gain_of(val, ki, p.a[cc], p.m) != gm) continue;
+    unsigned rank = 0;
+    for (int q = 0; q < n; ++q) {
+      const int kq = cg ? __ldcg(&t.keys[t.occ ? t.occ[q] : q]) : t.keys[t.occ ? t.occ[q] : q];
+      rank += (kq >= 0 && kq < cc) ? 1u : 0u;
+    }
+    const unsigned long long key = nido_key(rank);
+    if (key < tk) { tk = key; cand = cc; g = gm; }
+  }
+}
+
+__device__ __forceinline__ void decide(const MoveArgs& p, int v, int own, double ki, double aown, double eown,
+                                       double g, int cand) {
+  const double self = self_of(eown, ki, aown, p.m);
+  const double tot = __dsub_rn(g, self);
+  p.newc[v] = (cand >= 0 && tot > 0.) ? cand : own;
+}
+
+// ---- 32 < degree <= 256: one warp per vertex, table in shared memory -----------
+template <int kCap>
+__global__ void __launch_bounds__(256) k_move_warp(const int32_t* __restrict__ list, int64_t n, MoveArgs p) {
   extern __shared__ double smem[];
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-  double* vals = smem + (size_t)wid * capmax;
-  int* keys = reinterpret_cast<int*>(smem + (size_t)nwarps * capmax) + (size_t)wid * capmax;
-  for (int i = lane; i < capmax; i += 32) { keys[i] = -1; vals[i] = 0.; }
+  __shared__ int nocc_s[8];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  Table t;
+  t.vals = smem + (size_t)wid * kCap;
+  t.keys = reinterpret_cast<int*>(smem + 8 * kCap) + (size_t)wid * 2 * kCap;
+  t.occ = t.keys + kCap;
+  t.nocc = &nocc_s[wid];
+  for (int i = lane; i < kCap; i += 32) { t.keys[i] = -1; t.vals[i] = 0.; }
+  if (lane == 0) *t.nocc = 0;
   __syncwarp();
   const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
   for (int64_t task = warp; task < n; task += nw) {
     const int v = list[task];
     const int64_t s = p.off[v], eend = p.off[v + 1];
-    const unsigned cap = min((unsigned)capmax, next_pow2_cap(eend - s)), mask = cap - 1;
+    t.mask = min((unsigned)kCap, next_pow2_cap(eend - s)) - 1;
     const int own = p.comm[v];
     const double ki = p.k[v], aown = p.a[own];
-    for (int64_t base = s; base < eend; base += 32) {
-      const int64_t j = base + lane;
-      const bool ok = j < eend;
-      int c = -1;
-      double wt = 0.;
-      if (ok) {
-        const int u = p.adj[j];
-        c = p.comm[u];
-        wt = (u == v) ? 0. : p.w[j];
-      }
-      const unsigned peers = __match_any_sync(NIDO_FULL_MASK, c);
-      const bool lead = ok && lane == __ffs(peers) - 1;
-      const double e = fold_peers(peers, ok, wt);
-      if (lead) table_add<false>(keys, vals, mask, c, e, p.err);
-      __syncwarp();
-    }
+    accumulate_edges<false>(p, v, s, eend, 32, t);
+    const int nu = *t.nocc;
     double g = -NIDO_MAX_FLOAT, eown = 0.;
     unsigned long long tk = kNoKey;
     int cand = -1;
-    for (unsigned i = lane; i < cap; i += 32) {
-      const int cc = keys[i];
-      if (cc < 0) continue;
-      if (cc == own) {
-        eown = vals[i];
-      } else {
-        const double gg = gain_of(vals[i], ki, p.a[cc], p.m);
-        if (better(gg, (unsigned)cc, g, tk)) { g = gg; tk = (unsigned)cc; cand = cc; }
-      }
-    }
+    scan_entries(p, t, nu, lane, 32, own, ki, false, eown, g, tk, cand);
     eown = group_sum<32>(eown);
     if (p.tie == NIDO_TIE_NIDO) {
       const double gm = group_max<32>(g);
-      g = -NIDO_MAX_FLOAT; tk = kNoKey; cand = -1;
-      for (unsigned i = lane; i < cap; i += 32) {
-        const int cc = keys[i];
-        if (cc < 0 || cc == own) continue;
-        if (gain_of(vals[i], ki, p.a[cc], p.m) != gm) continue;
-        unsigned rank = 0;
-        for (unsigned q = 0; q < cap; ++q) {
-          const int kq = keys[q];
-          rank += (kq >= 0 && kq < cc) ? 1u : 0u;
-        }
-        const unsigned long long key = nido_key(rank);
-        if (key < tk) { tk = key; cand = cc; g = gm; }
-      }
+      nido_tie_entries(p, t, nu, lane, 32, own, ki, gm, false, g, tk, cand);
     }
     group_best<32>(g, tk, cand);
-    if (lane == 0) {
-      const double self = self_of(eown, ki, aown, p.m);
-      const double tot = __dsub_rn(g, self);
-      p.newc[v] = (cand >= 0 && tot > 0.) ? cand : own;
-    }
+    if (lane == 0) decide(p, v, own, ki, aown, eown, g, cand);
     __syncwarp();
-    for (unsigned i = lane; i < cap; i += 32) { keys[i] = -1; vals[i] = 0.; }
+    for (int i = lane; i < nu; i += 32) {
+      const int slot = t.occ[i];
+      t.keys[slot] = -1;
+      t.vals[slot] = 0.;
+    }
+    if (lane == 0) *t.nocc = 0;
     __syncwarp();
   }
 }
@@ -318,90 +377,119 @@ __device__ double block_max(double x, double* sx) {
   return t;
 }
 
-// ---- larger degrees: one CTA per vertex; table in shared memory or in a
-// per-CTA global-memory slab (kept cleared between vertices) -------------------
-template <bool kGlobal>
-__global__ void __launch_bounds__(512) k_move_cta(const int32_t* __restrict__ list, int64_t n, MoveArgs p,
-                                                  int capmax, int32_t* gkeys, double* gvals,
-                                                  int64_t gslab) {
+// Evaluate a filled table with the whole block and write newc[v].
+__device__ __forceinline__ void block_evaluate(const MoveArgs& p, const Table& t, int n, bool cg, int v, int own,
+                                               double ki, double aown, double* sg, unsigned long long* stk,
+                                               int* sc) {
+  double g = -NIDO_MAX_FLOAT, eown = 0.;
+  unsigned long long tk = kNoKey;
+  int cand = -1;
+  scan_entries(p, t, n, threadIdx.x, blockDim.x, own, ki, cg, eown, g, tk, cand);
+  eown = block_sum(eown, sg);
+  if (p.tie == NIDO_TIE_NIDO) {
+    const double gm = block_max(g, sg);
+    nido_tie_entries(p, t, n, threadIdx.x, blockDim.x, own, ki, gm, cg, g, tk, cand);
+  }
+  block_best(g, tk, cand, sg, stk, sc);
+  if (threadIdx.x == 0) decide(p, v, own, ki, aown, eown, g, cand);
+}
+
+// ---- 256 < degree <= 2048: one CTA per vertex, table in shared memory ----------
+template <int kThreads, int kCap>
+__global__ void __launch_bounds__(kThreads) k_move_cta(const int32_t* __restrict__ list, int64_t n, MoveArgs p) {
   extern __shared__ double smem[];
   __shared__ double sg[32];
   __shared__ unsigned long long stk[32];
   __shared__ int sc[32];
-  int* keys;
-  double* vals;
-  if (kGlobal) {
-    keys = gkeys + (size_t)blockIdx.x * gslab;
-    vals = gvals + (size_t)blockIdx.x * gslab;
-  } else {
-    vals = smem;
-    keys = reinterpret_cast<int*>(smem + capmax);
-    for (int i = threadIdx.x; i < capmax; i += blockDim.x) { keys[i] = -1; vals[i] = 0.; }
-    __syncthreads();
-  }
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  __shared__ int nocc_s;
+  Table t;
+  t.vals = smem;
+  t.keys = reinterpret_cast<int*>(smem + kCap);
+  t.occ = t.keys + kCap;
+  t.nocc = &nocc_s;
+  for (int i = threadIdx.x; i < kCap; i += kThreads) { t.keys[i] = -1; t.vals[i] = 0.; }
+  if (threadIdx.x == 0) nocc_s = 0;
+  __syncthreads();
+  const int wid = threadIdx.x >> 5;
   for (int64_t task = blockIdx.x; task < n; task += gridDim.x) {
     const int v = list[task];
     const int64_t s = p.off[v], eend = p.off[v + 1];
-    unsigned cap = next_pow2_cap(eend - s);
-    if (!kGlobal) cap = min(cap, (unsigned)capmax);
-    const unsigned mask = cap - 1;
+    t.mask = min((unsigned)kCap, next_pow2_cap(eend - s)) - 1;
     const int own = p.comm[v];
     const double ki = p.k[v], aown = p.a[own];
-    for (int64_t base = s + (int64_t)wid * 32; base < eend; base += blockDim.x) {
-      const int64_t j = base + lane;
-      const bool ok = j < eend;
-      int c = -1;
-      double wt = 0.;
-      if (ok) {
-        const int u = p.adj[j];
-        c = p.comm[u];
-        wt = (u == v) ? 0. : p.w[j];
-      }
-      const unsigned peers = __match_any_sync(NIDO_FULL_MASK, c);
-      const bool lead = ok && lane == __ffs(peers) - 1;
-      const double e = fold_peers(peers, ok, wt);
-      if (lead) table_add<true>(keys, vals, mask, c, e, p.err);
+    accumulate_edges<true>(p, v, s + (int64_t)wid * 32, eend, kThreads, t);
+    __syncthreads();
+    const int nu = nocc_s;
+    block_evaluate(p, t, nu, false, v, own, ki, aown, sg, stk, sc);
+    for (int i = threadIdx.x; i < nu; i += kThreads) {
+      const int slot = t.occ[i];
+      t.keys[slot] = -1;
+      t.vals[slot] = 0.;
     }
     __syncthreads();
-    double g = -NIDO_MAX_FLOAT, eown = 0.;
-    unsigned long long tk = kNoKey;
-    int cand = -1;
-    for (unsigned i = threadIdx.x; i < cap; i += blockDim.x) {
-      const int cc = keys[i];
-      if (cc < 0) continue;
-      if (cc == own) {
-        eown = vals[i];
-      } else {
-        const double gg = gain_of(vals[i], ki, p.a[cc], p.m);
-        if (better(gg, (unsigned)cc, g, tk)) { g = gg; tk = (unsigned)cc; cand = cc; }
-      }
-    }
-    eown = block_sum(eown, sg);
-    if (p.tie == NIDO_TIE_NIDO) {
-      const double gm = block_max(g, sg);
-      g = -NIDO_MAX_FLOAT; tk = kNoKey; cand = -1;
-      for (unsigned i = threadIdx.x; i < cap; i += blockDim.x) {
-        const int cc = keys[i];
-        if (cc < 0 || cc == own) continue;
-        if (gain_of(vals[i], ki, p.a[cc], p.m) != gm) continue;
-        unsigned rank = 0;
-        for (unsigned q = 0; q < cap; ++q) {
-          const int kq = keys[q];
-          rank += (kq >= 0 && kq < cc) ? 1u : 0u;
-        }
-        const unsigned long long key = nido_key(rank);
-        if (key < tk) { tk = key; cand = cc; g = gm; }
-      }
-    }
-    block_best(g, tk, cand, sg, stk, sc);
-    if (threadIdx.x == 0) {
-      const double self = self_of(eown, ki, aown, p.m);
-      const double tot = __dsub_rn(g, self);
-      p.newc[v] = (cand >= 0 && tot > 0.) ? cand : own;
-    }
-    for (unsigned i = threadIdx.x; i < cap; i += blockDim.x) { keys[i] = -1; vals[i] = 0.; }
+    if (threadIdx.x == 0) nocc_s = 0;
     __syncthreads();
+  }
+}
+
+// ---- degree > 2048: hub vertices split into segments of kHubSeg edges ----------
+// Each CTA takes one (hub, segment) item and merges its edges into the hub's
+// table in global memory (L2-resident); the CTA that finishes a hub's last
+// segment (an atomic ticket; nobody waits) evaluates and clears the table.
+constexpr int kHubSeg = 2048;
+constexpr int kHubThreads = 256;
+
+__global__ void __launch_bounds__(kHubThreads) k_move_hub(const int2* __restrict__ items, int64_t n,
+                                                          const int32_t* __restrict__ hub_v,
+                                                          const int64_t* __restrict__ hub_toff,
+                                                          const int32_t* __restrict__ hub_cap,
+                                                          const int32_t* __restrict__ hub_nseg,
+                                                          int32_t* __restrict__ hub_done, int32_t* gkeys,
+                                                          double* gvals, MoveArgs p) {
+  __shared__ double sg[32];
+  __shared__ unsigned long long stk[32];
+  __shared__ int sc[32];
+  __shared__ int last_s;
+  const int wid = threadIdx.x >> 5;
+  for (int64_t it = blockIdx.x; it < n; it += gridDim.x) {
+    const int2 item = items[it];
+    const int h = item.x;
+    const int v = hub_v[h];
+    Table t;
+    t.keys = gkeys + hub_toff[h];
+    t.vals = gvals + hub_toff[h];
+    t.occ = nullptr;
+    t.nocc = nullptr;
+    t.mask = (unsigned)hub_cap[h] - 1;
+    const int64_t s = p.off[v], eend = p.off[v + 1];
+    const int64_t s0 = s + (int64_t)item.y * kHubSeg;
+    const int64_t s1 = min(eend, s0 + kHubSeg);
+    accumulate_edges<true>(p, v, s0 + (int64_t)wid * 32, s1, kHubThreads, t);
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last_s = atomicAdd(&hub_done[h], 1) == hub_nseg[h] - 1;
+    __syncthreads();
+    if (last_s) {
+      __threadfence();
+      const int own = p.comm[v];
+      const double ki = p.k[v], aown = p.a[own];
+      block_evaluate(p, t, (int)(t.mask + 1), true, v, own, ki, aown, sg, stk, sc);
+      for (unsigned i = threadIdx.x; i <= t.mask; i += kHubThreads) {
+        t.keys[i] = -1;
+        t.vals[i] = 0.;
+      }
+      if (threadIdx.x == 0) hub_done[h] = 0;
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void k_hub_degrees(const int32_t* __restrict__ list, int64_t n, const int64_t* __restrict__ off,
+                              int64_t* __restrict__ out) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int v = list[i];
+    out[2 * i] = v;
+    out[2 * i + 1] = off[v + 1] - off[v];
   }
 }
 
@@ -410,20 +498,113 @@ inline unsigned grid_cap(int64_t blocks, int64_t cap) {
   return (unsigned)std::min<int64_t>(blocks, cap);
 }
 
-unsigned pow2_at_least(int64_t x) {
-  unsigned c = 64;
-  while ((int64_t)c < x) c <<= 1;
-  return c;
+template <typename T>
+int ensure(nido_graph_s* g, T** p, int64_t* cap, int64_t n) {
+  if (n <= *cap) return NIDO_OK;
+  if (*p) cudaFree(*p);
+  *p = nullptr;
+  *cap = 0;
+  const int64_t m = std::max<int64_t>(n, 1024);
+  NIDO_CUDA_TRY(cudaMalloc((void**)p, sizeof(T) * (size_t)m));
+  *cap = m;
+  (void)g;
+  return NIDO_OK;
 }
 
 }  // namespace
+
+// Per-phase plan of the hub tier: table offsets, segment items per batch.
+int plan_hubs(nido_graph_s* g) {
+  const int nb = g->nbatches;
+  const int64_t h0 = g->tier_off[(size_t)kTierHub * nb], h1 = g->tier_off[(size_t)(kTierHub + 1) * nb];
+  const int64_t nh = h1 - h0;
+  g->hub_item_off.assign(nb + 1, 0);
+  g->nhubs = nh;
+  if (nh == 0) return NIDO_OK;
+  cudaStream_t s = g->ctx->stream;
+  Arena ar(g->scratch, g->scratch_bytes);
+  int64_t* vd = ar.take<int64_t>(2 * nh);
+  if (!vd) return nido_set_error(NIDO_E_NOMEM, "scratch arena too small (hubs)");
+  k_hub_degrees<<<grid_cap((nh + 255) / 256, kSMs * 4), 256, 0, s>>>(g->perm + h0, nh, g->off, vd);
+  NIDO_LAUNCH_CHECK();
+  std::vector<int64_t> h(2 * nh);
+  NIDO_CUDA_TRY(cudaMemcpyAsync(h.data(), vd, sizeof(int64_t) * 2 * nh, cudaMemcpyDeviceToHost, s));
+  NIDO_CUDA_TRY(cudaStreamSynchronize(s));
+  std::vector<int32_t> hv(nh), hcap(nh), hseg(nh);
+  std::vector<int64_t> htoff(nh);
+  std::vector<int2> items;
+  int64_t toff = 0;
+  for (int64_t i = 0; i < nh; ++i) {
+    const int64_t d = h[2 * i + 1];
+    const int64_t u = std::min<int64_t>(d, g->nv);
+    int64_t cap = 64;
+    while (cap < 2 * u) cap <<= 1;
+    hv[i] = (int32_t)h[2 * i];
+    hcap[i] = (int32_t)cap;
+    htoff[i] = toff;
+    toff += cap;
+    hseg[i] = (int32_t)((d + kHubSeg - 1) / kHubSeg);
+  }
+  // items grouped by batch: hubs are listed by batch within the tier
+  for (int b = 0; b < nb; ++b) {
+    const int64_t a0 = g->tier_off[(size_t)kTierHub * nb + b] - h0;
+    const int64_t a1 = g->tier_off[(size_t)kTierHub * nb + b + 1] - h0;
+    for (int64_t i = a0; i < a1; ++i)
+      for (int sgi = 0; sgi < hseg[i]; ++sgi) items.push_back(make_int2((int)i, sgi));
+    g->hub_item_off[b + 1] = (int64_t)items.size();
+  }
+  NIDO_TRY(ensure(g, &g->hub_v, &g->hub_cap_hubs_v, nh));
+  NIDO_TRY(ensure(g, &g->hub_capv, &g->hub_cap_hubs_c, nh));
+  NIDO_TRY(ensure(g, &g->hub_nseg, &g->hub_cap_hubs_s, nh));
+  NIDO_TRY(ensure(g, &g->hub_toff, &g->hub_cap_hubs_t, nh));
+  NIDO_TRY(ensure(g, &g->hub_done, &g->hub_cap_hubs_d, nh));
+  NIDO_TRY(ensure(g, &g->hub_items, &g->hub_cap_items, (int64_t)items.size()));
+  if (toff > g->gslab) {
+    if (g->gkeys) cudaFree(g->gkeys);
+    if (g->gvals) cudaFree(g->gvals);
+    g->gkeys = nullptr;
+    g->gvals = nullptr;
+    g->gslab = 0;
+    NIDO_CUDA_TRY(cudaMalloc((void**)&g->gkeys, sizeof(int32_t) * (size_t)toff));
+    NIDO_CUDA_TRY(cudaMalloc((void**)&g->gvals, sizeof(double) * (size_t)toff));
+    NIDO_CUDA_TRY(cudaMemsetAsync(g->gkeys, 0xff, sizeof(int32_t) * (size_t)toff, s));
+    NIDO_CUDA_TRY(cudaMemsetAsync(g->gvals, 0, sizeof(double) * (size_t)toff, s));
+    g->gslab = toff;
+  }
+  NIDO_CUDA_TRY(cudaMemcpyAsync(g->hub_v, hv.data(), sizeof(int32_t) * nh, cudaMemcpyHostToDevice, s));
+  NIDO_CUDA_TRY(cudaMemcpyAsync(g->hub_capv, hcap.data(), sizeof(int32_t) * nh, cudaMemcpyHostToDevice, s));
+  NIDO_CUDA_TRY(cudaMemcpyAsync(g->hub_nseg, hseg.data(), sizeof(int32_t) * nh, cudaMemcpyHostToDevice, s));
+  NIDO_CUDA_TRY(cudaMemcpyAsync(g->hub_toff, htoff.data(), sizeof(int64_t) * nh, cudaMemcpyHostToDevice, s));
+  NIDO_CUDA_TRY(cudaMemsetAsync(g->hub_done, 0, sizeof(int32_t) * nh, s));
+  NIDO_CUDA_TRY(cudaMemcpyAsync(g->hub_items, items.data(), sizeof(int2) * items.size(), cudaMemcpyHostToDevice, s));
+  NIDO_CUDA_TRY(cudaStreamSynchronize(s));  // the host vectors go out of scope
+  return NIDO_OK;
+}
+
+namespace {
+constexpr int kWarpCap = 512;     // warp tier: degree <= 256
+constexpr int kCtaSCap = 2048;    // 128-thread CTA tier: degree <= 1024
+constexpr int kCtaLCap = 4096;    // 256-thread CTA tier: degree <= 2048
+
+template <typename K>
+int set_smem(K kernel, size_t bytes) {
+  NIDO_CUDA_TRY(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+  return NIDO_OK;
+}
+}  // namespace
+
+int move_init_attributes() {
+  NIDO_TRY(set_smem(k_move_warp<kWarpCap>, (size_t)8 * kWarpCap * 16));
+  NIDO_TRY(set_smem(k_move_cta<128, kCtaSCap>, (size_t)kCtaSCap * 16));
+  NIDO_TRY(set_smem(k_move_cta<256, kCtaLCap>, (size_t)kCtaLCap * 16));
+  return NIDO_OK;
+}
 
 int launch_move(nido_graph_s* g, int batch, int tie, cudaEvent_t ev_start, cudaEvent_t ev_end) {
   if (batch < 0 || batch >= g->nbatches)
     return nido_set_error(NIDO_E_INVALID, "louvain_update: batch %d out of range [0,%d)", batch, g->nbatches);
   if (!g->bins_valid) NIDO_TRY(build_batches(g));
   cudaStream_t s = g->ctx->stream;
-  const TierConfig& tc = g->ctx->tiers;
   MoveArgs p{g->off, g->adj, g->w, g->comm, g->k, g->a, g->newc, g->m, tie,
              reinterpret_cast<unsigned long long*>(g->dcount + 1)};
   const int nb = g->nbatches;
@@ -446,29 +627,21 @@ int launch_move(nido_graph_s* g, int batch, int tie, cudaEvent_t ev_start, cudaE
       case kTierG32:
         k_move_group<32><<<grid_cap((n + 7) / 8, kSMs * 16), 256, 0, s>>>(list, n, p);
         break;
-      case kTierWarp: {
-        const int capmax = (int)pow2_at_least(2 * (int64_t)tc.warp_max);
-        const int threads = 32 * tc.warps_per_cta;
-        const size_t sm = (size_t)tc.warps_per_cta * capmax * (sizeof(double) + sizeof(int));
-        NIDO_CUDA_TRY(cudaFuncSetAttribute(k_move_warp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-        k_move_warp<<<grid_cap((n + tc.warps_per_cta - 1) / tc.warps_per_cta, kSMs * 8), threads, sm, s>>>(
-            list, n, p, capmax);
+      case kTierWarp:
+        k_move_warp<kWarpCap><<<grid_cap((n + 7) / 8, kSMs * 4), 256, (size_t)8 * kWarpCap * 16, s>>>(list, n, p);
         break;
-      }
-      case kTierCta: {
-        const int capmax = (int)pow2_at_least(2 * (int64_t)tc.cta_max);
-        const size_t sm = (size_t)capmax * (sizeof(double) + sizeof(int));
-        NIDO_CUDA_TRY(cudaFuncSetAttribute(k_move_cta<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-        k_move_cta<false><<<grid_cap(n, kSMs * 2), tc.cta_threads, sm, s>>>(list, n, p, capmax, nullptr,
-                                                                            nullptr, 0);
+      case kTierCtaS:
+        k_move_cta<128, kCtaSCap><<<grid_cap(n, kSMs * 8), 128, (size_t)kCtaSCap * 16, s>>>(list, n, p);
         break;
-      }
+      case kTierCtaL:
+        k_move_cta<256, kCtaLCap><<<grid_cap(n, kSMs * 3), 256, (size_t)kCtaLCap * 16, s>>>(list, n, p);
+        break;
       default: {
-        if (g->gslabs <= 0 || (int64_t)pow2_at_least(2 * g->max_degree) > g->gslab)
-          return nido_set_error(NIDO_E_INVALID, "global hash slabs not sized for degree %lld",
-                                (long long)g->max_degree);
-        k_move_cta<true><<<grid_cap(n, g->gslabs), tc.cta_threads, 0, s>>>(list, n, p, 0, g->gkeys,
-                                                                          g->gvals, g->gslab);
+        const int64_t i0 = g->hub_item_off[batch], i1 = g->hub_item_off[batch + 1];
+        if (i1 > i0)
+          k_move_hub<<<grid_cap(i1 - i0, kSMs * 8), kHubThreads, 0, s>>>(
+              reinterpret_cast<const int2*>(g->hub_items) + i0, i1 - i0, g->hub_v, g->hub_toff, g->hub_capv,
+              g->hub_nseg, g->hub_done, g->gkeys, g->gvals, p);
         break;
       }
     }

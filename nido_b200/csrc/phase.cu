@@ -241,36 +241,47 @@ __global__ void k_batch_cuts(const int64_t* __restrict__ off, int64_t nv, int nb
   for (int i = 0; i <= nb; ++i) cuts[i] = parts[i];
 }
 
-__device__ __forceinline__ int tier_of(int64_t d, int warp_max, int cta_max) {
+__device__ __forceinline__ int tier_of(int64_t d) {
   if (d <= 4) return kTierG4;
   if (d <= 8) return kTierG8;
   if (d <= 16) return kTierG16;
   if (d <= 32) return kTierG32;
-  if (d <= warp_max) return kTierWarp;
-  if (d <= cta_max) return kTierCta;
-  return kTierGlobal;
+  if (d <= kWarpMaxDeg) return kTierWarp;
+  if (d <= kCtaSMaxDeg) return kTierCtaS;
+  if (d <= kCtaLMaxDeg) return kTierCtaL;
+  return kTierHub;
 }
 
 // key = tier * nb + batch, so every (tier, batch) range and every tier over
-// all batches is contiguous after the stable sort.
+// all batches is contiguous after the stable sort.  Counts and the maximum
+// degree are aggregated per warp before the global atomics.
 __global__ void k_tier_keys(const int64_t* __restrict__ off, int64_t nv, const int64_t* __restrict__ cuts,
-                            int nb, int warp_max, int cta_max, uint32_t* __restrict__ keys,
-                            uint32_t* __restrict__ vals, int64_t* __restrict__ counts,
-                            unsigned long long* __restrict__ maxdeg) {
-  for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < nv;
-       v += (int64_t)gridDim.x * blockDim.x) {
-    int lo = 0, hi = nb;  // batch b with cuts[b] <= v < cuts[b+1]
-    while (hi - lo > 1) {
-      const int mid = (lo + hi) / 2;
-      if (cuts[mid] <= v) lo = mid; else hi = mid;
+                            int nb, uint32_t* __restrict__ keys, uint32_t* __restrict__ vals,
+                            int64_t* __restrict__ counts, unsigned long long* __restrict__ maxdeg) {
+  const int lane = threadIdx.x & 31;
+  unsigned long long md = 0;
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t base = blockIdx.x * (int64_t)blockDim.x; base < nv; base += stride) {
+    const int64_t v = base + threadIdx.x;
+    uint32_t key = 0xffffffffu;
+    if (v < nv) {
+      int lo = 0, hi = nb;  // batch b with cuts[b] <= v < cuts[b+1]
+      while (hi - lo > 1) {
+        const int mid = (lo + hi) / 2;
+        if (cuts[mid] <= v) lo = mid; else hi = mid;
+      }
+      const int64_t d = off[v + 1] - off[v];
+      key = (uint32_t)(tier_of(d) * nb + lo);
+      keys[v] = key;
+      vals[v] = (uint32_t)v;
+      md = md > (unsigned long long)d ? md : (unsigned long long)d;
     }
-    const int64_t d = off[v + 1] - off[v];
-    const uint32_t key = (uint32_t)(tier_of(d, warp_max, cta_max) * nb + lo);
-    keys[v] = key;
-    vals[v] = (uint32_t)v;
-    atomicAdd((unsigned long long*)&counts[key], 1ull);
-    atomicMax(maxdeg, (unsigned long long)d);
+    const unsigned peers = __match_any_sync(NIDO_FULL_MASK, key);
+    if (key != 0xffffffffu && lane == __ffs(peers) - 1)
+      atomicAdd((unsigned long long*)&counts[key], (unsigned long long)__popc(peers));
   }
+  md = __reduce_max_sync(NIDO_FULL_MASK, (unsigned)md);
+  if (lane == 0 && md) atomicMax(maxdeg, md);
 }
 
 }  // namespace
@@ -352,10 +363,11 @@ int launch_modularity(nido_graph_s* g, double* q) {
         break;
       case kTierG32:
       case kTierWarp:
+      case kTierCtaS:
         k_q_self_group<32><<<grid_for(n, kThreads / 32), kThreads, 0, s>>>(list, n, g->off, g->adj, g->w, g->comm, selfv);
         break;
       default:
-        k_q_self_cta<512><<<grid_for(n, 1, 148 * 4), 512, 0, s>>>(list, n, g->off, g->adj, g->w, g->comm, selfv);
+        k_q_self_cta<256><<<grid_for(n, 1, 148 * 8), 256, 0, s>>>(list, n, g->off, g->adj, g->w, g->comm, selfv);
         break;
     }
     NIDO_LAUNCH_CHECK();
@@ -390,8 +402,7 @@ int build_batches(nido_graph_s* g) {
   NIDO_CUDA_TRY(cudaMemsetAsync(counts, 0, sizeof(int64_t) * (nkeys + 1), s));
   NIDO_CUDA_TRY(cudaMemsetAsync(maxdeg, 0, sizeof(unsigned long long), s));
   if (nv > 0) {
-    k_tier_keys<<<grid_for(nv, kThreads), kThreads, 0, s>>>(g->off, nv, dcuts, nb, g->ctx->tiers.warp_max,
-                                                           g->ctx->tiers.cta_max, keys, (uint32_t*)g->perm,
+    k_tier_keys<<<grid_for(nv, kThreads), kThreads, 0, s>>>(g->off, nv, dcuts, nb, keys, (uint32_t*)g->perm,
                                                            counts, maxdeg);
     NIDO_LAUNCH_CHECK();
     int bits = 0;
@@ -408,7 +419,7 @@ int build_batches(nido_graph_s* g) {
   NIDO_CUDA_TRY(cudaStreamSynchronize(s));
   g->max_degree = (int64_t)md;
   g->bins_valid = true;
-  return NIDO_OK;
+  return plan_hubs(g);
 }
 
 }  // namespace nido
