@@ -579,12 +579,19 @@ int launch_aggregation(nido_graph_s* g, int* done) {
     }
     first[n2] = (int64_t)items.size();
     const int64_t ni = (int64_t)items.size();
-    char* buf = nullptr;
     const size_t bytes = sizeof(int2) * ni + sizeof(int32_t) * 2 * n2 + sizeof(int64_t) * (2 * n2 + 1) +
                          sizeof(int64_t) * (ni + 1) + sizeof(int64_t) * scan_temp_elems(ni) +
-                         (sizeof(int32_t) * 2 + sizeof(double)) * slots + 8 * 256;
-    NIDO_CUDA_TRY(cudaMallocAsync((void**)&buf, bytes, s));
-    Arena pa(buf, bytes);
+                         (sizeof(int32_t) * 2 + sizeof(double)) * slots + 16 * 256;
+    if (bytes > g->agg_buf_bytes) {
+      NIDO_CUDA_TRY(cudaStreamSynchronize(s));
+      if (g->agg_buf) cudaFree(g->agg_buf);
+      g->agg_buf = nullptr;
+      g->agg_buf_bytes = 0;
+      const size_t want = bytes + bytes / 4;
+      NIDO_CUDA_TRY(cudaMalloc((void**)&g->agg_buf, want));
+      g->agg_buf_bytes = want;
+    }
+    Arena pa(g->agg_buf, g->agg_buf_bytes);
     int2* ditems = pa.take<int2>(ni);
     int32_t* dcids = pa.take<int32_t>(n2);
     int32_t* dcaps = pa.take<int32_t>(n2);
@@ -615,7 +622,6 @@ int launch_aggregation(nido_graph_s* g, int* done) {
     k_agg_seg_deg<<<grid_for(n2, 256, kSMs * 4), 256, 0, s>>>(n2, dcids, dfirst, segcnt, degp);
     NIDO_LAUNCH_CHECK();
     NIDO_CUDA_TRY(cudaStreamSynchronize(s));  // the host plan vectors go out of scope
-    NIDO_CUDA_TRY(cudaFreeAsync(buf, s));
   }
   // coarse offsets into off2, then the entries into the work CSR (when the
   // current graph is the work CSR, its lists are dead once pass 1 is done)

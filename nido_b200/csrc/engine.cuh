@@ -98,6 +98,18 @@ struct nido_graph_s {
           hub_cap_hubs_t = 0, hub_cap_hubs_d = 0;
   int64_t nhubs = 0;
   std::vector<int64_t> hub_item_off;  // items per batch
+  // table slices scanned in parallel, their per-slice results, and the hub
+  // index range of every batch
+  int2* hub_slices = nullptr;
+  int64_t* hub_slice_first = nullptr;
+  char* hub_res = nullptr;
+  int64_t hub_cap_slices = 0, hub_cap_first = 0, hub_cap_res = 0;
+  std::vector<int64_t> hub_slice_off;
+  std::vector<int64_t> hub_off_b;
+  // coarsening plan and tables of giant coarse vertices (grows, never shrinks,
+  // so runs after the first allocate nothing)
+  char* agg_buf = nullptr;
+  size_t agg_buf_bytes = 0;
 
   std::vector<int64_t> cuts;     // host batch cuts (nbatches+1)
   std::vector<int64_t> tier_off; // host: nbatches*kNumTiers+1 offsets into perm

@@ -484,6 +484,108 @@ __global__ void __launch_bounds__(kHubThreads) k_move_hub(const int2* __restrict
   }
 }
 
+// Fast path for the smallest-id rule: segments only merge (k_hub_insert),
+// then every kHubSlice-slot slice of a table is scanned and cleared by its
+// own CTA (k_hub_slices), and one warp per hub combines the slice results
+// (k_hub_combine).  The reference's tie rule needs ranks over the whole
+// table and uses k_move_hub instead.
+constexpr int kHubSlice = 4096;
+
+__global__ void __launch_bounds__(kHubThreads) k_hub_insert(const int2* __restrict__ items, int64_t n,
+                                                            const int32_t* __restrict__ hub_v,
+                                                            const int64_t* __restrict__ hub_toff,
+                                                            const int32_t* __restrict__ hub_cap, int32_t* gkeys,
+                                                            double* gvals, MoveArgs p) {
+  const int wid = threadIdx.x >> 5;
+  for (int64_t it = blockIdx.x; it < n; it += gridDim.x) {
+    const int2 item = items[it];
+    const int h = item.x;
+    const int v = hub_v[h];
+    Table t;
+    t.keys = gkeys + hub_toff[h];
+    t.vals = gvals + hub_toff[h];
+    t.occ = nullptr;
+    t.nocc = nullptr;
+    t.mask = (unsigned)hub_cap[h] - 1;
+    const int64_t s = p.off[v], eend = p.off[v + 1];
+    const int64_t s0 = s + (int64_t)item.y * kHubSeg;
+    accumulate_edges<true>(p, v, s0 + (int64_t)wid * 32, min(eend, s0 + kHubSeg), kHubThreads, t);
+  }
+}
+
+struct SliceResult {
+  double g;
+  double eown;
+  unsigned long long tk;
+  int cand;
+  int pad;
+};
+
+__global__ void __launch_bounds__(kHubThreads) k_hub_slices(const int2* __restrict__ slices, int64_t n,
+                                                            const int32_t* __restrict__ hub_v,
+                                                            const int64_t* __restrict__ hub_toff,
+                                                            const int32_t* __restrict__ hub_cap,
+                                                            int32_t* gkeys, double* gvals, MoveArgs p,
+                                                            SliceResult* __restrict__ res) {
+  __shared__ double sg[32];
+  __shared__ unsigned long long stk[32];
+  __shared__ int sc[32];
+  for (int64_t it = blockIdx.x; it < n; it += gridDim.x) {
+    const int2 sl = slices[it];
+    const int v = hub_v[sl.x];
+    int* keys = gkeys + hub_toff[sl.x] + (int64_t)sl.y * kHubSlice;
+    double* vals = gvals + hub_toff[sl.x] + (int64_t)sl.y * kHubSlice;
+    const int len = min(kHubSlice, hub_cap[sl.x] - sl.y * kHubSlice);
+    const int own = p.comm[v];
+    const double ki = p.k[v];
+    double g = -NIDO_MAX_FLOAT, eown = 0.;
+    unsigned long long tk = kNoKey;
+    int cand = -1;
+    for (int i = threadIdx.x; i < len; i += kHubThreads) {
+      const int cc = keys[i];
+      if (cc < 0) continue;
+      const double val = vals[i];
+      keys[i] = -1;
+      vals[i] = 0.;
+      if (cc == own) {
+        eown = val;
+      } else {
+        const double gg = gain_of(val, ki, p.a[cc], p.m);
+        if (better(gg, (unsigned)cc, g, tk)) { g = gg; tk = (unsigned)cc; cand = cc; }
+      }
+    }
+    eown = block_sum(eown, sg);
+    block_best(g, tk, cand, sg, stk, sc);
+    if (threadIdx.x == 0) res[it] = SliceResult{g, eown, tk, cand, 0};
+  }
+}
+
+__global__ void k_hub_combine(int64_t nh, const int32_t* __restrict__ hub_v, const int64_t* __restrict__ slice_first,
+                              const SliceResult* __restrict__ res, MoveArgs p) {
+  const int lane = threadIdx.x & 31;
+  const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t h = warp; h < nh; h += nw) {
+    const int64_t r0 = slice_first[h], r1 = slice_first[h + 1];
+    if (r1 == r0) continue;  // hub of another batch
+    double g = -NIDO_MAX_FLOAT, eown = 0.;
+    unsigned long long tk = kNoKey;
+    int cand = -1;
+    for (int64_t r = r0 + lane; r < r1; r += 32) {
+      const SliceResult x = res[r];
+      eown += x.eown;
+      if (better(x.g, x.tk, g, tk)) { g = x.g; tk = x.tk; cand = x.cand; }
+    }
+    eown = group_sum<32>(eown);
+    group_best<32>(g, tk, cand);
+    if (lane == 0) {
+      const int v = hub_v[h];
+      const int own = p.comm[v];
+      decide(p, v, own, p.k[v], p.a[own], eown, g, cand);
+    }
+  }
+}
+
 __global__ void k_hub_degrees(const int32_t* __restrict__ list, int64_t n, const int64_t* __restrict__ off,
                               int64_t* __restrict__ out) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
@@ -545,13 +647,24 @@ int plan_hubs(nido_graph_s* g) {
     toff += cap;
     hseg[i] = (int32_t)((d + kHubSeg - 1) / kHubSeg);
   }
-  // items grouped by batch: hubs are listed by batch within the tier
+  // items grouped by batch: hubs are listed by batch within the tier; the
+  // table slices of every hub follow one another
+  std::vector<int2> slices;
+  std::vector<int64_t> sfirst(nh + 1, 0);
+  g->hub_slice_off.assign(nb + 1, 0);
+  g->hub_off_b.assign(nb + 1, 0);
   for (int b = 0; b < nb; ++b) {
     const int64_t a0 = g->tier_off[(size_t)kTierHub * nb + b] - h0;
     const int64_t a1 = g->tier_off[(size_t)kTierHub * nb + b + 1] - h0;
-    for (int64_t i = a0; i < a1; ++i)
+    for (int64_t i = a0; i < a1; ++i) {
       for (int sgi = 0; sgi < hseg[i]; ++sgi) items.push_back(make_int2((int)i, sgi));
+      sfirst[i] = (int64_t)slices.size();
+      for (int sl = 0; sl * kHubSlice < hcap[i]; ++sl) slices.push_back(make_int2((int)i, sl));
+      sfirst[i + 1] = (int64_t)slices.size();
+    }
     g->hub_item_off[b + 1] = (int64_t)items.size();
+    g->hub_slice_off[b + 1] = (int64_t)slices.size();
+    g->hub_off_b[b + 1] = a1;
   }
   NIDO_TRY(ensure(g, &g->hub_v, &g->hub_cap_hubs_v, nh));
   NIDO_TRY(ensure(g, &g->hub_capv, &g->hub_cap_hubs_c, nh));
@@ -559,6 +672,11 @@ int plan_hubs(nido_graph_s* g) {
   NIDO_TRY(ensure(g, &g->hub_toff, &g->hub_cap_hubs_t, nh));
   NIDO_TRY(ensure(g, &g->hub_done, &g->hub_cap_hubs_d, nh));
   NIDO_TRY(ensure(g, &g->hub_items, &g->hub_cap_items, (int64_t)items.size()));
+  NIDO_TRY(ensure(g, &g->hub_slices, &g->hub_cap_slices, (int64_t)slices.size()));
+  NIDO_TRY(ensure(g, &g->hub_slice_first, &g->hub_cap_first, nh + 1));
+  NIDO_TRY(ensure(g, &g->hub_res, &g->hub_cap_res, (int64_t)(slices.size() * sizeof(SliceResult))));
+  NIDO_CUDA_TRY(cudaMemcpyAsync(g->hub_slices, slices.data(), sizeof(int2) * slices.size(), cudaMemcpyHostToDevice, s));
+  NIDO_CUDA_TRY(cudaMemcpyAsync(g->hub_slice_first, sfirst.data(), sizeof(int64_t) * (nh + 1), cudaMemcpyHostToDevice, s));
   if (toff > g->gslab) {
     if (g->gkeys) cudaFree(g->gkeys);
     if (g->gvals) cudaFree(g->gvals);
@@ -638,10 +756,24 @@ int launch_move(nido_graph_s* g, int batch, int tie, cudaEvent_t ev_start, cudaE
         break;
       default: {
         const int64_t i0 = g->hub_item_off[batch], i1 = g->hub_item_off[batch + 1];
-        if (i1 > i0)
+        if (i1 <= i0) break;
+        const int2* items = g->hub_items + i0;
+        if (tie == NIDO_TIE_NIDO) {
           k_move_hub<<<grid_cap(i1 - i0, kSMs * 8), kHubThreads, 0, s>>>(
-              reinterpret_cast<const int2*>(g->hub_items) + i0, i1 - i0, g->hub_v, g->hub_toff, g->hub_capv,
-              g->hub_nseg, g->hub_done, g->gkeys, g->gvals, p);
+              items, i1 - i0, g->hub_v, g->hub_toff, g->hub_capv, g->hub_nseg, g->hub_done, g->gkeys, g->gvals, p);
+          break;
+        }
+        k_hub_insert<<<grid_cap(i1 - i0, kSMs * 8), kHubThreads, 0, s>>>(items, i1 - i0, g->hub_v, g->hub_toff,
+                                                                        g->hub_capv, g->gkeys, g->gvals, p);
+        NIDO_LAUNCH_CHECK();
+        const int64_t s0 = g->hub_slice_off[batch], s1 = g->hub_slice_off[batch + 1];
+        SliceResult* res = reinterpret_cast<SliceResult*>(g->hub_res);
+        k_hub_slices<<<grid_cap(s1 - s0, kSMs * 8), kHubThreads, 0, s>>>(
+            g->hub_slices + s0, s1 - s0, g->hub_v, g->hub_toff, g->hub_capv, g->gkeys, g->gvals, p, res + s0);
+        NIDO_LAUNCH_CHECK();
+        const int64_t hb0 = g->hub_off_b[batch], hb1 = g->hub_off_b[batch + 1];
+        k_hub_combine<<<grid_cap((hb1 - hb0 + 7) / 8, kSMs * 4), 256, 0, s>>>(hb1 - hb0, g->hub_v + hb0,
+                                                                              g->hub_slice_first + hb0, res, p);
         break;
       }
     }
