@@ -184,30 +184,42 @@ struct Table {
   unsigned mask;
 };
 
+// Adds e to key c's value, inserting c when absent; returns the slot and
+// whether this call inserted it.
 template <bool kAtomicVals>
-__device__ __forceinline__ void table_add(const Table& t, int c, double e, unsigned long long* err) {
+__device__ __forceinline__ int table_add(const Table& t, int c, double e, bool& isnew, unsigned long long* err) {
   unsigned h = hash_slot(c, t.mask);
   volatile int* vk = t.keys;
+  isnew = false;
   for (unsigned probe = 0; probe <= t.mask; ++probe) {
     const int kk = vk[h];
     bool hit = kk == c;
     if (!hit && kk == -1) {
       const int old = atomicCAS(&t.keys[h], -1, c);
-      if (old == -1) {
-        if (t.occ) t.occ[atomicAdd(t.nocc, 1)] = (int)h;
-        hit = true;
-      } else {
-        hit = old == c;
-      }
+      isnew = old == -1;
+      hit = isnew || old == c;
     }
     if (hit) {
       if (kAtomicVals) atomicAdd(&t.vals[h], e);
       else t.vals[h] += e;
-      return;
+      return (int)h;
     }
     h = (h + 1) & t.mask;
   }
   atomicAdd(err, 1ull);
+  return -1;
+}
+
+// Appends the slots this warp inserted to the occupied list with one atomic
+// per warp.  Every lane of the warp must call it.
+__device__ __forceinline__ void occ_append(const Table& t, bool isnew, int slot) {
+  const unsigned nb = __ballot_sync(NIDO_FULL_MASK, isnew);
+  if (nb == 0u || t.occ == nullptr) return;
+  const int lane = threadIdx.x & 31, leader = __ffs(nb) - 1;
+  int base = 0;
+  if (lane == leader) base = atomicAdd(t.nocc, __popc(nb));
+  base = __shfl_sync(NIDO_FULL_MASK, base, leader);
+  if (isnew) t.occ[base + __popc(nb & lanemask_lt())] = slot;
 }
 
 __device__ __forceinline__ unsigned next_pow2_cap(int64_t d) {
@@ -216,28 +228,46 @@ __device__ __forceinline__ unsigned next_pow2_cap(int64_t d) {
   return c;
 }
 
-// Accumulate the edges [s, eend) of vertex v, one 32-edge chunk per warp step
-// starting at `first` and advancing by `stride` edges.  Every lane of the warp
-// takes part.
-template <bool kAtomicVals>
+// Accumulate the edges [first, eend) of vertex v: the warp takes 32-edge
+// chunks at first, first+stride, ...  kUnroll chunks are loaded (ids, weights,
+// then the communities) before any is merged, so each warp keeps several
+// dependent gathers in flight.  Chunks are merged in order.  Every lane of the
+// warp takes part.
+template <bool kAtomicVals, int kUnroll>
 __device__ __forceinline__ void accumulate_edges(const MoveArgs& p, int v, int64_t first, int64_t eend,
                                                  int64_t stride, const Table& t) {
   const int lane = threadIdx.x & 31;
-  for (int64_t base = first; base < eend; base += stride) {
-    const int64_t j = base + lane;
-    const bool ok = j < eend;
-    int c = -1;
-    double wt = 0.;
-    if (ok) {
-      const int u = p.adj[j];
-      c = p.comm[u];
-      wt = (u == v) ? 0. : p.w[j];
+  for (int64_t base = first; base < eend; base += kUnroll * stride) {
+    int u[kUnroll], c[kUnroll];
+    double wt[kUnroll];
+#pragma unroll
+    for (int k = 0; k < kUnroll; ++k) {
+      const int64_t j = base + k * stride + lane;
+      u[k] = -1;
+      wt[k] = 0.;
+      if (j < eend) {
+        u[k] = p.adj[j];
+        wt[k] = p.w[j];
+      }
     }
-    const unsigned peers = __match_any_sync(NIDO_FULL_MASK, c);
-    const bool lead = ok && lane == __ffs(peers) - 1;
-    const double e = fold_peers(peers, ok, wt);
-    if (lead) table_add<kAtomicVals>(t, c, e, p.err);
-    if (!kAtomicVals) __syncwarp();
+#pragma unroll
+    for (int k = 0; k < kUnroll; ++k) {
+      c[k] = u[k] >= 0 ? p.comm[u[k]] : -1;
+      if (u[k] == v) wt[k] = 0.;
+    }
+#pragma unroll
+    for (int k = 0; k < kUnroll; ++k) {
+      const bool ok = u[k] >= 0;
+      if (!__any_sync(NIDO_FULL_MASK, ok)) break;
+      const unsigned peers = __match_any_sync(NIDO_FULL_MASK, c[k]);
+      const bool lead = ok && lane == __ffs(peers) - 1;
+      const double e = fold_peers(peers, ok, wt[k]);
+      bool isnew = false;
+      int slot = -1;
+      if (lead) slot = table_add<kAtomicVals>(t, c[k], e, isnew, p.err);
+      occ_append(t, isnew, slot);
+      if (!kAtomicVals) __syncwarp();
+    }
   }
 }
 
@@ -312,7 +342,7 @@ __global__ void __launch_bounds__(256) k_move_warp(const int32_t* __restrict__ l
     t.mask = min((unsigned)kCap, next_pow2_cap(eend - s)) - 1;
     const int own = p.comm[v];
     const double ki = p.k[v], aown = p.a[own];
-    accumulate_edges<false>(p, v, s, eend, 32, t);
+    accumulate_edges<false, 4>(p, v, s, eend, 32, t);
     const int nu = *t.nocc;
     double g = -NIDO_MAX_FLOAT, eown = 0.;
     unsigned long long tk = kNoKey;
@@ -417,7 +447,7 @@ __global__ void __launch_bounds__(kThreads) k_move_cta(const int32_t* __restrict
     t.mask = min((unsigned)kCap, next_pow2_cap(eend - s)) - 1;
     const int own = p.comm[v];
     const double ki = p.k[v], aown = p.a[own];
-    accumulate_edges<true>(p, v, s + (int64_t)wid * 32, eend, kThreads, t);
+    accumulate_edges<true, 4>(p, v, s + (int64_t)wid * 32, eend, kThreads, t);
     __syncthreads();
     const int nu = nocc_s;
     block_evaluate(p, t, nu, false, v, own, ki, aown, sg, stk, sc);
@@ -464,7 +494,7 @@ __global__ void __launch_bounds__(kHubThreads) k_move_hub(const int2* __restrict
     const int64_t s = p.off[v], eend = p.off[v + 1];
     const int64_t s0 = s + (int64_t)item.y * kHubSeg;
     const int64_t s1 = min(eend, s0 + kHubSeg);
-    accumulate_edges<true>(p, v, s0 + (int64_t)wid * 32, s1, kHubThreads, t);
+    accumulate_edges<true, 2>(p, v, s0 + (int64_t)wid * 32, s1, kHubThreads, t);
     __threadfence();
     __syncthreads();
     if (threadIdx.x == 0) last_s = atomicAdd(&hub_done[h], 1) == hub_nseg[h] - 1;
@@ -495,7 +525,8 @@ __global__ void __launch_bounds__(kHubThreads) k_hub_insert(const int2* __restri
                                                             const int32_t* __restrict__ hub_v,
                                                             const int64_t* __restrict__ hub_toff,
                                                             const int32_t* __restrict__ hub_cap, int32_t* gkeys,
-                                                            double* gvals, MoveArgs p) {
+                                                            double* gvals, int32_t* gocc, int32_t* hub_nocc,
+                                                            MoveArgs p) {
   const int wid = threadIdx.x >> 5;
   for (int64_t it = blockIdx.x; it < n; it += gridDim.x) {
     const int2 item = items[it];
@@ -504,12 +535,12 @@ __global__ void __launch_bounds__(kHubThreads) k_hub_insert(const int2* __restri
     Table t;
     t.keys = gkeys + hub_toff[h];
     t.vals = gvals + hub_toff[h];
-    t.occ = nullptr;
-    t.nocc = nullptr;
+    t.occ = gocc + hub_toff[h];
+    t.nocc = hub_nocc + h;
     t.mask = (unsigned)hub_cap[h] - 1;
     const int64_t s = p.off[v], eend = p.off[v + 1];
     const int64_t s0 = s + (int64_t)item.y * kHubSeg;
-    accumulate_edges<true>(p, v, s0 + (int64_t)wid * 32, min(eend, s0 + kHubSeg), kHubThreads, t);
+    accumulate_edges<true, 4>(p, v, s0 + (int64_t)wid * 32, min(eend, s0 + kHubSeg), kHubThreads, t);
   }
 }
 
@@ -521,11 +552,14 @@ struct SliceResult {
   int pad;
 };
 
+// Slice y of hub x covers entries [y*kHubSlice, (y+1)*kHubSlice) of the hub's
+// occupied list; slices past the list's end have nothing to do.
 __global__ void __launch_bounds__(kHubThreads) k_hub_slices(const int2* __restrict__ slices, int64_t n,
                                                             const int32_t* __restrict__ hub_v,
                                                             const int64_t* __restrict__ hub_toff,
-                                                            const int32_t* __restrict__ hub_cap,
-                                                            int32_t* gkeys, double* gvals, MoveArgs p,
+                                                            const int32_t* __restrict__ hub_nocc,
+                                                            const int32_t* __restrict__ gocc, int32_t* gkeys,
+                                                            double* gvals, MoveArgs p,
                                                             SliceResult* __restrict__ res) {
   __shared__ double sg[32];
   __shared__ unsigned long long stk[32];
@@ -533,20 +567,22 @@ __global__ void __launch_bounds__(kHubThreads) k_hub_slices(const int2* __restri
   for (int64_t it = blockIdx.x; it < n; it += gridDim.x) {
     const int2 sl = slices[it];
     const int v = hub_v[sl.x];
-    int* keys = gkeys + hub_toff[sl.x] + (int64_t)sl.y * kHubSlice;
-    double* vals = gvals + hub_toff[sl.x] + (int64_t)sl.y * kHubSlice;
-    const int len = min(kHubSlice, hub_cap[sl.x] - sl.y * kHubSlice);
+    int* keys = gkeys + hub_toff[sl.x];
+    double* vals = gvals + hub_toff[sl.x];
+    const int* occ = gocc + hub_toff[sl.x];
+    const int i0 = sl.y * kHubSlice;
+    const int i1 = min(hub_nocc[sl.x], i0 + kHubSlice);
     const int own = p.comm[v];
     const double ki = p.k[v];
     double g = -NIDO_MAX_FLOAT, eown = 0.;
     unsigned long long tk = kNoKey;
     int cand = -1;
-    for (int i = threadIdx.x; i < len; i += kHubThreads) {
-      const int cc = keys[i];
-      if (cc < 0) continue;
-      const double val = vals[i];
-      keys[i] = -1;
-      vals[i] = 0.;
+    for (int i = i0 + threadIdx.x; i < i1; i += kHubThreads) {
+      const int slot = occ[i];
+      const int cc = keys[slot];
+      const double val = vals[slot];
+      keys[slot] = -1;
+      vals[slot] = 0.;
       if (cc == own) {
         eown = val;
       } else {
@@ -561,7 +597,7 @@ __global__ void __launch_bounds__(kHubThreads) k_hub_slices(const int2* __restri
 }
 
 __global__ void k_hub_combine(int64_t nh, const int32_t* __restrict__ hub_v, const int64_t* __restrict__ slice_first,
-                              const SliceResult* __restrict__ res, MoveArgs p) {
+                              const SliceResult* __restrict__ res, int32_t* __restrict__ hub_nocc, MoveArgs p) {
   const int lane = threadIdx.x & 31;
   const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
@@ -582,6 +618,7 @@ __global__ void k_hub_combine(int64_t nh, const int32_t* __restrict__ hub_v, con
       const int v = hub_v[h];
       const int own = p.comm[v];
       decide(p, v, own, p.k[v], p.a[own], eown, g, cand);
+      hub_nocc[h] = 0;
     }
   }
 }
@@ -677,14 +714,19 @@ int plan_hubs(nido_graph_s* g) {
   NIDO_TRY(ensure(g, &g->hub_res, &g->hub_cap_res, (int64_t)(slices.size() * sizeof(SliceResult))));
   NIDO_CUDA_TRY(cudaMemcpyAsync(g->hub_slices, slices.data(), sizeof(int2) * slices.size(), cudaMemcpyHostToDevice, s));
   NIDO_CUDA_TRY(cudaMemcpyAsync(g->hub_slice_first, sfirst.data(), sizeof(int64_t) * (nh + 1), cudaMemcpyHostToDevice, s));
+  NIDO_TRY(ensure(g, &g->hub_nocc, &g->hub_cap_nocc, nh));
+  NIDO_CUDA_TRY(cudaMemsetAsync(g->hub_nocc, 0, sizeof(int32_t) * nh, s));
   if (toff > g->gslab) {
     if (g->gkeys) cudaFree(g->gkeys);
     if (g->gvals) cudaFree(g->gvals);
+    if (g->gocc) cudaFree(g->gocc);
     g->gkeys = nullptr;
     g->gvals = nullptr;
+    g->gocc = nullptr;
     g->gslab = 0;
     NIDO_CUDA_TRY(cudaMalloc((void**)&g->gkeys, sizeof(int32_t) * (size_t)toff));
     NIDO_CUDA_TRY(cudaMalloc((void**)&g->gvals, sizeof(double) * (size_t)toff));
+    NIDO_CUDA_TRY(cudaMalloc((void**)&g->gocc, sizeof(int32_t) * (size_t)toff));
     NIDO_CUDA_TRY(cudaMemsetAsync(g->gkeys, 0xff, sizeof(int32_t) * (size_t)toff, s));
     NIDO_CUDA_TRY(cudaMemsetAsync(g->gvals, 0, sizeof(double) * (size_t)toff, s));
     g->gslab = toff;
@@ -700,7 +742,7 @@ int plan_hubs(nido_graph_s* g) {
 }
 
 namespace {
-constexpr int kWarpCap = 512;     // warp tier: degree <= 256
+constexpr int kWarpCap = 256;     // warp tier: degree <= 128
 constexpr int kCtaSCap = 2048;    // 128-thread CTA tier: degree <= 1024
 constexpr int kCtaLCap = 4096;    // 256-thread CTA tier: degree <= 2048
 
@@ -763,17 +805,18 @@ int launch_move(nido_graph_s* g, int batch, int tie, cudaEvent_t ev_start, cudaE
               items, i1 - i0, g->hub_v, g->hub_toff, g->hub_capv, g->hub_nseg, g->hub_done, g->gkeys, g->gvals, p);
           break;
         }
-        k_hub_insert<<<grid_cap(i1 - i0, kSMs * 8), kHubThreads, 0, s>>>(items, i1 - i0, g->hub_v, g->hub_toff,
-                                                                        g->hub_capv, g->gkeys, g->gvals, p);
+        k_hub_insert<<<grid_cap(i1 - i0, kSMs * 8), kHubThreads, 0, s>>>(
+            items, i1 - i0, g->hub_v, g->hub_toff, g->hub_capv, g->gkeys, g->gvals, g->gocc, g->hub_nocc, p);
         NIDO_LAUNCH_CHECK();
         const int64_t s0 = g->hub_slice_off[batch], s1 = g->hub_slice_off[batch + 1];
         SliceResult* res = reinterpret_cast<SliceResult*>(g->hub_res);
         k_hub_slices<<<grid_cap(s1 - s0, kSMs * 8), kHubThreads, 0, s>>>(
-            g->hub_slices + s0, s1 - s0, g->hub_v, g->hub_toff, g->hub_capv, g->gkeys, g->gvals, p, res + s0);
+            g->hub_slices + s0, s1 - s0, g->hub_v, g->hub_toff, g->hub_nocc, g->gocc, g->gkeys, g->gvals, p,
+            res + s0);
         NIDO_LAUNCH_CHECK();
         const int64_t hb0 = g->hub_off_b[batch], hb1 = g->hub_off_b[batch + 1];
-        k_hub_combine<<<grid_cap((hb1 - hb0 + 7) / 8, kSMs * 4), 256, 0, s>>>(hb1 - hb0, g->hub_v + hb0,
-                                                                              g->hub_slice_first + hb0, res, p);
+        k_hub_combine<<<grid_cap((hb1 - hb0 + 7) / 8, kSMs * 4), 256, 0, s>>>(
+            hb1 - hb0, g->hub_v + hb0, g->hub_slice_first + hb0, res, g->hub_nocc + hb0, p);
         break;
       }
     }
