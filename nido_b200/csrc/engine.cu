@@ -170,8 +170,7 @@ extern "C" int nido_graph_free(nido_graph g) {
   // hub-tier buffers are sized per phase outside the budget accounting
   for (void* p : {(void*)g->gkeys, (void*)g->gvals, (void*)g->hub_items, (void*)g->hub_v, (void*)g->hub_capv,
                   (void*)g->hub_nseg, (void*)g->hub_toff, (void*)g->hub_done, (void*)g->hub_slices,
-                  (void*)g->hub_slice_first, (void*)g->hub_res, (void*)g->agg_buf, (void*)g->gocc,
-                  (void*)g->hub_nocc})
+                  (void*)g->hub_slice_first, (void*)g->hub_res, (void*)g->agg_buf})
     if (p) cudaFree(p);
   delete g;
   return NIDO_OK;

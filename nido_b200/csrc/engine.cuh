@@ -25,7 +25,8 @@ enum Tier {
   kTierG16,     // d <= 16  : 16-lane group
   kTierG32,     // d <= 32  : one warp, registers
   kTierWarp,    // d <= 128  : one warp, shared-memory hash (256 slots)
-  kTierCtaS,    // d <= 1024 : one 128-thread CTA, shared-memory hash (2048 slots)
+  kTierCtaS,    // d <= 512  : one 128-thread CTA, shared-memory hash (1024 slots)
+  kTierCtaM,    // d <= 1024 : one 256-thread CTA, shared-memory hash (2048 slots)
   kTierCtaL,    // d <= 2048 : one 256-thread CTA, shared-memory hash (4096 slots)
   kTierHub,     // larger    : 2048-edge segments on many CTAs, hash in global memory (L2)
   kNumTiers
@@ -33,7 +34,8 @@ enum Tier {
 
 // degree bounds of the tiers (the shared-memory table sizes are fixed by them)
 constexpr int kWarpMaxDeg = 128;
-constexpr int kCtaSMaxDeg = 1024;
+constexpr int kCtaSMaxDeg = 512;
+constexpr int kCtaMMaxDeg = 1024;
 constexpr int kCtaLMaxDeg = 2048;
 
 struct nido_ctx_s {
@@ -87,9 +89,6 @@ struct nido_graph_s {
   // in all) and (hub, segment) work items, planned once per phase
   int32_t* gkeys = nullptr;
   double* gvals = nullptr;
-  int32_t* gocc = nullptr;       // occupied-slot lists of the hub tables
-  int32_t* hub_nocc = nullptr;   // list lengths (reset after every sweep)
-  int64_t hub_cap_nocc = 0;
   int64_t gslab = 0;
   int2* hub_items = nullptr;
   int32_t* hub_v = nullptr;

@@ -273,19 +273,36 @@ __device__ __forceinline__ void accumulate_edges(const MoveArgs& p, int v, int64
 
 // Scan entries i = t0, t0+step, ... of the occupied list (or of all slots when
 // occ is null): e_own and the best (gain, tie key, community) of this thread.
+// Entries are taken four at a time so that their a_c gathers are in flight
+// together.
 __device__ __forceinline__ void scan_entries(const MoveArgs& p, const Table& t, int n, int t0, int step,
                                              int own, double ki, bool cg, double& eown, double& g,
                                              unsigned long long& tk, int& cand) {
-  for (int i = t0; i < n; i += step) {
-    const int slot = t.occ ? t.occ[i] : i;
-    const int cc = cg ? __ldcg(&t.keys[slot]) : t.keys[slot];
-    if (cc < 0) continue;
-    const double val = cg ? __ldcg(&t.vals[slot]) : t.vals[slot];
-    if (cc == own) {
-      eown = val;
-    } else {
-      const double gg = gain_of(val, ki, p.a[cc], p.m);
-      if (better(gg, (unsigned)cc, g, tk)) { g = gg; tk = (unsigned)cc; cand = cc; }
+  constexpr int U = 4;
+  for (int i = t0; i < n; i += U * step) {
+    int cc[U];
+    double val[U], ac[U];
+#pragma unroll
+    for (int k = 0; k < U; ++k) {
+      const int ii = i + k * step;
+      cc[k] = -1;
+      if (ii < n) {
+        const int slot = t.occ ? t.occ[ii] : ii;
+        cc[k] = cg ? __ldcg(&t.keys[slot]) : t.keys[slot];
+        val[k] = cg ? __ldcg(&t.vals[slot]) : t.vals[slot];
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < U; ++k) ac[k] = (cc[k] >= 0 && cc[k] != own) ? p.a[cc[k]] : 0.;
+#pragma unroll
+    for (int k = 0; k < U; ++k) {
+      if (cc[k] < 0) continue;
+      if (cc[k] == own) {
+        eown = val[k];
+      } else {
+        const double gg = gain_of(val[k], ki, ac[k], p.m);
+        if (better(gg, (unsigned)cc[k], g, tk)) { g = gg; tk = (unsigned)cc[k]; cand = cc[k]; }
+      }
     }
   }
 }
@@ -415,13 +432,28 @@ __device__ __forceinline__ void block_evaluate(const MoveArgs& p, const Table& t
   unsigned long long tk = kNoKey;
   int cand = -1;
   scan_entries(p, t, n, threadIdx.x, blockDim.x, own, ki, cg, eown, g, tk, cand);
-  eown = block_sum(eown, sg);
   if (p.tie == NIDO_TIE_NIDO) {
+    eown = block_sum(eown, sg);
     const double gm = block_max(g, sg);
     nido_tie_entries(p, t, n, threadIdx.x, blockDim.x, own, ki, gm, cg, g, tk, cand);
   }
-  block_best(g, tk, cand, sg, stk, sc);
-  if (threadIdx.x == 0) decide(p, v, own, ki, aown, eown, g, cand);
+  // one reduction for the best entry and e_own (e_own is nonzero in one
+  // thread at most, so its sum is exact in any order)
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  if (p.tie != NIDO_TIE_NIDO) eown = group_sum<32>(eown);
+  group_best<32>(g, tk, cand);
+  __shared__ double se[32];
+  if (lane == 0) { sg[wid] = g; stk[wid] = tk; sc[wid] = cand; se[wid] = eown; }
+  __syncthreads();
+  if (wid == 0) {
+    g = lane < nw ? sg[lane] : -NIDO_MAX_FLOAT;
+    tk = lane < nw ? stk[lane] : kNoKey;
+    cand = lane < nw ? sc[lane] : -1;
+    double e2 = lane < nw ? se[lane] : 0.;
+    group_best<32>(g, tk, cand);
+    e2 = group_sum<32>(e2);
+    if (lane == 0) decide(p, v, own, ki, aown, p.tie == NIDO_TIE_NIDO ? eown : e2, g, cand);
+  }
 }
 
 // ---- 256 < degree <= 2048: one CTA per vertex, table in shared memory ----------
@@ -450,14 +482,15 @@ __global__ void __launch_bounds__(kThreads) k_move_cta(const int32_t* __restrict
     accumulate_edges<true, 4>(p, v, s + (int64_t)wid * 32, eend, kThreads, t);
     __syncthreads();
     const int nu = nocc_s;
+    // block_evaluate ends with a barrier that every thread reaches after
+    // reading nu, so the count can be reset right after it
     block_evaluate(p, t, nu, false, v, own, ki, aown, sg, stk, sc);
+    if (threadIdx.x == 0) nocc_s = 0;
     for (int i = threadIdx.x; i < nu; i += kThreads) {
       const int slot = t.occ[i];
       t.keys[slot] = -1;
       t.vals[slot] = 0.;
     }
-    __syncthreads();
-    if (threadIdx.x == 0) nocc_s = 0;
     __syncthreads();
   }
 }
@@ -525,8 +558,7 @@ __global__ void __launch_bounds__(kHubThreads) k_hub_insert(const int2* __restri
                                                             const int32_t* __restrict__ hub_v,
                                                             const int64_t* __restrict__ hub_toff,
                                                             const int32_t* __restrict__ hub_cap, int32_t* gkeys,
-                                                            double* gvals, int32_t* gocc, int32_t* hub_nocc,
-                                                            MoveArgs p) {
+                                                            double* gvals, MoveArgs p) {
   const int wid = threadIdx.x >> 5;
   for (int64_t it = blockIdx.x; it < n; it += gridDim.x) {
     const int2 item = items[it];
@@ -535,8 +567,8 @@ __global__ void __launch_bounds__(kHubThreads) k_hub_insert(const int2* __restri
     Table t;
     t.keys = gkeys + hub_toff[h];
     t.vals = gvals + hub_toff[h];
-    t.occ = gocc + hub_toff[h];
-    t.nocc = hub_nocc + h;
+    t.occ = nullptr;
+    t.nocc = nullptr;
     t.mask = (unsigned)hub_cap[h] - 1;
     const int64_t s = p.off[v], eend = p.off[v + 1];
     const int64_t s0 = s + (int64_t)item.y * kHubSeg;
@@ -552,13 +584,13 @@ struct SliceResult {
   int pad;
 };
 
-// Slice y of hub x covers entries [y*kHubSlice, (y+1)*kHubSlice) of the hub's
-// occupied list; slices past the list's end have nothing to do.
+// Slice y of hub x covers slots [y*kHubSlice, (y+1)*kHubSlice) of the hub's
+// table, read and cleared in order (the tables exceed L2, so coalesced
+// access matters more than skipping empty slots).
 __global__ void __launch_bounds__(kHubThreads) k_hub_slices(const int2* __restrict__ slices, int64_t n,
                                                             const int32_t* __restrict__ hub_v,
                                                             const int64_t* __restrict__ hub_toff,
-                                                            const int32_t* __restrict__ hub_nocc,
-                                                            const int32_t* __restrict__ gocc, int32_t* gkeys,
+                                                            const int32_t* __restrict__ hub_cap, int32_t* gkeys,
                                                             double* gvals, MoveArgs p,
                                                             SliceResult* __restrict__ res) {
   __shared__ double sg[32];
@@ -567,22 +599,20 @@ __global__ void __launch_bounds__(kHubThreads) k_hub_slices(const int2* __restri
   for (int64_t it = blockIdx.x; it < n; it += gridDim.x) {
     const int2 sl = slices[it];
     const int v = hub_v[sl.x];
-    int* keys = gkeys + hub_toff[sl.x];
-    double* vals = gvals + hub_toff[sl.x];
-    const int* occ = gocc + hub_toff[sl.x];
-    const int i0 = sl.y * kHubSlice;
-    const int i1 = min(hub_nocc[sl.x], i0 + kHubSlice);
+    int* keys = gkeys + hub_toff[sl.x] + (int64_t)sl.y * kHubSlice;
+    double* vals = gvals + hub_toff[sl.x] + (int64_t)sl.y * kHubSlice;
+    const int len = min(kHubSlice, hub_cap[sl.x] - sl.y * kHubSlice);
     const int own = p.comm[v];
     const double ki = p.k[v];
     double g = -NIDO_MAX_FLOAT, eown = 0.;
     unsigned long long tk = kNoKey;
     int cand = -1;
-    for (int i = i0 + threadIdx.x; i < i1; i += kHubThreads) {
-      const int slot = occ[i];
-      const int cc = keys[slot];
-      const double val = vals[slot];
-      keys[slot] = -1;
-      vals[slot] = 0.;
+    for (int i = threadIdx.x; i < len; i += kHubThreads) {
+      const int cc = keys[i];
+      if (cc < 0) continue;
+      const double val = vals[i];
+      keys[i] = -1;
+      vals[i] = 0.;
       if (cc == own) {
         eown = val;
       } else {
@@ -597,7 +627,7 @@ __global__ void __launch_bounds__(kHubThreads) k_hub_slices(const int2* __restri
 }
 
 __global__ void k_hub_combine(int64_t nh, const int32_t* __restrict__ hub_v, const int64_t* __restrict__ slice_first,
-                              const SliceResult* __restrict__ res, int32_t* __restrict__ hub_nocc, MoveArgs p) {
+                              const SliceResult* __restrict__ res, MoveArgs p) {
   const int lane = threadIdx.x & 31;
   const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
@@ -618,7 +648,6 @@ __global__ void k_hub_combine(int64_t nh, const int32_t* __restrict__ hub_v, con
       const int v = hub_v[h];
       const int own = p.comm[v];
       decide(p, v, own, p.k[v], p.a[own], eown, g, cand);
-      hub_nocc[h] = 0;
     }
   }
 }
@@ -714,19 +743,14 @@ int plan_hubs(nido_graph_s* g) {
   NIDO_TRY(ensure(g, &g->hub_res, &g->hub_cap_res, (int64_t)(slices.size() * sizeof(SliceResult))));
   NIDO_CUDA_TRY(cudaMemcpyAsync(g->hub_slices, slices.data(), sizeof(int2) * slices.size(), cudaMemcpyHostToDevice, s));
   NIDO_CUDA_TRY(cudaMemcpyAsync(g->hub_slice_first, sfirst.data(), sizeof(int64_t) * (nh + 1), cudaMemcpyHostToDevice, s));
-  NIDO_TRY(ensure(g, &g->hub_nocc, &g->hub_cap_nocc, nh));
-  NIDO_CUDA_TRY(cudaMemsetAsync(g->hub_nocc, 0, sizeof(int32_t) * nh, s));
   if (toff > g->gslab) {
     if (g->gkeys) cudaFree(g->gkeys);
     if (g->gvals) cudaFree(g->gvals);
-    if (g->gocc) cudaFree(g->gocc);
     g->gkeys = nullptr;
     g->gvals = nullptr;
-    g->gocc = nullptr;
     g->gslab = 0;
     NIDO_CUDA_TRY(cudaMalloc((void**)&g->gkeys, sizeof(int32_t) * (size_t)toff));
     NIDO_CUDA_TRY(cudaMalloc((void**)&g->gvals, sizeof(double) * (size_t)toff));
-    NIDO_CUDA_TRY(cudaMalloc((void**)&g->gocc, sizeof(int32_t) * (size_t)toff));
     NIDO_CUDA_TRY(cudaMemsetAsync(g->gkeys, 0xff, sizeof(int32_t) * (size_t)toff, s));
     NIDO_CUDA_TRY(cudaMemsetAsync(g->gvals, 0, sizeof(double) * (size_t)toff, s));
     g->gslab = toff;
@@ -743,7 +767,8 @@ int plan_hubs(nido_graph_s* g) {
 
 namespace {
 constexpr int kWarpCap = 256;     // warp tier: degree <= 128
-constexpr int kCtaSCap = 2048;    // 128-thread CTA tier: degree <= 1024
+constexpr int kCtaSCap = 1024;    // 128-thread CTA tier: degree <= 512
+constexpr int kCtaMCap = 2048;    // 256-thread CTA tier: degree <= 1024
 constexpr int kCtaLCap = 4096;    // 256-thread CTA tier: degree <= 2048
 
 template <typename K>
@@ -756,6 +781,7 @@ int set_smem(K kernel, size_t bytes) {
 int move_init_attributes() {
   NIDO_TRY(set_smem(k_move_warp<kWarpCap>, (size_t)8 * kWarpCap * 16));
   NIDO_TRY(set_smem(k_move_cta<128, kCtaSCap>, (size_t)kCtaSCap * 16));
+  NIDO_TRY(set_smem(k_move_cta<256, kCtaMCap>, (size_t)kCtaMCap * 16));
   NIDO_TRY(set_smem(k_move_cta<256, kCtaLCap>, (size_t)kCtaLCap * 16));
   return NIDO_OK;
 }
@@ -788,10 +814,13 @@ int launch_move(nido_graph_s* g, int batch, int tie, cudaEvent_t ev_start, cudaE
         k_move_group<32><<<grid_cap((n + 7) / 8, kSMs * 16), 256, 0, s>>>(list, n, p);
         break;
       case kTierWarp:
-        k_move_warp<kWarpCap><<<grid_cap((n + 7) / 8, kSMs * 4), 256, (size_t)8 * kWarpCap * 16, s>>>(list, n, p);
+        k_move_warp<kWarpCap><<<grid_cap((n + 7) / 8, kSMs * 7), 256, (size_t)8 * kWarpCap * 16, s>>>(list, n, p);
         break;
       case kTierCtaS:
-        k_move_cta<128, kCtaSCap><<<grid_cap(n, kSMs * 8), 128, (size_t)kCtaSCap * 16, s>>>(list, n, p);
+        k_move_cta<128, kCtaSCap><<<grid_cap(n, kSMs * 14), 128, (size_t)kCtaSCap * 16, s>>>(list, n, p);
+        break;
+      case kTierCtaM:
+        k_move_cta<256, kCtaMCap><<<grid_cap(n, kSMs * 7), 256, (size_t)kCtaMCap * 16, s>>>(list, n, p);
         break;
       case kTierCtaL:
         k_move_cta<256, kCtaLCap><<<grid_cap(n, kSMs * 3), 256, (size_t)kCtaLCap * 16, s>>>(list, n, p);
@@ -806,17 +835,17 @@ int launch_move(nido_graph_s* g, int batch, int tie, cudaEvent_t ev_start, cudaE
           break;
         }
         k_hub_insert<<<grid_cap(i1 - i0, kSMs * 8), kHubThreads, 0, s>>>(
-            items, i1 - i0, g->hub_v, g->hub_toff, g->hub_capv, g->gkeys, g->gvals, g->gocc, g->hub_nocc, p);
+            items, i1 - i0, g->hub_v, g->hub_toff, g->hub_capv, g->gkeys, g->gvals, p);
         NIDO_LAUNCH_CHECK();
         const int64_t s0 = g->hub_slice_off[batch], s1 = g->hub_slice_off[batch + 1];
         SliceResult* res = reinterpret_cast<SliceResult*>(g->hub_res);
         k_hub_slices<<<grid_cap(s1 - s0, kSMs * 8), kHubThreads, 0, s>>>(
-            g->hub_slices + s0, s1 - s0, g->hub_v, g->hub_toff, g->hub_nocc, g->gocc, g->gkeys, g->gvals, p,
+            g->hub_slices + s0, s1 - s0, g->hub_v, g->hub_toff, g->hub_capv, g->gkeys, g->gvals, p,
             res + s0);
         NIDO_LAUNCH_CHECK();
         const int64_t hb0 = g->hub_off_b[batch], hb1 = g->hub_off_b[batch + 1];
         k_hub_combine<<<grid_cap((hb1 - hb0 + 7) / 8, kSMs * 4), 256, 0, s>>>(
-            hb1 - hb0, g->hub_v + hb0, g->hub_slice_first + hb0, res, g->hub_nocc + hb0, p);
+            hb1 - hb0, g->hub_v + hb0, g->hub_slice_first + hb0, res, p);
         break;
       }
     }

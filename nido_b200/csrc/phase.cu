@@ -248,6 +248,7 @@ __device__ __forceinline__ int tier_of(int64_t d) {
   if (d <= 32) return kTierG32;
   if (d <= kWarpMaxDeg) return kTierWarp;
   if (d <= kCtaSMaxDeg) return kTierCtaS;
+  if (d <= kCtaMMaxDeg) return kTierCtaM;
   if (d <= kCtaLMaxDeg) return kTierCtaL;
   return kTierHub;
 }
@@ -364,6 +365,7 @@ int launch_modularity(nido_graph_s* g, double* q) {
       case kTierG32:
       case kTierWarp:
       case kTierCtaS:
+      case kTierCtaM:
         k_q_self_group<32><<<grid_for(n, kThreads / 32), kThreads, 0, s>>>(list, n, g->off, g->adj, g->w, g->comm, selfv);
         break;
       default:
