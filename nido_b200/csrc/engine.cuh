@@ -99,15 +99,18 @@ struct nido_graph_s {
   int64_t hub_cap_items = 0, hub_cap_hubs_v = 0, hub_cap_hubs_c = 0, hub_cap_hubs_s = 0,
           hub_cap_hubs_t = 0, hub_cap_hubs_d = 0;
   int64_t nhubs = 0;
-  std::vector<int64_t> hub_item_off;  // items per batch
+  // waves of hubs whose tables fit in L2 together: item, slice and hub ranges
+  struct HubWave {
+    int64_t i0, i1, s0, s1, h0, h1;
+  };
+  std::vector<HubWave> hub_waves;
+  std::vector<int64_t> hub_wave_off;  // waves of each batch
   // table slices scanned in parallel, their per-slice results, and the hub
   // index range of every batch
   int2* hub_slices = nullptr;
   int64_t* hub_slice_first = nullptr;
   char* hub_res = nullptr;
   int64_t hub_cap_slices = 0, hub_cap_first = 0, hub_cap_res = 0;
-  std::vector<int64_t> hub_slice_off;
-  std::vector<int64_t> hub_off_b;
   // coarsening plan and tables of giant coarse vertices (grows, never shrinks,
   // so runs after the first allocate nothing)
   char* agg_buf = nullptr;

@@ -553,6 +553,9 @@ __global__ void __launch_bounds__(kHubThreads) k_move_hub(const int2* __restrict
 // (k_hub_combine).  The reference's tie rule needs ranks over the whole
 // table and uses k_move_hub instead.
 constexpr int kHubSlice = 4096;
+// table slots of one wave of hubs: 4M slots (48 MB of keys and values) leave
+// room in the 126 MB L2 for the streamed adjacency and the gathers
+constexpr int64_t kHubWaveSlots = (int64_t)4 << 20;
 
 __global__ void __launch_bounds__(kHubThreads) k_hub_insert(const int2* __restrict__ items, int64_t n,
                                                             const int32_t* __restrict__ hub_v,
@@ -686,7 +689,8 @@ int plan_hubs(nido_graph_s* g) {
   const int nb = g->nbatches;
   const int64_t h0 = g->tier_off[(size_t)kTierHub * nb], h1 = g->tier_off[(size_t)(kTierHub + 1) * nb];
   const int64_t nh = h1 - h0;
-  g->hub_item_off.assign(nb + 1, 0);
+  g->hub_waves.clear();
+  g->hub_wave_off.assign(nb + 1, 0);
   g->nhubs = nh;
   if (nh == 0) return NIDO_OK;
   cudaStream_t s = g->ctx->stream;
@@ -701,7 +705,6 @@ int plan_hubs(nido_graph_s* g) {
   std::vector<int32_t> hv(nh), hcap(nh), hseg(nh);
   std::vector<int64_t> htoff(nh);
   std::vector<int2> items;
-  int64_t toff = 0;
   for (int64_t i = 0; i < nh; ++i) {
     const int64_t d = h[2 * i + 1];
     const int64_t u = std::min<int64_t>(d, g->nv);
@@ -709,29 +712,42 @@ int plan_hubs(nido_graph_s* g) {
     while (cap < 2 * u) cap <<= 1;
     hv[i] = (int32_t)h[2 * i];
     hcap[i] = (int32_t)cap;
-    htoff[i] = toff;
-    toff += cap;
     hseg[i] = (int32_t)((d + kHubSeg - 1) / kHubSeg);
   }
-  // items grouped by batch: hubs are listed by batch within the tier; the
-  // table slices of every hub follow one another
+  // Hubs are listed by batch within the tier.  Each batch's hubs are cut into
+  // waves whose tables together hold at most kHubWaveSlots slots (so they stay
+  // in L2); table offsets are relative to the wave, and every wave reuses the
+  // same region because its slice scan clears the tables.  Items and table
+  // slices of a hub follow one another.
   std::vector<int2> slices;
   std::vector<int64_t> sfirst(nh + 1, 0);
-  g->hub_slice_off.assign(nb + 1, 0);
-  g->hub_off_b.assign(nb + 1, 0);
+  g->hub_waves.clear();
+  g->hub_wave_off.assign(nb + 1, 0);
+  int64_t maxslots = 0;
   for (int b = 0; b < nb; ++b) {
     const int64_t a0 = g->tier_off[(size_t)kTierHub * nb + b] - h0;
     const int64_t a1 = g->tier_off[(size_t)kTierHub * nb + b + 1] - h0;
+    int64_t wslots = 0;
     for (int64_t i = a0; i < a1; ++i) {
+      if (i == a0 || wslots + hcap[i] > kHubWaveSlots) {
+        g->hub_waves.push_back({(int64_t)items.size(), 0, (int64_t)slices.size(), 0, i, 0});
+        wslots = 0;
+      }
+      htoff[i] = wslots;
+      wslots += hcap[i];
+      maxslots = std::max(maxslots, wslots);
       for (int sgi = 0; sgi < hseg[i]; ++sgi) items.push_back(make_int2((int)i, sgi));
       sfirst[i] = (int64_t)slices.size();
       for (int sl = 0; sl * kHubSlice < hcap[i]; ++sl) slices.push_back(make_int2((int)i, sl));
       sfirst[i + 1] = (int64_t)slices.size();
+      nido_graph_s::HubWave& w = g->hub_waves.back();
+      w.i1 = (int64_t)items.size();
+      w.s1 = (int64_t)slices.size();
+      w.h1 = i + 1;
     }
-    g->hub_item_off[b + 1] = (int64_t)items.size();
-    g->hub_slice_off[b + 1] = (int64_t)slices.size();
-    g->hub_off_b[b + 1] = a1;
+    g->hub_wave_off[b + 1] = (int64_t)g->hub_waves.size();
   }
+  const int64_t toff = maxslots;
   NIDO_TRY(ensure(g, &g->hub_v, &g->hub_cap_hubs_v, nh));
   NIDO_TRY(ensure(g, &g->hub_capv, &g->hub_cap_hubs_c, nh));
   NIDO_TRY(ensure(g, &g->hub_nseg, &g->hub_cap_hubs_s, nh));
@@ -826,27 +842,29 @@ int launch_move(nido_graph_s* g, int batch, int tie, cudaEvent_t ev_start, cudaE
         k_move_cta<256, kCtaLCap><<<grid_cap(n, kSMs * 3), 256, (size_t)kCtaLCap * 16, s>>>(list, n, p);
         break;
       default: {
-        const int64_t i0 = g->hub_item_off[batch], i1 = g->hub_item_off[batch + 1];
-        if (i1 <= i0) break;
-        const int2* items = g->hub_items + i0;
-        if (tie == NIDO_TIE_NIDO) {
-          k_move_hub<<<grid_cap(i1 - i0, kSMs * 8), kHubThreads, 0, s>>>(
-              items, i1 - i0, g->hub_v, g->hub_toff, g->hub_capv, g->hub_nseg, g->hub_done, g->gkeys, g->gvals, p);
-          break;
-        }
-        k_hub_insert<<<grid_cap(i1 - i0, kSMs * 8), kHubThreads, 0, s>>>(
-            items, i1 - i0, g->hub_v, g->hub_toff, g->hub_capv, g->gkeys, g->gvals, p);
-        NIDO_LAUNCH_CHECK();
-        const int64_t s0 = g->hub_slice_off[batch], s1 = g->hub_slice_off[batch + 1];
         SliceResult* res = reinterpret_cast<SliceResult*>(g->hub_res);
-        k_hub_slices<<<grid_cap(s1 - s0, kSMs * 8), kHubThreads, 0, s>>>(
-            g->hub_slices + s0, s1 - s0, g->hub_v, g->hub_toff, g->hub_capv, g->gkeys, g->gvals, p,
-            res + s0);
-        NIDO_LAUNCH_CHECK();
-        const int64_t hb0 = g->hub_off_b[batch], hb1 = g->hub_off_b[batch + 1];
-        k_hub_combine<<<grid_cap((hb1 - hb0 + 7) / 8, kSMs * 4), 256, 0, s>>>(
-            hb1 - hb0, g->hub_v + hb0, g->hub_slice_first + hb0, res, p);
-        break;
+        for (int64_t wv = g->hub_wave_off[batch]; wv < g->hub_wave_off[batch + 1]; ++wv) {
+          const nido_graph_s::HubWave& w = g->hub_waves[wv];
+          const int2* items = g->hub_items + w.i0;
+          if (tie == NIDO_TIE_NIDO) {
+            k_move_hub<<<grid_cap(w.i1 - w.i0, kSMs * 8), kHubThreads, 0, s>>>(
+                items, w.i1 - w.i0, g->hub_v, g->hub_toff, g->hub_capv, g->hub_nseg, g->hub_done, g->gkeys,
+                g->gvals, p);
+            NIDO_LAUNCH_CHECK();
+            continue;
+          }
+          k_hub_insert<<<grid_cap(w.i1 - w.i0, kSMs * 8), kHubThreads, 0, s>>>(
+              items, w.i1 - w.i0, g->hub_v, g->hub_toff, g->hub_capv, g->gkeys, g->gvals, p);
+          NIDO_LAUNCH_CHECK();
+          k_hub_slices<<<grid_cap(w.s1 - w.s0, kSMs * 8), kHubThreads, 0, s>>>(
+              g->hub_slices + w.s0, w.s1 - w.s0, g->hub_v, g->hub_toff, g->hub_capv, g->gkeys, g->gvals, p,
+              res + w.s0);
+          NIDO_LAUNCH_CHECK();
+          k_hub_combine<<<grid_cap((w.h1 - w.h0 + 7) / 8, kSMs * 4), 256, 0, s>>>(
+              w.h1 - w.h0, g->hub_v + w.h0, g->hub_slice_first + w.h0, res, p);
+          NIDO_LAUNCH_CHECK();
+        }
+        continue;
       }
     }
     NIDO_LAUNCH_CHECK();
