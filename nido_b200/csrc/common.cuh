@@ -46,9 +46,12 @@ __device__ __forceinline__ unsigned lanemask_lt() {
   return m;
 }
 
-// Multiplicative hash of a community id into a power-of-two table.
+// Multiplicative (Fibonacci) hash of a community id into a power-of-two table
+// of mask+1 >= 2 slots: the top log2(mask+1) bits of c * 2^32/phi.  (The low
+// bits of the product would only permute c mod 2^k, so ids that agree in
+// their low bits would collide.)
 __device__ __forceinline__ unsigned hash_slot(int c, unsigned mask) {
-  return ((unsigned)c * 0x9E3779B1u) & mask;
+  return ((unsigned)c * 0x9E3779B1u) >> __clz(mask);
 }
 
 // 3-bit bit reversal: the order in which the reference's 8-lane shuffle-down
