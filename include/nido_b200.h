@@ -145,6 +145,28 @@ int nido_get_clustering(nido_graph g, int64_t* clustering);
 /* Clustering::dump_partition (clustering.cpp:23-46); new_orders may be NULL */
 int nido_dump_partition(nido_graph g, const char* path, const int64_t* new_orders);
 
+/* Modularity of a partition from caller-owned DEVICE arrays, allocating no
+ * memory: for code that cannot call cudaMalloc (a stream being captured
+ * into a CUDA graph, an allocator or memory-pool callback, a process whose
+ * device memory is all handed to a fixed pool).  No counterpart in the
+ * reference, whose modularity cudaMallocs a partials buffer on every call.
+ * Layout as in the reference: d_off[nv+1] and d_adj (int64), d_w (FP64),
+ * d_comm[nv] (int64 community ids in [0, nv)), d_a[nv] community degrees
+ * a_c indexed by community id, m the mass; Q is written to d_q (device) on
+ * `stream` (a cudaStream_t, NULL for the legacy default stream), without a
+ * host synchronisation.  The reduction follows the reference's order, so Q
+ * matches nido_compute_modularity bit for bit on integer weights.
+ * Scratch: a fixed 4 MiB array (524,280 FP64 group partials, the
+ * reference's own maximum) inside the library, held by every GPU that loads
+ * it until exit; it covers any nv up to the limit of 2^31-2 vertices, and
+ * larger nv is rejected with NIDO_E_TOO_LARGE.  The first call on a device
+ * looks up the array's device address (cudaGetSymbolAddress), so make that
+ * first call before any stream capture.  All calls on a device share the
+ * array: calls that overlap on the GPU race and return wrong values. */
+int nido_modularity_noalloc(void* stream, int64_t nv, const int64_t* d_off, const int64_t* d_adj,
+                            const double* d_w, const int64_t* d_comm, const double* d_a, double m,
+                            double* d_q);
+
 /* ---- whole run: LouvainGPU::run (louvain_gpu.cpp:6-139) ------------------------ */
 /* Starts from the uploaded graph (any earlier coarsening is undone first).
  * out_comm (nv entries, may be NULL) receives the clustering of the original

@@ -90,6 +90,7 @@ def lib() -> C.CDLL:
             "nido_get_clustering": (C.c_int, [vp, _i64p]),
             "nido_dump_partition": (C.c_int, [vp, C.c_char_p, _i64p]),
             "nido_run": (C.c_int, [vp, C.POINTER(_Params), _i64p, C.POINTER(RunStats)]),
+            "nido_modularity_noalloc": (C.c_int, [vp, C.c_int64, vp, vp, vp, vp, vp, C.c_double, vp]),
             "nido_color": (C.c_int, [vp, C.POINTER(_Csr), C.c_uint64, _i64p, _i64p]),
             "nido_color_relabel": (C.c_int, [vp, C.POINTER(_Csr), _i64p, C.POINTER(_Csr), _i64p]),
             "nido_read_vite": (C.c_int, [C.c_char_p, C.POINTER(_Csr)]),
