@@ -55,6 +55,13 @@ WORKLOADS = {
                          "weights U[0.5,1.5], duplicates summed, seed 1", nbatches=1, tau=1e-6),
     "sbm": dict(desc="SBM 16,777,216 vertices, power-law community sizes (2.5, 16..65,536), average degree 32, "
                      "70% intra, lognormal(0,0.5) weights, seed 3", nbatches=32, tau=1e-6),
+    "serve": dict(desc="serving stream: Poisson arrivals, vertex counts log-uniform [1e3, 1e7], 50/50 SBM "
+                       "(power-law communities 2.5, 16..65,536, average degree 32, 70% intra) / R-MAT "
+                       "(edge factor 16), weights U[0.5,1.5], HBM budget 150 GB, seed 5", nbatches=2, tau=1e-6),
+    "many": dict(desc="many-graph batch: 4,096 independent graphs, vertex counts log-uniform [100, 1e6] scaled "
+                      "to a total of 1.5e9 directed edges (clamped >= 100), 50/50 SBM (power-law communities "
+                      "2.5, 16..65,536, 70% intra) / R-MAT (0.57,0.19,0.19,0.05), average degree U[8,64], "
+                      "integer weights U{1..8} as FP64, seed 4", nbatches=2, tau=1e-6),
 }
 
 
@@ -268,6 +275,236 @@ def run_ours(args, world, rank, local):
     }
 
 
+def run_many(args, world, rank, local):
+    """Many graphs per step: one nido_batch_run over the packed set against
+    the same engine run one graph at a time (nido_run per graph, graph
+    resident), on a systematic sample of the graphs."""
+    import torch
+
+    from nido_b200 import capi
+    from nido_b200 import workloads as W
+    wl = WORKLOADS["many"]
+    torch.cuda.set_device(local)
+    t0 = time.perf_counter()
+    vbase, U, (V, d, kind) = W.many_graphs_packed(args.many_graphs, 4, args.many_edges)
+    gen_s = time.perf_counter() - t0
+    ng = len(vbase) - 1
+    ctx = capi.Context(local)
+    stream = torch.cuda.ExternalStream(ctx.stream())
+    B = capi.Batch(ctx, nbatches=wl["nbatches"], packed=(vbase, U))
+    for _ in range(args.warmup):
+        res = B.run(tau=wl["tau"])
+    barrier(world)
+    ctx.sync()
+    sampler = ClockSampler(local)
+    sampler.start()
+    l0 = capi.lib().nido_launch_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    runs = [B.run(tau=wl["tau"]) for _ in range(args.steps)]
+    e1.record(stream)
+    ctx.sync()
+    launches = int(capi.lib().nido_launch_count() - l0)
+    ms = e0.elapsed_time(e1)
+    clocks = sampler.stop()
+    parts, q, ph, lo, st = runs[-1]
+    B.close()
+    ms_max = reduce_max(ms, world)
+    move_ms = sum(r[4].move_ms for r in runs)
+    move_bytes = sum(r[4].move_bytes for r in runs)
+
+    # the same engine one graph at a time on every stride-th graph
+    stride = max(1, ng // args.plain_sample)
+    sample = list(range(0, ng, stride))
+    plain_ms, dq, mismatch = 0.0, 0.0, 0
+    for i in sample:
+        Gi = W.unpack(vbase, U, i)
+        with capi.Graph(ctx, Gi, wl["nbatches"]) as g:
+            g.run(tau=wl["tau"])
+            ctx.sync()
+            p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            p0.record(stream)
+            cl, sti = g.run(tau=wl["tau"])
+            p1.record(stream)
+            ctx.sync()
+            plain_ms += p0.elapsed_time(p1)
+        dq = max(dq, abs(sti.final_q - q[i]))
+        mismatch += int(not np.array_equal(cl, parts[i]))
+    plain_gps = len(sample) / (plain_ms * 1e-3)
+
+    # end to end: pinned host CSR -> upload -> batched run -> partitions
+    for a in (U.off, U.adj, U.w):
+        capi.host_register(a)
+    barrier(world)
+    ctx.sync()
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    for _ in range(args.steps):
+        with capi.Batch(ctx, nbatches=wl["nbatches"], packed=(vbase, U)) as b2:
+            b2.run(tau=wl["tau"])
+    f1.record(stream)
+    ctx.sync()
+    e2e_ms = reduce_max(f0.elapsed_time(f1), world)
+    for a in (U.off, U.adj, U.w):
+        capi.host_unregister(a)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        from oracle import oracle as orc
+        threads = os.cpu_count() or 1
+        done, t_cpu = 0, 0.0
+        for i in sample:  # whole oracle runs on the sampled graphs, about 20 s of CPU work
+            Gi = W.unpack(vbase, U, i)
+            c0 = time.perf_counter()
+            orc.louvain(Gi.off, Gi.adj, Gi.w, nbatches=wl["nbatches"], tau=wl["tau"])
+            t_cpu += time.perf_counter() - c0
+            done += 1
+            if t_cpu > 20.0:
+                break
+        cpu = {"value": done / t_cpu, "unit": "graphs/s", "cores": threads, "kind": "port",
+               "sample": f"CPU oracle (port of the reference's algorithm), whole runs of {done} of the "
+                         f"sampled graphs ({t_cpu:.1f} s)"}
+    ctx.close()
+    if rank != 0:
+        return None
+    pk, pk_kind = peaks()
+    achieved = move_bytes / (move_ms * 1e-3) / 1e9 if move_ms > 0 else 0.0
+    sec = ms_max * 1e-3
+    desc = wl["desc"]
+    if args.many_graphs != 4096 or args.many_edges != 1.5e9:
+        desc += f" [reduced: {args.many_graphs} graphs, {args.many_edges:.3g} edge cap]"
+    return {
+        "metric": "graphs/s", "value": world * ng * args.steps / sec, "unit": "graphs/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "impl": "ours",
+        "config": {"workload": "many", "graph": desc, "ngraphs": ng, "nv": U.nv, "ne": U.ne,
+                   "nbatches": wl["nbatches"], "tau": wl["tau"], "parallelism": f"replicas x{world}",
+                   "l2": "inputs larger than L2", "generation_s": round(gen_s, 1)},
+        "plain": {"graphs_per_s": world * plain_gps, "sampled_graphs": len(sample),
+                  "batched_over_plain": (ng * args.steps / sec) / plain_gps,
+                  "max_abs_dq_vs_plain": dq, "partition_mismatches": mismatch},
+        "edges_scanned_per_s": world * st.edges_scanned * args.steps / sec,
+        "e2e": {"value": world * ng * args.steps / (e2e_ms * 1e-3), "unit": "graphs/s",
+                "h2d_bytes_per_step": U.off.nbytes + U.adj.nbytes + U.w.nbytes + vbase.nbytes,
+                "d2h_bytes_per_step": 8 * U.nv + 24 * ng},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
+                     "frac": achieved / pk["hbm_gbs"], "traffic": None,
+                     "kernel": "move phase (degree-tier kernels of one sweep over all graphs)",
+                     "peak_kind": pk_kind},
+        "cpu_baseline": cpu,
+        "clocks": clocks,
+        "gpu_launches": launches,
+    }
+
+
+def run_serve(args, world, rank, local):
+    """A stream of requests with Poisson arrivals through the request loop
+    (nido_server_*): graphs/s from first arrival to last result, and the
+    latency (arrival to result in host memory) of every request."""
+    from nido_b200 import capi
+    from nido_b200 import workloads as W
+    wl = WORKLOADS["serve"]
+    t0 = time.perf_counter()
+    arr, V, kind = W.serving_requests(args.serve_requests, args.serve_rate, 5, 1e3, args.serve_vmax)
+    graphs = [W.make_request(int(v), int(k), 5_000_003 + i) for i, (v, k) in enumerate(zip(V, kind))]
+    gen_s = time.perf_counter() - t0
+    budget = int(args.serve_budget_gb * 1e9)
+    srv = capi.Server(local, budget, workers=args.serve_workers)
+    warm = [W.make_request(2000 + 500 * i, i % 2, 77 + i) for i in range(args.warmup)]
+    for t in [srv.submit(g, wl["nbatches"], wl["tau"]) for g in warm]:
+        srv.wait(t)
+    barrier(world)
+    sampler = ClockSampler(local)
+    sampler.start()
+    l0 = capi.lib().nido_launch_count()
+    tickets = [None] * len(graphs)
+    start = time.perf_counter()
+
+    def submitter():
+        for i, g in enumerate(graphs):
+            dt = arr[i] - (time.perf_counter() - start)
+            if dt > 0:
+                time.sleep(dt)
+            tickets[i] = srv.submit(g, wl["nbatches"], wl["tau"])
+
+    th = threading.Thread(target=submitter)
+    th.start()
+    th.join()
+    infos = [srv.wait(t)[1] for t in tickets]
+    wall = time.perf_counter() - start
+    launches = int(capi.lib().nido_launch_count() - l0)
+    clocks = sampler.stop()
+    srv.close()
+    lat = np.array([i.latency_ms for i in infos])
+    wall_max = reduce_max(wall, world)
+    if rank != 0:
+        return None
+    ne = int(sum(g.ne for g in graphs))
+    dev_ms = float(sum(i.device_ms for i in infos))
+    return {
+        "metric": "graphs/s", "value": world * len(graphs) / wall_max, "unit": "graphs/s", "n_gpus": world,
+        "steps": 1, "warmup": args.warmup, "ms_per_step": wall_max * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "ours",
+        "config": {"workload": "serve", "graph": wl["desc"], "requests": len(graphs),
+                   "rate_per_s": args.serve_rate, "vmax": args.serve_vmax, "workers": args.serve_workers,
+                   "hbm_budget_bytes": budget, "total_edges": ne, "generation_s": round(gen_s, 1),
+                   "parallelism": f"replicas x{world}", "l2": "inputs larger than L2"},
+        "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                       "max": float(lat.max()), "mean_queue": float(np.mean([i.queue_ms for i in infos]))},
+        "overlap": {"sum_device_ms": dev_ms, "wall_ms": wall * 1e3,
+                    "concurrency": dev_ms / (wall * 1e3)},
+        "e2e": {"value": world * len(graphs) / wall_max, "unit": "graphs/s",
+                "h2d_bytes_per_step": int(sum(g.off.nbytes + g.adj.nbytes + g.w.nbytes for g in graphs)),
+                "d2h_bytes_per_step": int(sum(8 * g.nv for g in graphs))},
+        "roofline": None,
+        "cpu_baseline": None,
+        "clocks": clocks,
+        "gpu_launches": launches,
+    }
+
+
+def run_reference_set(args, world, wl):
+    """Reference arm of the graph-set workloads: whole CPU-oracle runs, all
+    host threads, one graph after another (the reference runs one graph per
+    process), each step about 20 s of graphs drawn in order from the set."""
+    from nido_b200 import workloads as W
+    from oracle import oracle as orc
+    threads = os.cpu_count() or 1
+    if args.workload == "many":
+        Vp, dp, kp = W.many_graph_plan(args.many_graphs, 4, args.many_edges)
+        stride = max(1, len(Vp) // args.plain_sample)
+        items = [(int(Vp[i]), float(dp[i]), int(kp[i]), i) for i in range(0, len(Vp), stride)]
+        make = lambda it: W.make_one(it[0], it[1], it[2], 3, 4 * 1_000_003 + it[3])  # W_INT8
+    else:
+        _, Vs, ks = W.serving_requests(args.serve_requests, args.serve_rate, 5, 1e3, args.serve_vmax)
+        items = [(int(v), int(k), i) for i, (v, k) in enumerate(zip(Vs, ks))]
+        make = lambda it: W.make_request(it[0], it[1], 5_000_003 + it[2])
+    pos, times = 0, []
+    for step in range(args.warmup + args.steps):
+        done, el = 0, 0.0
+        while el < 20.0:
+            G = make(items[pos % len(items)])
+            pos += 1
+            c0 = time.perf_counter()
+            orc.louvain(G.off, G.adj, G.w, nbatches=wl["nbatches"], tau=wl["tau"])
+            el += time.perf_counter() - c0
+            done += 1
+        if step >= args.warmup:
+            times.append((done, el))
+    value = sum(t[0] for t in times) / sum(t[1] for t in times)
+    sample = (f"CPU oracle (port of the reference's algorithm), {threads} threads, whole runs of graphs drawn "
+              f"in order from the {args.workload} set, about 20 s per step")
+    return {
+        "metric": "graphs/s", "value": value, "unit": "graphs/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 / value, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+        "config": {"workload": args.workload, "graph": wl["desc"], "nbatches": wl["nbatches"], "tau": wl["tau"]},
+        "cpu_baseline": {"value": value, "unit": "graphs/s", "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": "graphs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+
+
 def run_reference(args, world, rank):
     """The reference's path on the host cores: the CPU oracle (a port of nido's
     algorithm; nido itself has no CPU implementation), all threads, each step
@@ -277,6 +514,8 @@ def run_reference(args, world, rank):
     from nido_b200 import capi
     from oracle import oracle as orc
     wl = WORKLOADS[args.workload]
+    if args.workload in ("many", "serve"):
+        return run_reference_set(args, world, wl)
     G = make_graph(capi, args.workload)
     threads = os.cpu_count() or 1
     # warm-up 1: one whole run fixes the edges a run visits (the oracle's
@@ -321,12 +560,24 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="rmat22")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--many-graphs", type=int, default=4096)
+    ap.add_argument("--many-edges", type=float, default=1.5e9)
+    ap.add_argument("--plain-sample", type=int, default=256, help="graphs run one at a time for the comparison")
+    ap.add_argument("--serve-requests", type=int, default=32)
+    ap.add_argument("--serve-rate", type=float, default=4.0, help="Poisson arrival rate, requests per second")
+    ap.add_argument("--serve-vmax", type=float, default=1e7)
+    ap.add_argument("--serve-workers", type=int, default=4)
+    ap.add_argument("--serve-budget-gb", type=float, default=150.0)
     args = ap.parse_args()
     if args.warmup < 3:
         raise SystemExit("--warmup must be at least 3")
     world, rank, local = dist_setup(args)
     if args.impl == "reference":
         out = run_reference(args, world, rank)
+    elif args.workload == "many":
+        out = run_many(args, world, rank, local)
+    elif args.workload == "serve":
+        out = run_serve(args, world, rank, local)
     else:
         out = run_ours(args, world, rank, local)
     if out is not None:

@@ -173,6 +173,68 @@ int nido_modularity_noalloc(void* stream, int64_t nv, const int64_t* d_off, cons
  * vertices; stats may be NULL. */
 int nido_run(nido_graph g, const nido_params* p, int64_t* out_comm, nido_run_stats* stats);
 
+/* ---- many graphs in one run (no reference counterpart: nido runs one graph per
+ * process, louvain_gpu.cpp:6-139) ---------------------------------------------- */
+typedef struct nido_batch_s* nido_batch;
+/* Packs ngraphs independent graphs as one CSR over all their vertices: graph i
+ * owns vertices [vbase[i], vbase[i+1]) (vbase has ngraphs+1 entries from 0 to
+ * nv), neighbour ids are global, and every edge must stay inside its graph
+ * (NIDO_E_INVALID otherwise).  nbatches is the -b of every graph. */
+int nido_batch_upload(nido_ctx ctx, int32_t ngraphs, const int64_t* vbase, int64_t nv, int64_t ne,
+                      const int64_t* off, const int64_t* adj, const double* w, int32_t nbatches,
+                      nido_batch* out);
+/* Runs every graph to completion in one phase loop.  Each graph's result is
+ * the one nido_run gives for it alone (identical on integer weights).
+ * out_comm (nv entries): each vertex's community, numbered within its graph;
+ * out_q, out_phases, out_loops (ngraphs entries): final Q, phases and total
+ * loops of every graph.  Any output may be NULL. */
+int nido_batch_run(nido_batch b, const nido_params* p, int64_t* out_comm, double* out_q,
+                   int64_t* out_phases, int64_t* out_loops, nido_run_stats* stats);
+int nido_batch_size(nido_batch b, int32_t* ngraphs, int64_t* nv, int64_t* ne);
+int nido_batch_free(nido_batch b);
+
+/* ---- serving: a request loop with continuous batching on one GPU (no reference
+ * counterpart) ------------------------------------------------------------------ */
+typedef struct nido_server_s* nido_server;
+typedef struct {
+  int32_t status;      /* NIDO_OK or the run's error code */
+  int32_t worker;      /* worker (stream) that ran it */
+  double final_q;
+  int64_t phases;
+  int64_t total_loops;
+  double queue_ms;     /* submit -> admitted on a worker */
+  double run_ms;       /* admitted -> result in host memory */
+  double latency_ms;   /* submit -> result in host memory */
+  double device_ms;    /* device-event time of the run */
+  int64_t hbm_bytes;   /* reservation held against the budget while it ran */
+} nido_request_info;
+/* Device bytes reserved for a graph of this size while it runs: the upload,
+ * work buffers and scratch, the hub-table region (16 bytes a slot, at most
+ * max(4M, 4*nv) slots) and 20 bytes per edge for the coarsening plan. */
+int64_t nido_graph_footprint(int64_t nv, int64_t ne, int32_t nbatches);
+/* Device bytes a graph holds now (upload, scratch, hub tables, plan). */
+int nido_graph_device_bytes(nido_graph g, int64_t* bytes);
+/* nworkers threads, each with its own stream; requests are admitted in
+ * arrival order while their footprints fit in the budget (0: all free HBM
+ * less 1 GiB; never more than that). */
+int nido_server_create(int device, size_t hbm_budget_bytes, int32_t nworkers, nido_server* out);
+/* Queues a run of g with p.  g's arrays and out_comm (nv entries, may be
+ * NULL) must stay valid until nido_server_wait returns for *ticket.  A
+ * request larger than the whole budget is refused (NIDO_E_TOO_LARGE). */
+int nido_server_submit(nido_server s, const nido_csr* g, const nido_params* p, int64_t* out_comm,
+                       int64_t* ticket);
+/* *state: 0 queued, 1 running, 2 finished */
+int nido_server_poll(nido_server s, int64_t ticket, int32_t* state);
+/* Blocks until the request finishes (timeout_s < 0: no limit); NIDO_E_TIMEOUT
+ * leaves the ticket valid.  Returns the request's own status and releases
+ * the ticket. */
+int nido_server_wait(nido_server s, int64_t ticket, double timeout_s, nido_request_info* info);
+/* budget, bytes reserved by running requests, running and queued counts */
+int nido_server_budget(nido_server s, int64_t* budget, int64_t* reserved, int32_t* running,
+                       int32_t* queued);
+/* Finishes every queued request, then stops the workers. */
+int nido_server_destroy(nido_server s);
+
 /* ---- colouring for -c (Graph::coloring, graph.cpp:651-797) ---------------------- */
 /* Jones-Plassmann-Luby colouring on the device; colors has nv entries;
  * returns the number of colours in *ncolors. Proper (no two neighbours share a

@@ -51,6 +51,13 @@ class RunStats(C.Structure):
 _lib = None
 
 
+class RequestInfo(C.Structure):
+    _fields_ = [("status", C.c_int32), ("worker", C.c_int32), ("final_q", C.c_double),
+                ("phases", C.c_int64), ("total_loops", C.c_int64), ("queue_ms", C.c_double),
+                ("run_ms", C.c_double), ("latency_ms", C.c_double), ("device_ms", C.c_double),
+                ("hbm_bytes", C.c_int64)]
+
+
 def lib() -> C.CDLL:
     """Load the compiled library (raises if it has not been built)."""
     global _lib
@@ -91,6 +98,20 @@ def lib() -> C.CDLL:
             "nido_dump_partition": (C.c_int, [vp, C.c_char_p, _i64p]),
             "nido_run": (C.c_int, [vp, C.POINTER(_Params), _i64p, C.POINTER(RunStats)]),
             "nido_modularity_noalloc": (C.c_int, [vp, C.c_int64, vp, vp, vp, vp, vp, C.c_double, vp]),
+            "nido_batch_upload": (C.c_int, [vp, C.c_int32, _i64p, C.c_int64, C.c_int64, _i64p, _i64p, _f64p,
+                                            C.c_int32, C.POINTER(vp)]),
+            "nido_batch_run": (C.c_int, [vp, C.POINTER(_Params), _i64p, _f64p, _i64p, _i64p,
+                                         C.POINTER(RunStats)]),
+            "nido_batch_size": (C.c_int, [vp, C.POINTER(C.c_int32), _i64p, _i64p]),
+            "nido_batch_free": (C.c_int, [vp]),
+            "nido_graph_footprint": (C.c_int64, [C.c_int64, C.c_int64, C.c_int32]),
+            "nido_graph_device_bytes": (C.c_int, [vp, _i64p]),
+            "nido_server_create": (C.c_int, [C.c_int, C.c_size_t, C.c_int32, C.POINTER(vp)]),
+            "nido_server_submit": (C.c_int, [vp, C.POINTER(_Csr), C.POINTER(_Params), _i64p, _i64p]),
+            "nido_server_poll": (C.c_int, [vp, C.c_int64, C.POINTER(C.c_int32)]),
+            "nido_server_wait": (C.c_int, [vp, C.c_int64, C.c_double, C.POINTER(RequestInfo)]),
+            "nido_server_budget": (C.c_int, [vp, _i64p, _i64p, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
+            "nido_server_destroy": (C.c_int, [vp]),
             "nido_color": (C.c_int, [vp, C.POINTER(_Csr), C.c_uint64, _i64p, _i64p]),
             "nido_color_relabel": (C.c_int, [vp, C.POINTER(_Csr), _i64p, C.POINTER(_Csr), _i64p]),
             "nido_read_vite": (C.c_int, [C.c_char_p, C.POINTER(_Csr)]),
@@ -342,6 +363,11 @@ class Graph:
         p = None if new_orders is None else _p64(np.ascontiguousarray(new_orders, dtype=np.int64))
         _check(lib().nido_dump_partition(self.h, path.encode(), p))
 
+    def device_bytes(self) -> int:
+        b = C.c_int64()
+        _check(lib().nido_graph_device_bytes(self.h, C.byref(b)))
+        return b.value
+
     def run(self, tau: float = 1e-6, max_iter: int = 500, tie: int = NIDO_TIE_SMALLEST_ID,
             verbose: bool = False):
         """LouvainGPU::run; returns (clustering of the input vertices, RunStats)."""
@@ -350,3 +376,124 @@ class Graph:
         st = RunStats()
         _check(lib().nido_run(self.h, C.byref(p), _p64(out), C.byref(st)))
         return out, st
+
+
+def pack_graphs(graphs: list[Csr]):
+    """Disjoint union of graphs as one CSR: returns (vbase, Csr) where graph i
+    owns vertices [vbase[i], vbase[i+1]) and its neighbour ids are shifted by
+    vbase[i]."""
+    nvs = np.array([g.nv for g in graphs], np.int64)
+    nes = np.array([g.ne for g in graphs], np.int64)
+    vbase = np.zeros(len(graphs) + 1, np.int64)
+    np.cumsum(nvs, out=vbase[1:])
+    ebase = np.zeros(len(graphs) + 1, np.int64)
+    np.cumsum(nes, out=ebase[1:])
+    off = np.empty(vbase[-1] + 1, np.int64)
+    adj = np.empty(ebase[-1], np.int64)
+    w = np.empty(ebase[-1], np.float64)
+    for i, g in enumerate(graphs):
+        off[vbase[i]:vbase[i + 1]] = g.off[:-1] + ebase[i]
+        adj[ebase[i]:ebase[i + 1]] = g.adj + vbase[i]
+        w[ebase[i]:ebase[i + 1]] = g.w
+    off[-1] = ebase[-1]
+    return vbase, Csr(off, adj, w)
+
+
+class Batch:
+    """Many independent graphs resident on the device as one packed CSR
+    (nido_batch), run together by nido_batch_run."""
+
+    def __init__(self, ctx: Context, graphs: list[Csr] | None = None, nbatches: int = 2,
+                 packed: tuple[np.ndarray, Csr] | None = None):
+        self.ctx = ctx
+        vbase, u = packed if packed is not None else pack_graphs(graphs)
+        self.vbase = np.ascontiguousarray(vbase, dtype=np.int64)
+        self.ngraphs = len(self.vbase) - 1
+        self.nv = u.nv
+        self.nbatches = nbatches
+        s = u._struct()
+        h = C.c_void_p()
+        _check(lib().nido_batch_upload(ctx.h, self.ngraphs, _p64(self.vbase), s.nv, s.ne, s.off, s.adj, s.w,
+                                       nbatches, C.byref(h)))
+        self.h = h
+
+    def close(self):
+        if self.h:
+            lib().nido_batch_free(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def run(self, tau: float = 1e-6, max_iter: int = 500, tie: int = NIDO_TIE_SMALLEST_ID):
+        """Returns (per-graph clusterings, final Q per graph, phases per graph,
+        loops per graph, RunStats)."""
+        p = _Params(self.nbatches, tie, tau, max_iter, 0, 0)
+        out = np.empty(self.nv, np.int64)
+        q = np.empty(self.ngraphs, np.float64)
+        ph = np.empty(self.ngraphs, np.int64)
+        lo = np.empty(self.ngraphs, np.int64)
+        st = RunStats()
+        _check(lib().nido_batch_run(self.h, C.byref(p), _p64(out), _pf(q), _p64(ph), _p64(lo), C.byref(st)))
+        parts = [out[self.vbase[i]:self.vbase[i + 1]] for i in range(self.ngraphs)]
+        return parts, q, ph, lo, st
+
+
+def graph_footprint(nv: int, ne: int, nbatches: int = 2) -> int:
+    return int(lib().nido_graph_footprint(nv, ne, nbatches))
+
+
+class Server:
+    """Request loop on one GPU (nido_server_*): submit() queues a run and
+    returns a ticket, wait() returns (clustering, RequestInfo)."""
+
+    def __init__(self, device: int = 0, hbm_budget: int = 0, workers: int = 4):
+        h = C.c_void_p()
+        _check(lib().nido_server_create(device, hbm_budget, workers, C.byref(h)))
+        self.h = h
+        self._keep = {}
+
+    def submit(self, g: Csr, nbatches: int = 2, tau: float = 1e-6, max_iter: int = 500,
+               tie: int = NIDO_TIE_SMALLEST_ID) -> int:
+        s = g._struct()
+        p = _Params(nbatches, tie, tau, max_iter, 0, 0)
+        out = np.empty(g.nv, np.int64)
+        t = C.c_int64()
+        _check(lib().nido_server_submit(self.h, C.byref(s), C.byref(p), _p64(out), C.byref(t)))
+        self._keep[t.value] = (g, out)  # the engine reads and writes these until wait()
+        return t.value
+
+    def poll(self, ticket: int) -> int:
+        st = C.c_int32()
+        _check(lib().nido_server_poll(self.h, ticket, C.byref(st)))
+        return st.value
+
+    def wait(self, ticket: int, timeout: float = -1.0):
+        info = RequestInfo()
+        rc = lib().nido_server_wait(self.h, ticket, timeout, C.byref(info))
+        if rc == -6:  # NIDO_E_TIMEOUT: still pending
+            _check(rc)
+        _, out = self._keep.pop(ticket)
+        _check(rc)
+        return out, info
+
+    def budget(self):
+        b, r = C.c_int64(), C.c_int64()
+        run, q = C.c_int32(), C.c_int32()
+        _check(lib().nido_server_budget(self.h, C.byref(b), C.byref(r), C.byref(run), C.byref(q)))
+        return b.value, r.value, run.value, q.value
+
+    def close(self):
+        if self.h:
+            lib().nido_server_destroy(self.h)
+            self.h = None
+            self._keep.clear()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()

@@ -70,6 +70,14 @@ __global__ void k_newid(const int32_t* __restrict__ comm, const int64_t* __restr
   }
 }
 
+// Communities never span graphs (no edge does), so the renumber keeps every
+// graph's vertices contiguous and its new first vertex is cid[old first].
+__global__ void k_graph_bases(const int64_t* __restrict__ gbase, int ng, const int64_t* __restrict__ cid,
+                              int64_t* __restrict__ gbase2) {
+  for (int64_t g = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g <= ng; g += (int64_t)gridDim.x * blockDim.x)
+    gbase2[g] = cid[gbase[g]];
+}
+
 __global__ void k_compose(int32_t* __restrict__ clus, int64_t n0, const int32_t* __restrict__ newid) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n0; i += (int64_t)gridDim.x * blockDim.x)
     clus[i] = newid[clus[i]];
@@ -508,6 +516,10 @@ int launch_aggregation(nido_graph_s* g, int* done) {
   NIDO_LAUNCH_CHECK();
   k_compose<<<grid_for(g->nv0, 256, kSMs * 16), 256, 0, s>>>(g->clus, g->nv0, newid);
   NIDO_LAUNCH_CHECK();
+  if (g->gid) {  // many graphs: each graph's first coarse vertex
+    k_graph_bases<<<grid_for(g->ngraphs + 1, 256, kSMs), 256, 0, s>>>(g->gbase, g->ngraphs, cid, g->gbase2);
+    NIDO_LAUNCH_CHECK();
+  }
   int64_t nvp = 0;
   NIDO_CUDA_TRY(cudaMemcpyAsync(&nvp, cid + nv, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
   NIDO_CUDA_TRY(cudaStreamSynchronize(s));
@@ -584,11 +596,11 @@ int launch_aggregation(nido_graph_s* g, int* done) {
                          (sizeof(int32_t) * 2 + sizeof(double)) * slots + 16 * 256;
     if (bytes > g->agg_buf_bytes) {
       NIDO_CUDA_TRY(cudaStreamSynchronize(s));
-      if (g->agg_buf) cudaFree(g->agg_buf);
+      raw_free(g->ctx, g->agg_buf);
       g->agg_buf = nullptr;
       g->agg_buf_bytes = 0;
       const size_t want = bytes + bytes / 4;
-      NIDO_CUDA_TRY(cudaMalloc((void**)&g->agg_buf, want));
+      NIDO_CUDA_TRY(raw_alloc(g->ctx, (void**)&g->agg_buf, want));
       g->agg_buf_bytes = want;
     }
     Arena pa(g->agg_buf, g->agg_buf_bytes);

@@ -16,6 +16,17 @@
 
 using nido::Arena;
 
+namespace nido {
+cudaError_t raw_alloc(nido_ctx_s* ctx, void** p, size_t bytes) {
+  return ctx->async_alloc ? cudaMallocAsync(p, bytes, ctx->stream) : cudaMalloc(p, bytes);
+}
+void raw_free(nido_ctx_s* ctx, void* p) {
+  if (!p) return;
+  if (ctx->async_alloc) cudaFreeAsync(p, ctx->stream);
+  else cudaFree(p);
+}
+}  // namespace nido
+
 namespace {
 
 template <typename T>
@@ -23,7 +34,7 @@ int dev_alloc(nido_ctx ctx, T** p, int64_t n) {
   const size_t bytes = sizeof(T) * (size_t)(n > 0 ? n : 1);
   if (ctx->budget && ctx->used + bytes > ctx->budget)
     return nido_set_error(NIDO_E_NOMEM, "HBM budget of %zu bytes exceeded", ctx->budget);
-  cudaError_t e = cudaMalloc((void**)p, bytes);
+  cudaError_t e = nido::raw_alloc(ctx, (void**)p, bytes);
   if (e != cudaSuccess) {
     *p = nullptr;
     cudaGetLastError();
@@ -35,7 +46,7 @@ int dev_alloc(nido_ctx ctx, T** p, int64_t n) {
 
 void dev_free(nido_ctx ctx, void* p, size_t bytes) {
   if (p) {
-    cudaFree(p);
+    nido::raw_free(ctx, p);
     ctx->used -= std::min(ctx->used, bytes);
   }
 }
@@ -99,6 +110,13 @@ int prepare_phase(nido_graph g) {
 
 namespace nido {
 int graph_prepare_phase(nido_graph g) { return prepare_phase(g); }
+int device_alloc(nido_ctx ctx, void** p, size_t bytes) {
+  char* q = nullptr;
+  const int st = dev_alloc(ctx, &q, (int64_t)bytes);
+  *p = q;
+  return st;
+}
+void device_free(nido_ctx ctx, void* p, size_t bytes) { dev_free(ctx, p, bytes); }
 }
 
 extern "C" int nido_ctx_create(int device, size_t hbm_budget_bytes, nido_ctx* out) {
@@ -170,8 +188,9 @@ extern "C" int nido_graph_free(nido_graph g) {
   // hub-tier buffers are sized per phase outside the budget accounting
   for (void* p : {(void*)g->gkeys, (void*)g->gvals, (void*)g->hub_items, (void*)g->hub_v, (void*)g->hub_capv,
                   (void*)g->hub_nseg, (void*)g->hub_toff, (void*)g->hub_done, (void*)g->hub_slices,
-                  (void*)g->hub_slice_first, (void*)g->hub_res, (void*)g->agg_buf})
-    if (p) cudaFree(p);
+                  (void*)g->hub_slice_first, (void*)g->hub_res, (void*)g->agg_buf, (void*)g->hub_occ,
+                  (void*)g->hub_nocc})
+    nido::raw_free(ctx, p);
   delete g;
   return NIDO_OK;
 }
@@ -237,6 +256,17 @@ extern "C" int nido_graph_upload(nido_ctx ctx, int64_t nv, int64_t ne, const int
   if (st == NIDO_OK) st = nido::launch_singleton(g);
   if (st != NIDO_OK) { nido_graph_free(g); return st; }
   *out = g;
+  return NIDO_OK;
+}
+
+extern "C" int nido_graph_device_bytes(nido_graph g, int64_t* bytes) {
+  if (!g || !bytes) return nido_set_error(NIDO_E_INVALID, "null argument");
+  const int64_t V = g->cap_v, E = g->cap_e;
+  int64_t b = 24 * (V + 1) + 36 * E + 28 * V + 4 * g->nv0 + 128 + (int64_t)g->scratch_bytes;
+  b += 16 * g->gslab + 4 * g->hub_cap_nocc + 8 * g->hub_cap_items + 4 * (g->hub_cap_hubs_v + g->hub_cap_hubs_c + g->hub_cap_hubs_s +
+                                                   g->hub_cap_hubs_d) +
+       8 * (g->hub_cap_hubs_t + g->hub_cap_slices + g->hub_cap_first) + g->hub_cap_res + (int64_t)g->agg_buf_bytes;
+  *bytes = b;
   return NIDO_OK;
 }
 
@@ -550,7 +580,8 @@ extern "C" int nido_run(nido_graph g, const nido_params* p, int64_t* out_comm, n
   st.total_ms = tot;
   st.phases = phases;
   int64_t nerr = 0;
-  NIDO_CUDA_TRY(cudaMemcpy(&nerr, g->dcount + 1, sizeof(int64_t), cudaMemcpyDeviceToHost));
+  NIDO_CUDA_TRY(cudaMemcpyAsync(&nerr, g->dcount + 1, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
+  NIDO_CUDA_TRY(cudaStreamSynchronize(s));
   if (nerr) return nido_set_error(NIDO_E_CUDA, "hash table overflow in %lld probes", (long long)nerr);
   lap(1);
   if (out_comm) NIDO_TRY(nido_get_clustering(g, out_comm));

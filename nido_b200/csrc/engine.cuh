@@ -45,6 +45,10 @@ struct nido_ctx_s {
   size_t used = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   std::vector<cudaEvent_t> move_ev;  // 2 per batch, for per-iteration move timing
+  // stream-ordered allocation (cudaMallocAsync / cudaFreeAsync on the
+  // context's stream): allocating or freeing then does not wait for the work
+  // of other contexts on the same GPU
+  bool async_alloc = false;
 };
 
 struct nido_graph_s {
@@ -96,6 +100,11 @@ struct nido_graph_s {
   int32_t* hub_nseg = nullptr;
   int64_t* hub_toff = nullptr;
   int32_t* hub_done = nullptr;
+  // occupied slots of every hub table in insertion order (same offsets as the
+  // tables) and their counts, so the slice scans touch only used slots
+  int32_t* hub_occ = nullptr;
+  int32_t* hub_nocc = nullptr;
+  int64_t hub_cap_nocc = 0;
   int64_t hub_cap_items = 0, hub_cap_hubs_v = 0, hub_cap_hubs_c = 0, hub_cap_hubs_s = 0,
           hub_cap_hubs_t = 0, hub_cap_hubs_d = 0;
   int64_t nhubs = 0;
@@ -115,6 +124,18 @@ struct nido_graph_s {
   // so runs after the first allocate nothing)
   char* agg_buf = nullptr;
   size_t agg_buf_bytes = 0;
+
+  // many-graph mode (null / empty for one graph): the graph of every current
+  // vertex, the mass of every graph, and the batch of every vertex relative to
+  // its own graph's -b cuts
+  int32_t* gid = nullptr;
+  double* mg = nullptr;
+  int32_t* vbatch = nullptr;
+  int64_t* gbase = nullptr;   // first vertex of every graph (ngraphs+1)
+  int64_t* gcuts = nullptr;   // -b cuts of every graph, relative (ngraphs*(nbatches+1))
+  int32_t* gactive = nullptr; // graph iterating in the current phase
+  int64_t* gbase2 = nullptr;  // first vertex of every graph after coarsening
+  int32_t ngraphs = 1;
 
   std::vector<int64_t> cuts;     // host batch cuts (nbatches+1)
   std::vector<int64_t> tier_off; // host: nbatches*kNumTiers+1 offsets into perm
@@ -148,6 +169,14 @@ int launch_singleton(nido_graph_s* g);
 int launch_set_comm(nido_graph_s* g);                   // a from comm
 int launch_commit(nido_graph_s* g, int64_t v0, int64_t v1);
 int launch_modularity(nido_graph_s* g, double* q);      // host value
+int launch_q_self(nido_graph_s* g, double* selfv);      // per-vertex in-community weight
+int graph_prepare_phase(nido_graph_s* g);               // k, m, tier lists (engine.cu)
+// device memory of a context: stream-ordered when ctx->async_alloc (engine.cu)
+cudaError_t raw_alloc(nido_ctx_s* ctx, void** p, size_t bytes);
+void raw_free(nido_ctx_s* ctx, void* p);  // null is a no-op
+// device memory counted against the context's HBM budget (engine.cu)
+int device_alloc(nido_ctx_s* ctx, void** p, size_t bytes);
+void device_free(nido_ctx_s* ctx, void* p, size_t bytes);
 int build_batches(nido_graph_s* g);                     // cuts (host) + tier lists
 // move phase (move.cu)
 // ev_start / ev_end (may be null) are recorded around the tier kernels

@@ -39,7 +39,18 @@ struct MoveArgs {
   double m;
   int tie;
   unsigned long long* err;  // probe-limit failures (never expected)
+  // many-graph mode: graph of every vertex and mass of every graph (null for
+  // one graph, whose mass is m)
+  const int32_t* __restrict__ gid;
+  const double* __restrict__ mg;
 };
+
+// The mass of v's graph (kernels are instantiated per mode, so the
+// one-graph kernels carry no graph-id lookup).
+template <bool kMulti>
+__device__ __forceinline__ double vertex_mass(const MoveArgs& p, int v) {
+  return kMulti ? p.mg[p.gid[v]] : p.m;
+}
 
 constexpr unsigned long long kNoKey = ~0ull;
 
@@ -102,7 +113,7 @@ __device__ __forceinline__ double group_sum(double x) {
 }
 
 // ---- degree <= 32: registers ---------------------------------------------------
-template <int G>
+template <int G, bool kMulti>
 __global__ void __launch_bounds__(256) k_move_group(const int32_t* __restrict__ list, int64_t n,
                                                     MoveArgs p) {
   constexpr int VPW = 32 / G;
@@ -114,7 +125,7 @@ __global__ void __launch_bounds__(256) k_move_group(const int32_t* __restrict__ 
     const bool vok = idx < n;
     int v = 0, own = -1;
     int64_t s = 0, d = 0;
-    double ki = 0., aown = 0.;
+    double ki = 0., aown = 0., m = p.m;
     if (vok) {
       v = list[idx];
       s = p.off[v];
@@ -122,6 +133,7 @@ __global__ void __launch_bounds__(256) k_move_group(const int32_t* __restrict__ 
       own = p.comm[v];
       ki = p.k[v];
       aown = p.a[own];
+      m = vertex_mass<kMulti>(p, v);
     }
     const bool ok = gl < d;
     int c = -1;
@@ -142,7 +154,7 @@ __global__ void __launch_bounds__(256) k_move_group(const int32_t* __restrict__ 
       if (c == own) {
         eown = e;
       } else {
-        g = gain_of(e, ki, p.a[c], p.m);
+        g = gain_of(e, ki, p.a[c], m);
         tk = (unsigned)c;
         cand = c;
       }
@@ -162,7 +174,7 @@ __global__ void __launch_bounds__(256) k_move_group(const int32_t* __restrict__ 
     }
     group_best<G>(g, tk, cand);
     if (gl == 0 && vok) {
-      const double self = self_of(eown, ki, aown, p.m);
+      const double self = self_of(eown, ki, aown, m);
       const double tot = __dsub_rn(g, self);
       p.newc[v] = (cand >= 0 && tot > 0.) ? cand : own;
     }
@@ -185,12 +197,27 @@ struct Table {
 };
 
 // Adds e to key c's value, inserting c when absent; returns the slot and
-// whether this call inserted it.
-template <bool kAtomicVals>
+// whether this call inserted it.  Tables in global memory (kGlobal) go
+// straight to the compare-and-swap, one L2 round trip per probe; shared-memory
+// tables read the key first.
+template <bool kAtomicVals, bool kGlobal = false>
 __device__ __forceinline__ int table_add(const Table& t, int c, double e, bool& isnew, unsigned long long* err) {
   unsigned h = hash_slot(c, t.mask);
   volatile int* vk = t.keys;
   isnew = false;
+  if (kGlobal) {
+    for (unsigned probe = 0; probe <= t.mask; ++probe) {
+      const int old = atomicCAS(&t.keys[h], -1, c);
+      if (old == -1 || old == c) {
+        isnew = old == -1;
+        atomicAdd(&t.vals[h], e);
+        return (int)h;
+      }
+      h = (h + 1) & t.mask;
+    }
+    atomicAdd(err, 1ull);
+    return -1;
+  }
   for (unsigned probe = 0; probe <= t.mask; ++probe) {
     const int kk = vk[h];
     bool hit = kk == c;
@@ -233,7 +260,7 @@ __device__ __forceinline__ unsigned next_pow2_cap(int64_t d) {
 // then the communities) before any is merged, so each warp keeps several
 // dependent gathers in flight.  Chunks are merged in order.  Every lane of the
 // warp takes part.
-template <bool kAtomicVals, int kUnroll>
+template <bool kAtomicVals, int kUnroll, bool kGlobal = false>
 __device__ __forceinline__ void accumulate_edges(const MoveArgs& p, int v, int64_t first, int64_t eend,
                                                  int64_t stride, const Table& t) {
   const int lane = threadIdx.x & 31;
@@ -264,7 +291,7 @@ __device__ __forceinline__ void accumulate_edges(const MoveArgs& p, int v, int64
       const double e = fold_peers(peers, ok, wt[k]);
       bool isnew = false;
       int slot = -1;
-      if (lead) slot = table_add<kAtomicVals>(t, c[k], e, isnew, p.err);
+      if (lead) slot = table_add<kAtomicVals, kGlobal>(t, c[k], e, isnew, p.err);
       occ_append(t, isnew, slot);
       if (!kAtomicVals) __syncwarp();
     }
@@ -275,7 +302,7 @@ __device__ __forceinline__ void accumulate_edges(const MoveArgs& p, int v, int64
 // occ is null): e_own and the best (gain, tie key, community) of this thread.
 // Entries are taken four at a time so that their a_c gathers are in flight
 // together.
-__device__ __forceinline__ void scan_entries(const MoveArgs& p, const Table& t, int n, int t0, int step,
+__device__ __forceinline__ void scan_entries(const MoveArgs& p, double m, const Table& t, int n, int t0, int step,
                                              int own, double ki, bool cg, double& eown, double& g,
                                              unsigned long long& tk, int& cand) {
   constexpr int U = 4;
@@ -300,7 +327,7 @@ __device__ __forceinline__ void scan_entries(const MoveArgs& p, const Table& t, 
       if (cc[k] == own) {
         eown = val[k];
       } else {
-        const double gg = gain_of(val[k], ki, ac[k], p.m);
+        const double gg = gain_of(val[k], ki, ac[k], m);
         if (better(gg, (unsigned)cc[k], g, tk)) { g = gg; tk = (unsigned)cc[k]; cand = cc[k]; }
       }
     }
@@ -310,7 +337,7 @@ __device__ __forceinline__ void scan_entries(const MoveArgs& p, const Table& t, 
 // The reference's tie rule over the same entries: among communities whose
 // gain equals gm, the smallest (bitrev3(rank mod 8), rank), where rank counts
 // the vertex's neighbour communities with a smaller id.
-__device__ __forceinline__ void nido_tie_entries(const MoveArgs& p, const Table& t, int n, int t0, int step,
+__device__ __forceinline__ void nido_tie_entries(const MoveArgs& p, double m, const Table& t, int n, int t0, int step,
                                                  int own, double ki, double gm, bool cg, double& g,
                                                  unsigned long long& tk, int& cand) {
   g = -NIDO_MAX_FLOAT; tk = kNoKey; cand = -1;
@@ -319,7 +346,7 @@ __device__ __forceinline__ void nido_tie_entries(const MoveArgs& p, const Table&
     const int cc = cg ? __ldcg(&t.keys[slot]) : t.keys[slot];
     if (cc < 0 || cc == own) continue;
     const double val = cg ? __ldcg(&t.vals[slot]) : t.vals[slot];
-    if (gain_of(val, ki, p.a[cc], p.m) != gm) continue;
+    if (gain_of(val, ki, p.a[cc], m) != gm) continue;
     unsigned rank = 0;
     for (int q = 0; q < n; ++q) {
       const int kq = cg ? __ldcg(&t.keys[t.occ ? t.occ[q] : q]) : t.keys[t.occ ? t.occ[q] : q];
@@ -330,15 +357,15 @@ __device__ __forceinline__ void nido_tie_entries(const MoveArgs& p, const Table&
   }
 }
 
-__device__ __forceinline__ void decide(const MoveArgs& p, int v, int own, double ki, double aown, double eown,
+__device__ __forceinline__ void decide(const MoveArgs& p, double m, int v, int own, double ki, double aown, double eown,
                                        double g, int cand) {
-  const double self = self_of(eown, ki, aown, p.m);
+  const double self = self_of(eown, ki, aown, m);
   const double tot = __dsub_rn(g, self);
   p.newc[v] = (cand >= 0 && tot > 0.) ? cand : own;
 }
 
 // ---- 32 < degree <= 256: one warp per vertex, table in shared memory -----------
-template <int kCap>
+template <int kCap, bool kMulti>
 __global__ void __launch_bounds__(256) k_move_warp(const int32_t* __restrict__ list, int64_t n, MoveArgs p) {
   extern __shared__ double smem[];
   __shared__ int nocc_s[8];
@@ -364,14 +391,15 @@ __global__ void __launch_bounds__(256) k_move_warp(const int32_t* __restrict__ l
     double g = -NIDO_MAX_FLOAT, eown = 0.;
     unsigned long long tk = kNoKey;
     int cand = -1;
-    scan_entries(p, t, nu, lane, 32, own, ki, false, eown, g, tk, cand);
+    const double m = vertex_mass<kMulti>(p, v);
+    scan_entries(p, m, t, nu, lane, 32, own, ki, false, eown, g, tk, cand);
     eown = group_sum<32>(eown);
     if (p.tie == NIDO_TIE_NIDO) {
       const double gm = group_max<32>(g);
-      nido_tie_entries(p, t, nu, lane, 32, own, ki, gm, false, g, tk, cand);
+      nido_tie_entries(p, m, t, nu, lane, 32, own, ki, gm, false, g, tk, cand);
     }
     group_best<32>(g, tk, cand);
-    if (lane == 0) decide(p, v, own, ki, aown, eown, g, cand);
+    if (lane == 0) decide(p, m, v, own, ki, aown, eown, g, cand);
     __syncwarp();
     for (int i = lane; i < nu; i += 32) {
       const int slot = t.occ[i];
@@ -425,17 +453,17 @@ __device__ double block_max(double x, double* sx) {
 }
 
 // Evaluate a filled table with the whole block and write newc[v].
-__device__ __forceinline__ void block_evaluate(const MoveArgs& p, const Table& t, int n, bool cg, int v, int own,
+__device__ __forceinline__ void block_evaluate(const MoveArgs& p, double m, const Table& t, int n, bool cg, int v, int own,
                                                double ki, double aown, double* sg, unsigned long long* stk,
                                                int* sc) {
   double g = -NIDO_MAX_FLOAT, eown = 0.;
   unsigned long long tk = kNoKey;
   int cand = -1;
-  scan_entries(p, t, n, threadIdx.x, blockDim.x, own, ki, cg, eown, g, tk, cand);
+  scan_entries(p, m, t, n, threadIdx.x, blockDim.x, own, ki, cg, eown, g, tk, cand);
   if (p.tie == NIDO_TIE_NIDO) {
     eown = block_sum(eown, sg);
     const double gm = block_max(g, sg);
-    nido_tie_entries(p, t, n, threadIdx.x, blockDim.x, own, ki, gm, cg, g, tk, cand);
+    nido_tie_entries(p, m, t, n, threadIdx.x, blockDim.x, own, ki, gm, cg, g, tk, cand);
   }
   // one reduction for the best entry and e_own (e_own is nonzero in one
   // thread at most, so its sum is exact in any order)
@@ -452,12 +480,12 @@ __device__ __forceinline__ void block_evaluate(const MoveArgs& p, const Table& t
     double e2 = lane < nw ? se[lane] : 0.;
     group_best<32>(g, tk, cand);
     e2 = group_sum<32>(e2);
-    if (lane == 0) decide(p, v, own, ki, aown, p.tie == NIDO_TIE_NIDO ? eown : e2, g, cand);
+    if (lane == 0) decide(p, m, v, own, ki, aown, p.tie == NIDO_TIE_NIDO ? eown : e2, g, cand);
   }
 }
 
 // ---- 256 < degree <= 2048: one CTA per vertex, table in shared memory ----------
-template <int kThreads, int kCap>
+template <int kThreads, int kCap, bool kMulti>
 __global__ void __launch_bounds__(kThreads) k_move_cta(const int32_t* __restrict__ list, int64_t n, MoveArgs p) {
   extern __shared__ double smem[];
   __shared__ double sg[32];
@@ -484,7 +512,7 @@ __global__ void __launch_bounds__(kThreads) k_move_cta(const int32_t* __restrict
     const int nu = nocc_s;
     // block_evaluate ends with a barrier that every thread reaches after
     // reading nu, so the count can be reset right after it
-    block_evaluate(p, t, nu, false, v, own, ki, aown, sg, stk, sc);
+    block_evaluate(p, vertex_mass<kMulti>(p, v), t, nu, false, v, own, ki, aown, sg, stk, sc);
     if (threadIdx.x == 0) nocc_s = 0;
     for (int i = threadIdx.x; i < nu; i += kThreads) {
       const int slot = t.occ[i];
@@ -502,6 +530,7 @@ __global__ void __launch_bounds__(kThreads) k_move_cta(const int32_t* __restrict
 constexpr int kHubSeg = 2048;
 constexpr int kHubThreads = 256;
 
+template <bool kMulti>
 __global__ void __launch_bounds__(kHubThreads) k_move_hub(const int2* __restrict__ items, int64_t n,
                                                           const int32_t* __restrict__ hub_v,
                                                           const int64_t* __restrict__ hub_toff,
@@ -527,7 +556,7 @@ __global__ void __launch_bounds__(kHubThreads) k_move_hub(const int2* __restrict
     const int64_t s = p.off[v], eend = p.off[v + 1];
     const int64_t s0 = s + (int64_t)item.y * kHubSeg;
     const int64_t s1 = min(eend, s0 + kHubSeg);
-    accumulate_edges<true, 2>(p, v, s0 + (int64_t)wid * 32, s1, kHubThreads, t);
+    accumulate_edges<true, 2, true>(p, v, s0 + (int64_t)wid * 32, s1, kHubThreads, t);
     __threadfence();
     __syncthreads();
     if (threadIdx.x == 0) last_s = atomicAdd(&hub_done[h], 1) == hub_nseg[h] - 1;
@@ -536,7 +565,7 @@ __global__ void __launch_bounds__(kHubThreads) k_move_hub(const int2* __restrict
       __threadfence();
       const int own = p.comm[v];
       const double ki = p.k[v], aown = p.a[own];
-      block_evaluate(p, t, (int)(t.mask + 1), true, v, own, ki, aown, sg, stk, sc);
+      block_evaluate(p, vertex_mass<kMulti>(p, v), t, (int)(t.mask + 1), true, v, own, ki, aown, sg, stk, sc);
       for (unsigned i = threadIdx.x; i <= t.mask; i += kHubThreads) {
         t.keys[i] = -1;
         t.vals[i] = 0.;
@@ -561,7 +590,8 @@ __global__ void __launch_bounds__(kHubThreads) k_hub_insert(const int2* __restri
                                                             const int32_t* __restrict__ hub_v,
                                                             const int64_t* __restrict__ hub_toff,
                                                             const int32_t* __restrict__ hub_cap, int32_t* gkeys,
-                                                            double* gvals, MoveArgs p) {
+                                                            double* gvals, int32_t* __restrict__ hub_occ,
+                                                            int32_t* __restrict__ hub_nocc, MoveArgs p) {
   const int wid = threadIdx.x >> 5;
   for (int64_t it = blockIdx.x; it < n; it += gridDim.x) {
     const int2 item = items[it];
@@ -570,12 +600,12 @@ __global__ void __launch_bounds__(kHubThreads) k_hub_insert(const int2* __restri
     Table t;
     t.keys = gkeys + hub_toff[h];
     t.vals = gvals + hub_toff[h];
-    t.occ = nullptr;
-    t.nocc = nullptr;
+    t.occ = hub_occ + hub_toff[h];
+    t.nocc = hub_nocc + h;
     t.mask = (unsigned)hub_cap[h] - 1;
     const int64_t s = p.off[v], eend = p.off[v + 1];
     const int64_t s0 = s + (int64_t)item.y * kHubSeg;
-    accumulate_edges<true, 4>(p, v, s0 + (int64_t)wid * 32, min(eend, s0 + kHubSeg), kHubThreads, t);
+    accumulate_edges<true, 4, true>(p, v, s0 + (int64_t)wid * 32, min(eend, s0 + kHubSeg), kHubThreads, t);
   }
 }
 
@@ -587,13 +617,16 @@ struct SliceResult {
   int pad;
 };
 
-// Slice y of hub x covers slots [y*kHubSlice, (y+1)*kHubSlice) of the hub's
-// table, read and cleared in order (the tables exceed L2, so coalesced
-// access matters more than skipping empty slots).
+// Slice y of hub x covers entries [y*kHubSlice, (y+1)*kHubSlice) of the
+// hub's occupied-slot list (slices past the hub's count return at once);
+// every listed slot is read and cleared.  The tables of a wave are L2
+// resident, so the scattered slot reads stay on chip.
+template <bool kMulti>
 __global__ void __launch_bounds__(kHubThreads) k_hub_slices(const int2* __restrict__ slices, int64_t n,
                                                             const int32_t* __restrict__ hub_v,
                                                             const int64_t* __restrict__ hub_toff,
-                                                            const int32_t* __restrict__ hub_cap, int32_t* gkeys,
+                                                            const int32_t* __restrict__ hub_occ,
+                                                            const int32_t* __restrict__ hub_nocc, int32_t* gkeys,
                                                             double* gvals, MoveArgs p,
                                                             SliceResult* __restrict__ res) {
   __shared__ double sg[32];
@@ -601,25 +634,31 @@ __global__ void __launch_bounds__(kHubThreads) k_hub_slices(const int2* __restri
   __shared__ int sc[32];
   for (int64_t it = blockIdx.x; it < n; it += gridDim.x) {
     const int2 sl = slices[it];
+    const int len = min(kHubSlice, hub_nocc[sl.x] - sl.y * kHubSlice);
+    if (len <= 0) {  // uniform over the block
+      if (threadIdx.x == 0) res[it] = SliceResult{-NIDO_MAX_FLOAT, 0., kNoKey, -1, 0};
+      continue;
+    }
     const int v = hub_v[sl.x];
-    int* keys = gkeys + hub_toff[sl.x] + (int64_t)sl.y * kHubSlice;
-    double* vals = gvals + hub_toff[sl.x] + (int64_t)sl.y * kHubSlice;
-    const int len = min(kHubSlice, hub_cap[sl.x] - sl.y * kHubSlice);
+    int* keys = gkeys + hub_toff[sl.x];
+    double* vals = gvals + hub_toff[sl.x];
+    const int32_t* occ = hub_occ + hub_toff[sl.x] + (int64_t)sl.y * kHubSlice;
     const int own = p.comm[v];
     const double ki = p.k[v];
+    const double m = vertex_mass<kMulti>(p, v);
     double g = -NIDO_MAX_FLOAT, eown = 0.;
     unsigned long long tk = kNoKey;
     int cand = -1;
     for (int i = threadIdx.x; i < len; i += kHubThreads) {
-      const int cc = keys[i];
-      if (cc < 0) continue;
-      const double val = vals[i];
-      keys[i] = -1;
-      vals[i] = 0.;
+      const int slot = occ[i];
+      const int cc = keys[slot];
+      const double val = vals[slot];
+      keys[slot] = -1;
+      vals[slot] = 0.;
       if (cc == own) {
         eown = val;
       } else {
-        const double gg = gain_of(val, ki, p.a[cc], p.m);
+        const double gg = gain_of(val, ki, p.a[cc], m);
         if (better(gg, (unsigned)cc, g, tk)) { g = gg; tk = (unsigned)cc; cand = cc; }
       }
     }
@@ -629,8 +668,9 @@ __global__ void __launch_bounds__(kHubThreads) k_hub_slices(const int2* __restri
   }
 }
 
+template <bool kMulti>
 __global__ void k_hub_combine(int64_t nh, const int32_t* __restrict__ hub_v, const int64_t* __restrict__ slice_first,
-                              const SliceResult* __restrict__ res, MoveArgs p) {
+                              const SliceResult* __restrict__ res, int32_t* __restrict__ hub_nocc, MoveArgs p) {
   const int lane = threadIdx.x & 31;
   const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
@@ -650,7 +690,8 @@ __global__ void k_hub_combine(int64_t nh, const int32_t* __restrict__ hub_v, con
     if (lane == 0) {
       const int v = hub_v[h];
       const int own = p.comm[v];
-      decide(p, v, own, p.k[v], p.a[own], eown, g, cand);
+      decide(p, vertex_mass<kMulti>(p, v), v, own, p.k[v], p.a[own], eown, g, cand);
+      hub_nocc[h] = 0;  // every slice of this hub has read its count
     }
   }
 }
@@ -672,13 +713,12 @@ inline unsigned grid_cap(int64_t blocks, int64_t cap) {
 template <typename T>
 int ensure(nido_graph_s* g, T** p, int64_t* cap, int64_t n) {
   if (n <= *cap) return NIDO_OK;
-  if (*p) cudaFree(*p);
+  raw_free(g->ctx, *p);
   *p = nullptr;
   *cap = 0;
   const int64_t m = std::max<int64_t>(n, 1024);
-  NIDO_CUDA_TRY(cudaMalloc((void**)p, sizeof(T) * (size_t)m));
+  NIDO_CUDA_TRY(raw_alloc(g->ctx, (void**)p, sizeof(T) * (size_t)m));
   *cap = m;
-  (void)g;
   return NIDO_OK;
 }
 
@@ -759,14 +799,19 @@ int plan_hubs(nido_graph_s* g) {
   NIDO_TRY(ensure(g, &g->hub_res, &g->hub_cap_res, (int64_t)(slices.size() * sizeof(SliceResult))));
   NIDO_CUDA_TRY(cudaMemcpyAsync(g->hub_slices, slices.data(), sizeof(int2) * slices.size(), cudaMemcpyHostToDevice, s));
   NIDO_CUDA_TRY(cudaMemcpyAsync(g->hub_slice_first, sfirst.data(), sizeof(int64_t) * (nh + 1), cudaMemcpyHostToDevice, s));
+  NIDO_TRY(ensure(g, &g->hub_nocc, &g->hub_cap_nocc, nh));
+  NIDO_CUDA_TRY(cudaMemsetAsync(g->hub_nocc, 0, sizeof(int32_t) * nh, s));
   if (toff > g->gslab) {
-    if (g->gkeys) cudaFree(g->gkeys);
-    if (g->gvals) cudaFree(g->gvals);
+    raw_free(g->ctx, g->gkeys);
+    raw_free(g->ctx, g->gvals);
+    raw_free(g->ctx, g->hub_occ);
     g->gkeys = nullptr;
     g->gvals = nullptr;
+    g->hub_occ = nullptr;
     g->gslab = 0;
-    NIDO_CUDA_TRY(cudaMalloc((void**)&g->gkeys, sizeof(int32_t) * (size_t)toff));
-    NIDO_CUDA_TRY(cudaMalloc((void**)&g->gvals, sizeof(double) * (size_t)toff));
+    NIDO_CUDA_TRY(raw_alloc(g->ctx, (void**)&g->gkeys, sizeof(int32_t) * (size_t)toff));
+    NIDO_CUDA_TRY(raw_alloc(g->ctx, (void**)&g->gvals, sizeof(double) * (size_t)toff));
+    NIDO_CUDA_TRY(raw_alloc(g->ctx, (void**)&g->hub_occ, sizeof(int32_t) * (size_t)toff));
     NIDO_CUDA_TRY(cudaMemsetAsync(g->gkeys, 0xff, sizeof(int32_t) * (size_t)toff, s));
     NIDO_CUDA_TRY(cudaMemsetAsync(g->gvals, 0, sizeof(double) * (size_t)toff, s));
     g->gslab = toff;
@@ -794,12 +839,88 @@ int set_smem(K kernel, size_t bytes) {
 }
 }  // namespace
 
-int move_init_attributes() {
-  NIDO_TRY(set_smem(k_move_warp<kWarpCap>, (size_t)8 * kWarpCap * 16));
-  NIDO_TRY(set_smem(k_move_cta<128, kCtaSCap>, (size_t)kCtaSCap * 16));
-  NIDO_TRY(set_smem(k_move_cta<256, kCtaMCap>, (size_t)kCtaMCap * 16));
-  NIDO_TRY(set_smem(k_move_cta<256, kCtaLCap>, (size_t)kCtaLCap * 16));
+namespace {
+template <bool kMulti>
+int set_smem_mode() {
+  NIDO_TRY(set_smem(k_move_warp<kWarpCap, kMulti>, (size_t)8 * kWarpCap * 16));
+  NIDO_TRY(set_smem(k_move_cta<128, kCtaSCap, kMulti>, (size_t)kCtaSCap * 16));
+  NIDO_TRY(set_smem(k_move_cta<256, kCtaMCap, kMulti>, (size_t)kCtaMCap * 16));
+  NIDO_TRY(set_smem(k_move_cta<256, kCtaLCap, kMulti>, (size_t)kCtaLCap * 16));
   return NIDO_OK;
+}
+
+// the tier kernels of one batch; kMulti: many graphs (per-vertex mass)
+template <bool kMulti>
+int launch_tiers(nido_graph_s* g, int batch, int tie, const MoveArgs& p) {
+  cudaStream_t s = g->ctx->stream;
+  const int nb = g->nbatches;
+  for (int t = 0; t < kNumTiers; ++t) {
+    const int64_t b0 = g->tier_off[(size_t)t * nb + batch], b1 = g->tier_off[(size_t)t * nb + batch + 1];
+    const int64_t n = b1 - b0;
+    if (n <= 0) continue;
+    const int32_t* list = g->perm + b0;
+    switch (t) {
+      case kTierG4:
+        k_move_group<4, kMulti><<<grid_cap((n + 63) / 64, kSMs * 16), 256, 0, s>>>(list, n, p);
+        break;
+      case kTierG8:
+        k_move_group<8, kMulti><<<grid_cap((n + 31) / 32, kSMs * 16), 256, 0, s>>>(list, n, p);
+        break;
+      case kTierG16:
+        k_move_group<16, kMulti><<<grid_cap((n + 15) / 16, kSMs * 16), 256, 0, s>>>(list, n, p);
+        break;
+      case kTierG32:
+        k_move_group<32, kMulti><<<grid_cap((n + 7) / 8, kSMs * 16), 256, 0, s>>>(list, n, p);
+        break;
+      case kTierWarp:
+        k_move_warp<kWarpCap, kMulti><<<grid_cap((n + 7) / 8, kSMs * 7), 256, (size_t)8 * kWarpCap * 16, s>>>(
+            list, n, p);
+        break;
+      case kTierCtaS:
+        k_move_cta<128, kCtaSCap, kMulti><<<grid_cap(n, kSMs * 14), 128, (size_t)kCtaSCap * 16, s>>>(list, n, p);
+        break;
+      case kTierCtaM:
+        k_move_cta<256, kCtaMCap, kMulti><<<grid_cap(n, kSMs * 7), 256, (size_t)kCtaMCap * 16, s>>>(list, n, p);
+        break;
+      case kTierCtaL:
+        k_move_cta<256, kCtaLCap, kMulti><<<grid_cap(n, kSMs * 3), 256, (size_t)kCtaLCap * 16, s>>>(list, n, p);
+        break;
+      default: {
+        SliceResult* res = reinterpret_cast<SliceResult*>(g->hub_res);
+        for (int64_t wv = g->hub_wave_off[batch]; wv < g->hub_wave_off[batch + 1]; ++wv) {
+          const nido_graph_s::HubWave& w = g->hub_waves[wv];
+          const int2* items = g->hub_items + w.i0;
+          if (tie == NIDO_TIE_NIDO) {
+            k_move_hub<kMulti><<<grid_cap(w.i1 - w.i0, kSMs * 8), kHubThreads, 0, s>>>(
+                items, w.i1 - w.i0, g->hub_v, g->hub_toff, g->hub_capv, g->hub_nseg, g->hub_done, g->gkeys,
+                g->gvals, p);
+            NIDO_LAUNCH_CHECK();
+            continue;
+          }
+          k_hub_insert<<<grid_cap(w.i1 - w.i0, kSMs * 8), kHubThreads, 0, s>>>(
+              items, w.i1 - w.i0, g->hub_v, g->hub_toff, g->hub_capv, g->gkeys, g->gvals, g->hub_occ,
+              g->hub_nocc, p);
+          NIDO_LAUNCH_CHECK();
+          k_hub_slices<kMulti><<<grid_cap(w.s1 - w.s0, kSMs * 8), kHubThreads, 0, s>>>(
+              g->hub_slices + w.s0, w.s1 - w.s0, g->hub_v, g->hub_toff, g->hub_occ, g->hub_nocc, g->gkeys,
+              g->gvals, p, res + w.s0);
+          NIDO_LAUNCH_CHECK();
+          k_hub_combine<kMulti><<<grid_cap((w.h1 - w.h0 + 7) / 8, kSMs * 4), 256, 0, s>>>(
+              w.h1 - w.h0, g->hub_v + w.h0, g->hub_slice_first + w.h0, res, g->hub_nocc + w.h0, p);
+          NIDO_LAUNCH_CHECK();
+        }
+        continue;
+      }
+    }
+    NIDO_LAUNCH_CHECK();
+  }
+  return NIDO_OK;
+}
+}  // namespace
+
+int move_init_attributes() {
+  NIDO_TRY(set_smem_mode<false>());
+  return set_smem_mode<true>();
 }
 
 int launch_move(nido_graph_s* g, int batch, int tie, cudaEvent_t ev_start, cudaEvent_t ev_end) {
@@ -808,67 +929,9 @@ int launch_move(nido_graph_s* g, int batch, int tie, cudaEvent_t ev_start, cudaE
   if (!g->bins_valid) NIDO_TRY(build_batches(g));
   cudaStream_t s = g->ctx->stream;
   MoveArgs p{g->off, g->adj, g->w, g->comm, g->k, g->a, g->newc, g->m, tie,
-             reinterpret_cast<unsigned long long*>(g->dcount + 1)};
-  const int nb = g->nbatches;
+             reinterpret_cast<unsigned long long*>(g->dcount + 1), g->gid, g->mg};
   if (ev_start) NIDO_CUDA_TRY(cudaEventRecord(ev_start, s));
-  for (int t = 0; t < kNumTiers; ++t) {
-    const int64_t b0 = g->tier_off[(size_t)t * nb + batch], b1 = g->tier_off[(size_t)t * nb + batch + 1];
-    const int64_t n = b1 - b0;
-    if (n <= 0) continue;
-    const int32_t* list = g->perm + b0;
-    switch (t) {
-      case kTierG4:
-        k_move_group<4><<<grid_cap((n + 63) / 64, kSMs * 16), 256, 0, s>>>(list, n, p);
-        break;
-      case kTierG8:
-        k_move_group<8><<<grid_cap((n + 31) / 32, kSMs * 16), 256, 0, s>>>(list, n, p);
-        break;
-      case kTierG16:
-        k_move_group<16><<<grid_cap((n + 15) / 16, kSMs * 16), 256, 0, s>>>(list, n, p);
-        break;
-      case kTierG32:
-        k_move_group<32><<<grid_cap((n + 7) / 8, kSMs * 16), 256, 0, s>>>(list, n, p);
-        break;
-      case kTierWarp:
-        k_move_warp<kWarpCap><<<grid_cap((n + 7) / 8, kSMs * 7), 256, (size_t)8 * kWarpCap * 16, s>>>(list, n, p);
-        break;
-      case kTierCtaS:
-        k_move_cta<128, kCtaSCap><<<grid_cap(n, kSMs * 14), 128, (size_t)kCtaSCap * 16, s>>>(list, n, p);
-        break;
-      case kTierCtaM:
-        k_move_cta<256, kCtaMCap><<<grid_cap(n, kSMs * 7), 256, (size_t)kCtaMCap * 16, s>>>(list, n, p);
-        break;
-      case kTierCtaL:
-        k_move_cta<256, kCtaLCap><<<grid_cap(n, kSMs * 3), 256, (size_t)kCtaLCap * 16, s>>>(list, n, p);
-        break;
-      default: {
-        SliceResult* res = reinterpret_cast<SliceResult*>(g->hub_res);
-        for (int64_t wv = g->hub_wave_off[batch]; wv < g->hub_wave_off[batch + 1]; ++wv) {
-          const nido_graph_s::HubWave& w = g->hub_waves[wv];
-          const int2* items = g->hub_items + w.i0;
-          if (tie == NIDO_TIE_NIDO) {
-            k_move_hub<<<grid_cap(w.i1 - w.i0, kSMs * 8), kHubThreads, 0, s>>>(
-                items, w.i1 - w.i0, g->hub_v, g->hub_toff, g->hub_capv, g->hub_nseg, g->hub_done, g->gkeys,
-                g->gvals, p);
-            NIDO_LAUNCH_CHECK();
-            continue;
-          }
-          k_hub_insert<<<grid_cap(w.i1 - w.i0, kSMs * 8), kHubThreads, 0, s>>>(
-              items, w.i1 - w.i0, g->hub_v, g->hub_toff, g->hub_capv, g->gkeys, g->gvals, p);
-          NIDO_LAUNCH_CHECK();
-          k_hub_slices<<<grid_cap(w.s1 - w.s0, kSMs * 8), kHubThreads, 0, s>>>(
-              g->hub_slices + w.s0, w.s1 - w.s0, g->hub_v, g->hub_toff, g->hub_capv, g->gkeys, g->gvals, p,
-              res + w.s0);
-          NIDO_LAUNCH_CHECK();
-          k_hub_combine<<<grid_cap((w.h1 - w.h0 + 7) / 8, kSMs * 4), 256, 0, s>>>(
-              w.h1 - w.h0, g->hub_v + w.h0, g->hub_slice_first + w.h0, res, p);
-          NIDO_LAUNCH_CHECK();
-        }
-        continue;
-      }
-    }
-    NIDO_LAUNCH_CHECK();
-  }
+  NIDO_TRY(g->gid ? launch_tiers<true>(g, batch, tie, p) : launch_tiers<false>(g, batch, tie, p));
   if (ev_end) NIDO_CUDA_TRY(cudaEventRecord(ev_end, s));
   return NIDO_OK;
 }

@@ -11,6 +11,7 @@
 #include <algorithm>
 
 #include "common.cuh"
+#include "cuts.cuh"
 #include "engine.cuh"
 #include "primitives.cuh"
 
@@ -206,39 +207,11 @@ __global__ void k_q_groups(int64_t nv, int64_t S, int64_t ngroups, const double*
 }
 
 // Batch cuts of partition_graph_edge_batch (graph_gpu.cpp:303-339) on one
-// thread, with a binary search per cut instead of the linear scan.
+// thread.
 __global__ void k_batch_cuts(const int64_t* __restrict__ off, int64_t nv, int nb,
                              int64_t* __restrict__ cuts, int64_t* __restrict__ parts) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  const int64_t ave = (off[nv] - off[0]) / nb;
-  int np = 0;
-  parts[np++] = 0;
-  int64_t start = 0;
-  while (np <= nb + 1) {
-    // first i in (start, nv] with off[i] - off[start] > ave
-    const int64_t target = off[start] + ave;
-    int64_t lo = start + 1, hi = nv + 1;
-    while (lo < hi) {
-      const int64_t mid = lo + (hi - lo) / 2;
-      if (off[mid] > target) hi = mid; else lo = mid + 1;
-    }
-    if (lo <= nv) {
-      parts[np++] = lo;
-      start = lo;
-      if (lo == nv) break;
-    } else {
-      parts[np++] = nv;
-      break;
-    }
-  }
-  if (np > nb + 1) {
-    const int64_t nnv = (nv - parts[nb]) / nb;
-    for (int i = 1; i < nb; ++i) parts[i] += nnv;
-    parts[nb] = nv;
-  } else {
-    while (np < nb + 1) parts[np++] = nv;
-  }
-  for (int i = 0; i <= nb; ++i) cuts[i] = parts[i];
+  batch_cuts(off, nv, nb, cuts, parts);
 }
 
 __device__ __forceinline__ int tier_of(int64_t d) {
@@ -256,26 +229,44 @@ __device__ __forceinline__ int tier_of(int64_t d) {
 // key = tier * nb + batch, so every (tier, batch) range and every tier over
 // all batches is contiguous after the stable sort.  Counts and the maximum
 // degree are aggregated per warp before the global atomics.
+// Many-graph mode (gid non-null): the batch is found in the vertex's own
+// graph's cuts (gcuts, nb+1 per graph, relative to gbase), vertices of graphs
+// that are not iterating get the key past all tiers, and every vertex's batch
+// is stored in vbatch.
 __global__ void k_tier_keys(const int64_t* __restrict__ off, int64_t nv, const int64_t* __restrict__ cuts,
                             int nb, uint32_t* __restrict__ keys, uint32_t* __restrict__ vals,
-                            int64_t* __restrict__ counts, unsigned long long* __restrict__ maxdeg) {
+                            int64_t* __restrict__ counts, unsigned long long* __restrict__ maxdeg,
+                            const int32_t* __restrict__ gid, const int64_t* __restrict__ gbase,
+                            const int64_t* __restrict__ gcuts, const int32_t* __restrict__ gactive,
+                            int32_t* __restrict__ vbatch) {
   const int lane = threadIdx.x & 31;
+  const uint32_t skip = (uint32_t)(kNumTiers * nb);
   unsigned long long md = 0;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   for (int64_t base = blockIdx.x * (int64_t)blockDim.x; base < nv; base += stride) {
     const int64_t v = base + threadIdx.x;
     uint32_t key = 0xffffffffu;
     if (v < nv) {
-      int lo = 0, hi = nb;  // batch b with cuts[b] <= v < cuts[b+1]
+      const int64_t* c = cuts;
+      int64_t x = v;
+      bool active = true;
+      if (gid) {
+        const int g = gid[v];
+        c = gcuts + (int64_t)g * (nb + 1);
+        x = v - gbase[g];
+        active = gactive[g] != 0;
+      }
+      int lo = 0, hi = nb;  // batch b with c[b] <= x < c[b+1]
       while (hi - lo > 1) {
         const int mid = (lo + hi) / 2;
-        if (cuts[mid] <= v) lo = mid; else hi = mid;
+        if (c[mid] <= x) lo = mid; else hi = mid;
       }
+      if (vbatch) vbatch[v] = lo;
       const int64_t d = off[v + 1] - off[v];
-      key = (uint32_t)(tier_of(d) * nb + lo);
+      key = active ? (uint32_t)(tier_of(d) * nb + lo) : skip;
       keys[v] = key;
       vals[v] = (uint32_t)v;
-      md = md > (unsigned long long)d ? md : (unsigned long long)d;
+      if (active) md = md > (unsigned long long)d ? md : (unsigned long long)d;
     }
     const unsigned peers = __match_any_sync(NIDO_FULL_MASK, key);
     if (key != 0xffffffffu && lane == __ffs(peers) - 1)
@@ -332,20 +323,10 @@ int launch_commit(nido_graph_s* g, int64_t v0, int64_t v1) {
   return NIDO_OK;
 }
 
-int launch_modularity(nido_graph_s* g, double* q) {
+// Per-vertex in-community weight (self-loops included) of every listed
+// vertex, over all tiers of the current tier lists.
+int launch_q_self(nido_graph_s* g, double* selfv) {
   cudaStream_t s = g->ctx->stream;
-  const int64_t nv = g->nv;
-  if (nv == 0) { *q = 0.; return NIDO_OK; }
-  if (!g->bins_valid) NIDO_TRY(build_batches(g));
-  Arena ar(g->scratch, g->scratch_bytes);
-  double* selfv = ar.take<double>(nv);
-  int64_t grid = (nv + 7) / 8;
-  if (grid > 65535) grid = 65535;
-  const int64_t S = 128 * grid;
-  const int64_t nslots = std::min<int64_t>(S, nv);
-  const int64_t ngroups = (nslots + 15) / 16;
-  double* modv = ar.take<double>(ngroups);
-  if (!selfv || !modv) return nido_set_error(NIDO_E_NOMEM, "scratch arena too small (modularity)");
   const int nb = g->nbatches;
   for (int t = 0; t < kNumTiers; ++t) {
     const int64_t b0 = g->tier_off[(size_t)t * nb], b1 = g->tier_off[(size_t)(t + 1) * nb];
@@ -374,6 +355,24 @@ int launch_modularity(nido_graph_s* g, double* q) {
     }
     NIDO_LAUNCH_CHECK();
   }
+  return NIDO_OK;
+}
+
+int launch_modularity(nido_graph_s* g, double* q) {
+  cudaStream_t s = g->ctx->stream;
+  const int64_t nv = g->nv;
+  if (nv == 0) { *q = 0.; return NIDO_OK; }
+  if (!g->bins_valid) NIDO_TRY(build_batches(g));
+  Arena ar(g->scratch, g->scratch_bytes);
+  double* selfv = ar.take<double>(nv);
+  int64_t grid = (nv + 7) / 8;
+  if (grid > 65535) grid = 65535;
+  const int64_t S = 128 * grid;
+  const int64_t nslots = std::min<int64_t>(S, nv);
+  const int64_t ngroups = (nslots + 15) / 16;
+  double* modv = ar.take<double>(ngroups);
+  if (!selfv || !modv) return nido_set_error(NIDO_E_NOMEM, "scratch arena too small (modularity)");
+  NIDO_TRY(launch_q_self(g, selfv));
   const int64_t threads = ngroups * 16;
   k_q_groups<<<(unsigned)((threads + 255) / 256), 256, 0, s>>>(nv, S, ngroups, selfv, g->a, g->dm, modv);
   NIDO_LAUNCH_CHECK();
@@ -399,23 +398,28 @@ int build_batches(nido_graph_s* g) {
   uint32_t* vals2 = ar.take<uint32_t>(nv);
   int64_t* rtemp = ar.take<int64_t>(std::max(radix_temp_elems(nv), scan_temp_elems(nkeys)));
   if (!rtemp) return nido_set_error(NIDO_E_NOMEM, "scratch arena too small (batches)");
-  k_batch_cuts<<<1, 1, 0, s>>>(g->off, nv, nb, dcuts, dparts);
-  NIDO_LAUNCH_CHECK();
+  const bool multi = g->gid != nullptr;  // many graphs: per-graph cuts in g->gcuts
+  if (!multi) {
+    k_batch_cuts<<<1, 1, 0, s>>>(g->off, nv, nb, dcuts, dparts);
+    NIDO_LAUNCH_CHECK();
+  }
   NIDO_CUDA_TRY(cudaMemsetAsync(counts, 0, sizeof(int64_t) * (nkeys + 1), s));
   NIDO_CUDA_TRY(cudaMemsetAsync(maxdeg, 0, sizeof(unsigned long long), s));
   if (nv > 0) {
     k_tier_keys<<<grid_for(nv, kThreads), kThreads, 0, s>>>(g->off, nv, dcuts, nb, keys, (uint32_t*)g->perm,
-                                                           counts, maxdeg);
+                                                           counts, maxdeg, g->gid, g->gbase, g->gcuts,
+                                                           g->gactive, g->vbatch);
     NIDO_LAUNCH_CHECK();
     int bits = 0;
-    while (((int64_t)1 << bits) < nkeys) ++bits;
+    while (((int64_t)1 << bits) < nkeys + 1) ++bits;
     NIDO_TRY(radix_sort_pairs(keys, (uint32_t*)g->perm, keys2, vals2, nv, bits, rtemp, s));
   }
   NIDO_TRY(scan_exclusive_i64(counts, counts, nkeys, rtemp, s));
   g->cuts.assign(nb + 1, 0);
   g->tier_off.assign(nkeys + 1, 0);
   unsigned long long md = 0;
-  NIDO_CUDA_TRY(cudaMemcpyAsync(g->cuts.data(), dcuts, sizeof(int64_t) * (nb + 1), cudaMemcpyDeviceToHost, s));
+  if (!multi)
+    NIDO_CUDA_TRY(cudaMemcpyAsync(g->cuts.data(), dcuts, sizeof(int64_t) * (nb + 1), cudaMemcpyDeviceToHost, s));
   NIDO_CUDA_TRY(cudaMemcpyAsync(g->tier_off.data(), counts, sizeof(int64_t) * (nkeys + 1), cudaMemcpyDeviceToHost, s));
   NIDO_CUDA_TRY(cudaMemcpyAsync(&md, maxdeg, sizeof(md), cudaMemcpyDeviceToHost, s));
   NIDO_CUDA_TRY(cudaStreamSynchronize(s));

@@ -1,0 +1,109 @@
+"""The request loop (nido_server_*): results are the same alone and in the
+mix (bit-exact on integer weights; NMI >= 0.95 and |dQ| <= 1e-3 on FP64
+weights), admission never reserves more than the HBM budget, and the
+footprint a request reserves covers what its graph really holds."""
+import threading
+import time
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def requests(capi, wmode):
+    rng = np.random.default_rng(61)
+    gs = []
+    for i in range(10):
+        nv = int(np.exp(rng.uniform(np.log(1e3), np.log(2e5))))
+        if i % 2:
+            gs.append(capi.gen_rmat(nv, 16 * nv, wmode=wmode, seed=200 + i))
+        else:
+            gs.append(capi.gen_sbm(nv, 2.5, 16, 65536, 32.0, 0.7, wmode, True, 200 + i))
+    return gs
+
+
+def alone(capi, ctx, gs, tie=0):
+    out = []
+    for G in gs:
+        with capi.Graph(ctx, G, 2) as g:
+            cl, st = g.run(tie=tie)
+            out.append((cl, st.final_q, g.device_bytes()))
+    return out
+
+
+def test_same_alone_and_mixed_integer(nido_lib, ctx):
+    gs = requests(nido_lib, nido_lib.W_INT8)
+    want = alone(nido_lib, ctx, gs)
+    with nido_lib.Server(0, 0, workers=4) as srv:
+        ts = [srv.submit(G) for G in gs]
+        got = [srv.wait(t) for t in ts]
+    workers = {info.worker for _, info in got}
+    assert len(workers) > 1  # the mix really ran on several streams
+    for (cl, q, _), (out, info) in zip(want, got):
+        assert info.status == 0
+        assert np.array_equal(out, cl)
+        assert info.final_q == q
+
+
+def test_same_alone_and_mixed_fp64(nido_lib, ctx, orc):
+    gs = requests(nido_lib, nido_lib.W_UNIFORM)
+    want = alone(nido_lib, ctx, gs)
+    with nido_lib.Server(0, 0, workers=3) as srv:
+        ts = []
+        for G in gs:  # staggered arrivals: later requests join while earlier ones run
+            ts.append(srv.submit(G))
+            time.sleep(0.002)
+        got = [srv.wait(t) for t in ts]
+    for G, (cl, q, _), (out, info) in zip(gs, want, got):
+        assert abs(info.final_q - q) <= 1e-3
+        assert orc.nmi(out, cl) >= 0.95
+        assert abs(orc.partition_modularity(G.off, G.adj, G.w, out) - info.final_q) <= 1e-5
+
+
+def test_footprint_covers_device_bytes(nido_lib, ctx):
+    gs = requests(nido_lib, nido_lib.W_INT8)
+    for G, (_, _, used) in zip(gs, alone(nido_lib, ctx, gs)):
+        assert nido_lib.graph_footprint(G.nv, G.ne, 2) >= used
+
+
+def test_admission_respects_budget(nido_lib):
+    gs = requests(nido_lib, nido_lib.W_INT8)
+    fps = [nido_lib.graph_footprint(G.nv, G.ne, 2) for G in gs]
+    budget = 2 * max(fps)
+    with nido_lib.Server(0, budget, workers=6) as srv:
+        b, _, _, _ = srv.budget()
+        assert b == budget
+        seen = []
+        stop = threading.Event()
+
+        def watch():
+            while not stop.is_set():
+                seen.append(srv.budget())
+                time.sleep(0.0005)
+
+        th = threading.Thread(target=watch)
+        th.start()
+        ts = [srv.submit(G) for G in gs]
+        infos = [srv.wait(t)[1] for t in ts]
+        stop.set()
+        th.join()
+        assert all(r <= budget for _, r, _, _ in seen)
+        assert all(i.status == 0 and i.hbm_bytes == f for i, f in zip(infos, fps))
+        with pytest.raises(nido_lib.NidoError) as e:
+            big = nido_lib.gen_rmat(1 << 20, 16 << 20, wmode=nido_lib.W_ONE, seed=3)
+            srv.submit(big)
+        assert e.value.code == -5  # NIDO_E_TOO_LARGE
+
+
+def test_wait_timeout_keeps_ticket(nido_lib):
+    G = nido_lib.gen_rmat(1 << 17, 16 << 17, wmode=nido_lib.W_INT8, seed=7)
+    with nido_lib.Server(0, 0, workers=1) as srv:
+        t1 = srv.submit(G)
+        t2 = srv.submit(G)
+        with pytest.raises(nido_lib.NidoError) as e:
+            srv.wait(t2, timeout=0.0)
+        assert e.value.code == -6  # NIDO_E_TIMEOUT
+        a, ia = srv.wait(t1)
+        b, ib = srv.wait(t2)
+        assert np.array_equal(a, b) and ib.queue_ms >= ia.run_ms * 0.5

@@ -1,0 +1,146 @@
+"""Host-side pieces that need no GPU: the C ABI's exported symbols, Vite
+files, the generators, graph packing for batched runs, the command line's
+option handling, and the replica plumbing of bench.py over gloo."""
+import ctypes as C
+import os
+import re
+import socket
+import subprocess
+
+import numpy as np
+import pytest
+
+from conftest import ROOT, load_golden
+
+HEADER = os.path.join(ROOT, "include", "nido_b200.h")
+
+
+def declared_functions():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(nido_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol(nido_lib):
+    names = declared_functions()
+    assert len(names) >= 40
+    L = C.CDLL(nido_lib.LIB_PATH)
+    missing = [n for n in names if not hasattr(L, n)]
+    assert not missing, missing
+    assert nido_lib.lib().nido_version().decode()
+
+
+def test_no_device_is_an_error_not_a_fallback(nido_lib):
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    with pytest.raises(nido_lib.NidoError) as e:
+        nido_lib.Context(0)
+    assert e.value.code == -7  # NIDO_E_NODEVICE
+
+
+def test_vite_round_trip_and_errors(nido_lib, tmp_path):
+    d = load_golden("selfloop_int")
+    g = nido_lib.Csr(d["off"], d["adj"], d["w"])
+    p = str(tmp_path / "g.bin")
+    nido_lib.write_vite(p, g)
+    h = nido_lib.read_vite(p)
+    assert np.array_equal(h.off, g.off) and np.array_equal(h.adj, g.adj) and np.array_equal(h.w, g.w)
+    # header (nv, ne) then (nv+1) offsets, ne (tail, weight) records
+    raw = open(p, "rb").read()
+    assert len(raw) == 16 + 8 * (g.nv + 1) + 16 * g.ne
+    open(p, "wb").write(raw[: len(raw) - 8])
+    with pytest.raises(nido_lib.NidoError):
+        nido_lib.read_vite(p)
+    with pytest.raises(nido_lib.NidoError):
+        nido_lib.read_vite(str(tmp_path / "missing.bin"))
+
+
+@pytest.mark.parametrize("kind", ["planted", "rmat", "sbm"])
+def test_generators_symmetric_and_seeded(nido_lib, kind):
+    c = nido_lib
+    make = {
+        "planted": lambda s: c.gen_planted(16, 32, 8.0, 0.8, c.W_INT8, s),
+        "rmat": lambda s: c.gen_rmat(1 << 10, 8 << 10, wmode=c.W_ONE, seed=s),
+        "sbm": lambda s: c.gen_sbm(3000, cmin=16, cmax=256, avg_degree=10.0, wmode=c.W_LOGNORMAL, seed=s),
+    }[kind]
+    g, g2, g3 = make(7), make(7), make(8)
+    assert np.array_equal(g.adj, g2.adj) and np.array_equal(g.w, g2.w)
+    assert not (g.ne == g3.ne and np.array_equal(g.adj, g3.adj))
+    src = np.repeat(np.arange(g.nv), np.diff(g.off))
+    fwd = dict(zip(zip(src.tolist(), g.adj.tolist()), g.w.tolist()))
+    assert all(fwd.get((v, u)) == w for (u, v), w in fwd.items())  # symmetric with equal weights
+    assert (g.adj != src).all() or kind != "rmat"  # R-MAT drops self-loops
+    for v in range(g.nv):  # sorted, no duplicates
+        row = g.adj[g.off[v]:g.off[v + 1]]
+        assert (np.diff(row) > 0).all()
+
+
+def test_pack_graphs_layout(nido_lib):
+    c = nido_lib
+    a = c.gen_planted(4, 8, 4.0, 0.8, c.W_INT8, 1)
+    b = c.Csr(np.zeros(1, np.int64), np.zeros(0, np.int64), np.zeros(0))
+    d = c.gen_rmat(64, 256, wmode=c.W_ONE, seed=3)
+    vbase, u = c.pack_graphs([a, b, d])
+    assert vbase.tolist() == [0, a.nv, a.nv, a.nv + d.nv]
+    assert u.nv == a.nv + d.nv and u.ne == a.ne + d.ne
+    assert np.array_equal(u.off[: a.nv + 1], a.off)
+    assert np.array_equal(u.off[a.nv:] - a.ne, d.off)
+    assert np.array_equal(u.adj[a.ne:] - a.nv, d.adj)
+    src = np.repeat(np.arange(u.nv), np.diff(u.off))
+    g_of = np.searchsorted(vbase, src, side="right") - 1
+    assert (u.adj >= vbase[g_of]).all() and (u.adj < vbase[g_of + 1]).all()
+
+
+CLI = os.path.join(ROOT, "nido_b200", "bin", "nido_louvain")
+
+
+@pytest.mark.skipif(not os.path.exists(CLI), reason="command-line program not built")
+def test_cli_options():
+    r = subprocess.run([CLI, "-h"], capture_output=True, text=True)
+    assert r.returncode == 0 and "-f" in r.stdout
+    r = subprocess.run([CLI, "-r", "100"], capture_output=True, text=True)
+    assert r.returncode != 0 and "not supported" in r.stderr
+    r = subprocess.run([CLI], capture_output=True, text=True)
+    assert r.returncode != 0 and "missing" in r.stderr
+    r = subprocess.run([CLI, "-f", "/nonexistent.bin"], capture_output=True, text=True)
+    assert r.returncode != 0
+
+
+def _free_port():
+    s = socket.socket()
+    s.bind(("127.0.0.1", 0))
+    port = s.getsockname()[1]
+    s.close()
+    return port
+
+
+def _replica_worker(rank, world, port, q):
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), WORLD_SIZE=str(world),
+                      RANK=str(rank), LOCAL_RANK=str(rank))
+    import sys
+    sys.path.insert(0, ROOT)
+    import bench
+    w, r, _ = bench.dist_setup(None)
+    bench.barrier(w)
+    mx = bench.reduce_max(10.0 + r, w)
+    import torch.distributed as dist
+    dist.destroy_process_group()
+    q.put((r, w, mx))
+
+
+def test_bench_replica_plumbing_gloo():
+    """bench.py --gpus 2 runs independent replicas: ranks meet only at the
+    barrier and the max-over-ranks of the timed region."""
+    import torch.multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    ps = [ctx.Process(target=_replica_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in ps:
+        p.start()
+    for p in ps:
+        p.join(120)
+        assert p.exitcode == 0
+    got = sorted(q.get(timeout=10) for _ in range(2))
+    assert got == [(0, 2, 11.0), (1, 2, 11.0)]
