@@ -66,15 +66,8 @@ WORKLOADS = {
 
 
 def make_graph(capi, name):
-    if name == "rmat22":
-        return capi.gen_rmat(1 << 22, 16 << 22, wmode=capi.W_ONE, seed=2)
-    if name == "rmat20":
-        return capi.gen_rmat(1 << 20, 16 << 20, wmode=capi.W_ONE, seed=2)
-    if name == "planted":
-        return capi.gen_planted(256, 256, 32.0, 0.8, capi.W_UNIFORM, 1)
-    if name == "sbm":
-        return capi.gen_sbm(1 << 24, 2.5, 16, 65536, 32.0, 0.7, capi.W_LOGNORMAL, True, 3)
-    raise SystemExit(f"unknown workload {name}")
+    from nido_b200 import workloads
+    return workloads.single_graph(name)
 
 
 class ClockSampler:

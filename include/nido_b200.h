@@ -59,7 +59,8 @@ typedef struct {
   double tau;        /* -t, default 1e-6 */
   int64_t max_iter;  /* -i, default 500 */
   int32_t verbose;   /* print the reference's per-loop lines to stdout */
-  int32_t reserved;
+  int32_t tune;      /* 1: autotune the degree tiers on the first phase of the
+                        first run of this graph (nido_tune), then keep them */
 } nido_params;
 
 /* Per-run statistics (the reference prints these, louvain_gpu.cpp:43-131). */
@@ -76,7 +77,7 @@ typedef struct {
   /* host wall time per section (ms): [0] restart from the uploaded graph,
    * [1] enqueueing moves and commits, [2] modularity including the wait for
    * the device, [3] aggregation, [4] per-phase preparation after
-   * aggregation, [5] download of the clustering */
+   * aggregation, [5] download of the clustering, [6] autotuning */
   double host_ms[8];
   double q_phase[200];
   int64_t loops_phase[200];
@@ -167,6 +168,26 @@ int nido_modularity_noalloc(void* stream, int64_t nv, const int64_t* d_off, cons
                             const double* d_w, const int64_t* d_comm, const double* d_a, double m,
                             double* d_q);
 
+/* ---- degree tiers and their autotuner (no reference counterpart: the reference
+ * bins by fixed degree bounds, graph_gpu.cpp:602-624) -------------------------- */
+typedef struct {
+  int32_t warp_max_degree;   /* one warp, 256-slot shared table; <= 128 */
+  int32_t cta_s_max_degree;  /* 128-thread CTA, 1024 slots; <= 512 */
+  int32_t cta_m_max_degree;  /* 256-thread CTA, 2048 slots; <= 1024 */
+  int32_t cta_l_max_degree;  /* 256-thread CTA, 4096 slots; <= 2048; above: hub tier */
+  int64_t hub_wave_slots;    /* hub-table slots processed together (L2 residency) */
+} nido_tier_config;
+/* Thresholds must be non-decreasing, at least 32 and within the capacities
+ * above; results on integer weights do not depend on them. */
+int nido_get_tier_config(nido_graph g, nido_tier_config* c);
+int nido_set_tier_config(nido_graph g, const nido_tier_config* c);
+/* Times `sweeps` move sweeps of every -b batch (no commit) on the graph's
+ * current state for candidate configurations (coordinate descent over the
+ * thresholds and the hub wave size), keeps the fastest and returns it with
+ * its sweep time.  Overwrites the move targets: call it before a run
+ * (nido_run starts from a fresh singleton partition). */
+int nido_tune(nido_graph g, int32_t tie_mode, int32_t sweeps, nido_tier_config* best, double* best_ms);
+
 /* ---- whole run: LouvainGPU::run (louvain_gpu.cpp:6-139) ------------------------ */
 /* Starts from the uploaded graph (any earlier coarsening is undone first).
  * out_comm (nv entries, may be NULL) receives the clustering of the original
@@ -209,8 +230,9 @@ typedef struct {
   int64_t hbm_bytes;   /* reservation held against the budget while it ran */
 } nido_request_info;
 /* Device bytes reserved for a graph of this size while it runs: the upload,
- * work buffers and scratch, the hub-table region (16 bytes a slot, at most
- * max(4M, 4*nv) slots) and 20 bytes per edge for the coarsening plan. */
+ * work buffers and scratch, plus the hub-table and coarsening-plan regions,
+ * which are processed in waves and so bounded by max(8M, 4*nv) and
+ * max(4M, 4*nv) slots. */
 int64_t nido_graph_footprint(int64_t nv, int64_t ne, int32_t nbatches);
 /* Device bytes a graph holds now (upload, scratch, hub tables, plan). */
 int nido_graph_device_bytes(nido_graph g, int64_t* bytes);

@@ -36,7 +36,7 @@ class _Csr(C.Structure):
 
 class _Params(C.Structure):
     _fields_ = [("nbatches", C.c_int32), ("tie_mode", C.c_int32), ("tau", C.c_double),
-                ("max_iter", C.c_int64), ("verbose", C.c_int32), ("reserved", C.c_int32)]
+                ("max_iter", C.c_int64), ("verbose", C.c_int32), ("tune", C.c_int32)]
 
 
 class RunStats(C.Structure):
@@ -49,6 +49,15 @@ class RunStats(C.Structure):
 
 
 _lib = None
+
+
+class TierConfig(C.Structure):
+    _fields_ = [("warp_max_degree", C.c_int32), ("cta_s_max_degree", C.c_int32),
+                ("cta_m_max_degree", C.c_int32), ("cta_l_max_degree", C.c_int32),
+                ("hub_wave_slots", C.c_int64)]
+
+    def as_dict(self):
+        return {f: getattr(self, f) for f, _ in self._fields_}
 
 
 class RequestInfo(C.Structure):
@@ -105,6 +114,9 @@ def lib() -> C.CDLL:
             "nido_batch_size": (C.c_int, [vp, C.POINTER(C.c_int32), _i64p, _i64p]),
             "nido_batch_free": (C.c_int, [vp]),
             "nido_graph_footprint": (C.c_int64, [C.c_int64, C.c_int64, C.c_int32]),
+            "nido_get_tier_config": (C.c_int, [vp, C.POINTER(TierConfig)]),
+            "nido_set_tier_config": (C.c_int, [vp, C.POINTER(TierConfig)]),
+            "nido_tune": (C.c_int, [vp, C.c_int32, C.c_int32, C.POINTER(TierConfig), _f64p]),
             "nido_graph_device_bytes": (C.c_int, [vp, _i64p]),
             "nido_server_create": (C.c_int, [C.c_int, C.c_size_t, C.c_int32, C.POINTER(vp)]),
             "nido_server_submit": (C.c_int, [vp, C.POINTER(_Csr), C.POINTER(_Params), _i64p, _i64p]),
@@ -363,15 +375,29 @@ class Graph:
         p = None if new_orders is None else _p64(np.ascontiguousarray(new_orders, dtype=np.int64))
         _check(lib().nido_dump_partition(self.h, path.encode(), p))
 
+    def tier_config(self) -> TierConfig:
+        c = TierConfig()
+        _check(lib().nido_get_tier_config(self.h, C.byref(c)))
+        return c
+
+    def set_tier_config(self, c: TierConfig):
+        _check(lib().nido_set_tier_config(self.h, C.byref(c)))
+
+    def tune(self, tie: int = NIDO_TIE_SMALLEST_ID, sweeps: int = 2):
+        c = TierConfig()
+        ms = C.c_double()
+        _check(lib().nido_tune(self.h, tie, sweeps, C.byref(c), C.byref(ms)))
+        return c, ms.value
+
     def device_bytes(self) -> int:
         b = C.c_int64()
         _check(lib().nido_graph_device_bytes(self.h, C.byref(b)))
         return b.value
 
     def run(self, tau: float = 1e-6, max_iter: int = 500, tie: int = NIDO_TIE_SMALLEST_ID,
-            verbose: bool = False):
+            verbose: bool = False, tune: bool = False):
         """LouvainGPU::run; returns (clustering of the input vertices, RunStats)."""
-        p = _Params(self.nbatches, tie, tau, max_iter, int(verbose), 0)
+        p = _Params(self.nbatches, tie, tau, max_iter, int(verbose), int(tune))
         out = np.empty(self.nv0, np.int64)
         st = RunStats()
         _check(lib().nido_run(self.h, C.byref(p), _p64(out), C.byref(st)))
@@ -428,10 +454,11 @@ class Batch:
     def __exit__(self, *a):
         self.close()
 
-    def run(self, tau: float = 1e-6, max_iter: int = 500, tie: int = NIDO_TIE_SMALLEST_ID):
+    def run(self, tau: float = 1e-6, max_iter: int = 500, tie: int = NIDO_TIE_SMALLEST_ID,
+            tune: bool = False):
         """Returns (per-graph clusterings, final Q per graph, phases per graph,
         loops per graph, RunStats)."""
-        p = _Params(self.nbatches, tie, tau, max_iter, 0, 0)
+        p = _Params(self.nbatches, tie, tau, max_iter, 0, int(tune))
         out = np.empty(self.nv, np.int64)
         q = np.empty(self.ngraphs, np.float64)
         ph = np.empty(self.ngraphs, np.int64)

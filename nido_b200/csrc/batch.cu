@@ -617,8 +617,13 @@ extern "C" int nido_batch_run(nido_batch B, const nido_params* p, int64_t* out_c
     NIDO_TRY(batch_list(B, act, base, &ql));  // synchronizes
     int64_t listed_v = 0, listed_e = 0;
     for (int32_t i : act) { listed_v += base[i + 1] - base[i]; listed_e += edges[i]; }
-    // singleton start and Q_old
+    // singleton start and Q_old (the tier autotuner, when asked, times move
+    // sweeps of the first phase and leaves the tier lists rebuilt)
     NIDO_TRY(launch_singleton(g));
+    if (p->tune && !g->tuned && phase == 0) {
+      NIDO_TRY(tune_tiers(g, p->tie_mode, 2, nullptr));
+      NIDO_TRY(launch_singleton(g));
+    }
     NIDO_CUDA_TRY(cudaMemsetAsync(B->gagg, 0, sizeof(int32_t) * ng, s));
     NIDO_CUDA_TRY(cudaMemsetAsync(B->giter, 0, sizeof(int32_t) * ng, s));
     NIDO_CUDA_TRY(cudaMemsetAsync(B->loops_phase, 0, sizeof(int32_t) * ng, s));

@@ -348,6 +348,9 @@ __global__ void __launch_bounds__(kAggThreads) k_agg_cta(const int32_t* __restri
 // first list position per id), count first occurrences per segment, and, after
 // a scan of the counts, emit every id at its first-occurrence rank.
 constexpr int kAggSeg = 4096;
+// table slots of one wave of giant coarse vertices (4M slots of key, first
+// position and value: 64 MB, L2 resident); one larger table is a wave alone
+constexpr int64_t kAggWaveSlots = (int64_t)4 << 20;
 
 struct SegArgs {
   const int2* __restrict__ items;
@@ -371,9 +374,10 @@ __device__ __forceinline__ void seg_range(const AggArgs& q, const SegArgs& a, in
   s1 = min(P1, s0 + kAggSeg);
 }
 
-__global__ void __launch_bounds__(256) k_agg_seg_insert(int64_t n, AggArgs q, SegArgs a) {
+// items [it0, it0 + n) of the list (one wave)
+__global__ void __launch_bounds__(256) k_agg_seg_insert(int64_t it0, int64_t n, AggArgs q, SegArgs a) {
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  for (int64_t it = blockIdx.x; it < n; it += gridDim.x) {
+  for (int64_t it = it0 + blockIdx.x; it < it0 + n; it += gridDim.x) {
     const int2 item = a.items[it];
     int cp;
     int64_t m0, m1, P0, s0, s1;
@@ -414,11 +418,12 @@ __global__ void __launch_bounds__(256) k_agg_seg_insert(int64_t n, AggArgs q, Se
 
 // count (kEmit false) or emit (kEmit true) first occurrences of a segment
 template <bool kEmit>
-__global__ void __launch_bounds__(256) k_agg_seg_scan(int64_t n, AggArgs q, SegArgs a, int64_t* segcnt) {
+__global__ void __launch_bounds__(256) k_agg_seg_scan(int64_t it0, int64_t n, AggArgs q, SegArgs a,
+                                                      int64_t* segcnt) {
   __shared__ int wsum[8];
   __shared__ int64_t running_s;
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  for (int64_t it = blockIdx.x; it < n; it += gridDim.x) {
+  for (int64_t it = it0 + blockIdx.x; it < it0 + n; it += gridDim.x) {
     const int2 item = a.items[it];
     int cp;
     int64_t m0, m1, P0, s0, s1;
@@ -564,7 +569,8 @@ int launch_aggregation(nido_graph_s* g, int* done) {
   }
   if (cnt[2] > 0) {
     // plan: per giant coarse vertex a table of >= 2*min(D, nvp) slots and
-    // ceil(D / kAggSeg) segment items
+    // ceil(D / kAggSeg) segment items; giants go in waves whose tables share
+    // one region of at most kAggWaveSlots slots (or one larger table)
     const int64_t n2 = cnt[2];
     const int32_t* list2 = list + cnt[0] + cnt[1];
     int64_t* dsz = ar.take<int64_t>(n2);
@@ -577,18 +583,25 @@ int launch_aggregation(nido_graph_s* g, int* done) {
     NIDO_CUDA_TRY(cudaMemcpyAsync(cids.data(), list2, sizeof(int32_t) * n2, cudaMemcpyDeviceToHost, s));
     NIDO_CUDA_TRY(cudaStreamSynchronize(s));
     std::vector<int64_t> toff(n2), first(n2 + 1);
+    std::vector<int64_t> wave_g{0};  // first giant of every wave, then n2
     std::vector<int2> items;
-    int64_t slots = 0;
+    int64_t slots = 0, wslots = 0;
     for (int64_t i = 0; i < n2; ++i) {
       const int64_t u = std::min<int64_t>(D[i], nvp);
       int64_t cap = 64;
       while (cap < 2 * u) cap <<= 1;
       caps[i] = (int32_t)cap;
-      toff[i] = slots;
-      slots += cap;
+      if (i > 0 && wslots + cap > kAggWaveSlots) {
+        wave_g.push_back(i);
+        wslots = 0;
+      }
+      toff[i] = wslots;
+      wslots += cap;
+      slots = std::max(slots, wslots);
       first[i] = (int64_t)items.size();
       for (int64_t sg = 0; sg * kAggSeg < D[i]; ++sg) items.push_back(make_int2((int)i, (int)sg));
     }
+    wave_g.push_back(n2);
     first[n2] = (int64_t)items.size();
     const int64_t ni = (int64_t)items.size();
     const size_t bytes = sizeof(int2) * ni + sizeof(int32_t) * 2 * n2 + sizeof(int64_t) * (2 * n2 + 1) +
@@ -619,20 +632,27 @@ int launch_aggregation(nido_graph_s* g, int* done) {
     NIDO_CUDA_TRY(cudaMemcpyAsync(dcaps, caps.data(), sizeof(int32_t) * n2, cudaMemcpyHostToDevice, s));
     NIDO_CUDA_TRY(cudaMemcpyAsync(dtoff, toff.data(), sizeof(int64_t) * n2, cudaMemcpyHostToDevice, s));
     NIDO_CUDA_TRY(cudaMemcpyAsync(dfirst, first.data(), sizeof(int64_t) * (n2 + 1), cudaMemcpyHostToDevice, s));
-    NIDO_CUDA_TRY(cudaMemsetAsync(tkeys, 0xff, sizeof(int32_t) * slots, s));
-    NIDO_CUDA_TRY(cudaMemsetAsync(tfpos, 0x7f, sizeof(int32_t) * slots, s));
-    NIDO_CUDA_TRY(cudaMemsetAsync(tvals, 0, sizeof(double) * slots, s));
     SegArgs sa{ditems, dcids, dtoff, dcaps, dfirst, tkeys, tvals, tfpos};
-    const unsigned gi = grid_for(ni, 1, kSMs * 8);
-    k_agg_seg_insert<<<gi, 256, 0, s>>>(ni, q, sa);
-    NIDO_LAUNCH_CHECK();
-    k_agg_seg_scan<false><<<gi, 256, 0, s>>>(ni, q, sa, segcnt);
-    NIDO_LAUNCH_CHECK();
-    NIDO_TRY(scan_exclusive_i64(segcnt, segcnt, ni, stemp, s));
-    k_agg_seg_scan<true><<<gi, 256, 0, s>>>(ni, q, sa, segcnt);
-    NIDO_LAUNCH_CHECK();
-    k_agg_seg_deg<<<grid_for(n2, 256, kSMs * 4), 256, 0, s>>>(n2, dcids, dfirst, segcnt, degp);
-    NIDO_LAUNCH_CHECK();
+    for (size_t wv = 0; wv + 1 < wave_g.size(); ++wv) {
+      const int64_t g0 = wave_g[wv], g1 = wave_g[wv + 1];
+      const int64_t i0 = first[g0], nw = first[g1] - i0;
+      const int64_t ws = toff[g1 - 1] + caps[g1 - 1];
+      NIDO_CUDA_TRY(cudaMemsetAsync(tkeys, 0xff, sizeof(int32_t) * ws, s));
+      NIDO_CUDA_TRY(cudaMemsetAsync(tfpos, 0x7f, sizeof(int32_t) * ws, s));
+      NIDO_CUDA_TRY(cudaMemsetAsync(tvals, 0, sizeof(double) * ws, s));
+      const unsigned gi = grid_for(nw, 1, kSMs * 8);
+      k_agg_seg_insert<<<gi, 256, 0, s>>>(i0, nw, q, sa);
+      NIDO_LAUNCH_CHECK();
+      k_agg_seg_scan<false><<<gi, 256, 0, s>>>(i0, nw, q, sa, segcnt);
+      NIDO_LAUNCH_CHECK();
+      // within the wave: each giant's output offsets need only differences
+      // of this scan (segcnt[i0 + nw] is overwritten by the next wave)
+      NIDO_TRY(scan_exclusive_i64(segcnt + i0, segcnt + i0, nw, stemp, s));
+      k_agg_seg_scan<true><<<gi, 256, 0, s>>>(i0, nw, q, sa, segcnt);
+      NIDO_LAUNCH_CHECK();
+      k_agg_seg_deg<<<grid_for(g1 - g0, 256, kSMs * 4), 256, 0, s>>>(g1 - g0, dcids + g0, dfirst + g0, segcnt, degp);
+      NIDO_LAUNCH_CHECK();
+    }
     NIDO_CUDA_TRY(cudaStreamSynchronize(s));  // the host plan vectors go out of scope
   }
   // coarse offsets into off2, then the entries into the work CSR (when the

@@ -188,8 +188,7 @@ extern "C" int nido_graph_free(nido_graph g) {
   // hub-tier buffers are sized per phase outside the budget accounting
   for (void* p : {(void*)g->gkeys, (void*)g->gvals, (void*)g->hub_items, (void*)g->hub_v, (void*)g->hub_capv,
                   (void*)g->hub_nseg, (void*)g->hub_toff, (void*)g->hub_done, (void*)g->hub_slices,
-                  (void*)g->hub_slice_first, (void*)g->hub_res, (void*)g->agg_buf, (void*)g->hub_occ,
-                  (void*)g->hub_nocc})
+                  (void*)g->hub_slice_first, (void*)g->hub_res, (void*)g->agg_buf})
     nido::raw_free(ctx, p);
   delete g;
   return NIDO_OK;
@@ -263,7 +262,7 @@ extern "C" int nido_graph_device_bytes(nido_graph g, int64_t* bytes) {
   if (!g || !bytes) return nido_set_error(NIDO_E_INVALID, "null argument");
   const int64_t V = g->cap_v, E = g->cap_e;
   int64_t b = 24 * (V + 1) + 36 * E + 28 * V + 4 * g->nv0 + 128 + (int64_t)g->scratch_bytes;
-  b += 16 * g->gslab + 4 * g->hub_cap_nocc + 8 * g->hub_cap_items + 4 * (g->hub_cap_hubs_v + g->hub_cap_hubs_c + g->hub_cap_hubs_s +
+  b += 12 * g->gslab + 8 * g->hub_cap_items + 4 * (g->hub_cap_hubs_v + g->hub_cap_hubs_c + g->hub_cap_hubs_s +
                                                    g->hub_cap_hubs_d) +
        8 * (g->hub_cap_hubs_t + g->hub_cap_slices + g->hub_cap_first) + g->hub_cap_res + (int64_t)g->agg_buf_bytes;
   *bytes = b;
@@ -472,6 +471,93 @@ extern "C" int nido_dump_partition(nido_graph g, const char* path, const int64_t
   return NIDO_OK;
 }
 
+// ---- degree-tier autotuner ------------------------------------------------------
+
+namespace nido {
+namespace {
+bool config_ok(const TierConfig& c) {
+  return c.warp_max >= 32 && c.warp_max <= kWarpMaxDeg && c.ctas_max >= c.warp_max && c.ctas_max <= kCtaSMaxDeg &&
+         c.ctam_max >= c.ctas_max && c.ctam_max <= kCtaMMaxDeg && c.ctal_max >= c.ctam_max &&
+         c.ctal_max <= kCtaLMaxDeg && c.hub_wave_slots >= 4096;
+}
+
+// one move sweep over every batch, timed on the device (ms)
+int time_sweeps(nido_graph_s* g, int tie, int sweeps, double* ms) {
+  cudaStream_t s = g->ctx->stream;
+  g->bins_valid = false;
+  NIDO_TRY(build_batches(g));
+  for (int b = 0; b < g->nbatches; ++b) NIDO_TRY(launch_move(g, b, tie, nullptr, nullptr));  // warm
+  NIDO_CUDA_TRY(cudaEventRecord(g->ctx->ev0, s));
+  for (int i = 0; i < sweeps; ++i)
+    for (int b = 0; b < g->nbatches; ++b) NIDO_TRY(launch_move(g, b, tie, nullptr, nullptr));
+  NIDO_CUDA_TRY(cudaEventRecord(g->ctx->ev1, s));
+  NIDO_CUDA_TRY(cudaEventSynchronize(g->ctx->ev1));
+  float t = 0.f;
+  NIDO_CUDA_TRY(cudaEventElapsedTime(&t, g->ctx->ev0, g->ctx->ev1));
+  *ms = t / sweeps;
+  return NIDO_OK;
+}
+}  // namespace
+
+int tune_tiers(nido_graph_s* g, int tie, int sweeps, double* best_ms) {
+  if (sweeps < 1) sweeps = 1;
+  TierConfig best = g->cfg;
+  double bt = 0.;
+  NIDO_TRY(time_sweeps(g, tie, sweeps, &bt));
+  // coordinate descent: each knob in turn, a candidate kept when 2% faster
+  auto try_cfg = [&](const TierConfig& c) -> int {
+    if (!config_ok(c)) return NIDO_OK;
+    g->cfg = c;
+    double t = 0.;
+    NIDO_TRY(time_sweeps(g, tie, sweeps, &t));
+    if (t < 0.98 * bt) { bt = t; best = c; }
+    g->cfg = best;
+    return NIDO_OK;
+  };
+  for (int32_t v : {1024, 1536}) { TierConfig c = best; c.ctal_max = v; NIDO_TRY(try_cfg(c)); }
+  for (int32_t v : {384, 256}) { TierConfig c = best; c.ctas_max = v; NIDO_TRY(try_cfg(c)); }
+  for (int32_t v : {96, 64}) { TierConfig c = best; c.warp_max = v; NIDO_TRY(try_cfg(c)); }
+  if (g->max_degree > best.ctal_max)
+    for (int64_t v : {(int64_t)2 << 20, (int64_t)8 << 20}) { TierConfig c = best; c.hub_wave_slots = v; NIDO_TRY(try_cfg(c)); }
+  g->cfg = best;
+  g->bins_valid = false;
+  NIDO_TRY(build_batches(g));
+  g->tuned = true;
+  if (best_ms) *best_ms = bt;
+  return NIDO_OK;
+}
+}  // namespace nido
+
+extern "C" int nido_get_tier_config(nido_graph g, nido_tier_config* c) {
+  if (!g || !c) return nido_set_error(NIDO_E_INVALID, "null argument");
+  *c = nido_tier_config{g->cfg.warp_max, g->cfg.ctas_max, g->cfg.ctam_max, g->cfg.ctal_max, g->cfg.hub_wave_slots};
+  return NIDO_OK;
+}
+
+extern "C" int nido_set_tier_config(nido_graph g, const nido_tier_config* c) {
+  if (!g || !c) return nido_set_error(NIDO_E_INVALID, "null argument");
+  TierConfig t;
+  t.warp_max = c->warp_max_degree;
+  t.ctas_max = c->cta_s_max_degree;
+  t.ctam_max = c->cta_m_max_degree;
+  t.ctal_max = c->cta_l_max_degree;
+  t.hub_wave_slots = c->hub_wave_slots;
+  if (!nido::config_ok(t)) return nido_set_error(NIDO_E_INVALID, "tier thresholds out of range or decreasing");
+  g->cfg = t;
+  g->bins_valid = false;
+  return nido::build_batches(g);
+}
+
+extern "C" int nido_tune(nido_graph g, int32_t tie_mode, int32_t sweeps, nido_tier_config* best, double* best_ms) {
+  if (!g) return nido_set_error(NIDO_E_INVALID, "null graph");
+  if (tie_mode != NIDO_TIE_SMALLEST_ID && tie_mode != NIDO_TIE_NIDO)
+    return nido_set_error(NIDO_E_INVALID, "unknown tie mode %d", tie_mode);
+  NIDO_CUDA_TRY(cudaSetDevice(g->ctx->device));
+  NIDO_TRY(nido::tune_tiers(g, tie_mode, sweeps, best_ms));
+  if (best) NIDO_TRY(nido_get_tier_config(g, best));
+  return NIDO_OK;
+}
+
 // LouvainGPU::run (louvain_gpu.cpp:28-124): phases of singleton start,
 // iterations of batched moves until dQ <= tau or max_iter, undo of an
 // iteration that lowered Q, and aggregation when the phase gained more
@@ -508,6 +594,11 @@ extern "C" int nido_run(nido_graph g, const nido_params* p, int64_t* out_comm, n
   int64_t phases = 0;
   while (!done && phases < 200) {
     if (p->verbose) printf("PHASE #%lld: \n", (long long)phases);
+    if (p->tune && !g->tuned && phases == 0) {
+      NIDO_TRY(nido::launch_singleton(g));
+      NIDO_TRY(nido::tune_tiers(g, p->tie_mode, 2, nullptr));
+      lap(6);
+    }
     NIDO_TRY(nido::launch_singleton(g));
     double Q;
     NIDO_TRY(nido::launch_modularity(g, &Q));

@@ -38,6 +38,17 @@ constexpr int kCtaSMaxDeg = 512;
 constexpr int kCtaMMaxDeg = 1024;
 constexpr int kCtaLMaxDeg = 2048;
 
+// Degree thresholds of the shared-memory tiers and the hub wave size.  The
+// defaults are the kernels' capacities; the tuner (engine.cu) may lower the
+// thresholds (a tier takes any degree up to its capacity) and pick the wave.
+struct TierConfig {
+  int32_t warp_max = kWarpMaxDeg;
+  int32_t ctas_max = kCtaSMaxDeg;
+  int32_t ctam_max = kCtaMMaxDeg;
+  int32_t ctal_max = kCtaLMaxDeg;
+  int64_t hub_wave_slots = (int64_t)4 << 20;
+};
+
 struct nido_ctx_s {
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -100,11 +111,6 @@ struct nido_graph_s {
   int32_t* hub_nseg = nullptr;
   int64_t* hub_toff = nullptr;
   int32_t* hub_done = nullptr;
-  // occupied slots of every hub table in insertion order (same offsets as the
-  // tables) and their counts, so the slice scans touch only used slots
-  int32_t* hub_occ = nullptr;
-  int32_t* hub_nocc = nullptr;
-  int64_t hub_cap_nocc = 0;
   int64_t hub_cap_items = 0, hub_cap_hubs_v = 0, hub_cap_hubs_c = 0, hub_cap_hubs_s = 0,
           hub_cap_hubs_t = 0, hub_cap_hubs_d = 0;
   int64_t nhubs = 0;
@@ -141,6 +147,8 @@ struct nido_graph_s {
   std::vector<int64_t> tier_off; // host: nbatches*kNumTiers+1 offsets into perm
   bool bins_valid = false;
   int64_t max_degree = 0;
+  TierConfig cfg;
+  bool tuned = false;
   double host_pinned_dummy = 0;
 };
 
@@ -183,6 +191,9 @@ int build_batches(nido_graph_s* g);                     // cuts (host) + tier li
 int launch_move(nido_graph_s* g, int batch, int tie, cudaEvent_t ev_start, cudaEvent_t ev_end);
 int plan_hubs(nido_graph_s* g);          // per phase, after the tier lists
 int move_init_attributes();              // once per device
+// times `sweeps` move sweeps (no commit) for candidate tier configurations
+// and keeps the fastest in g->cfg (engine.cu); clobbers newc
+int tune_tiers(nido_graph_s* g, int tie, int sweeps, double* best_ms);
 // coarsening (coarsen.cu)
 int launch_aggregation(nido_graph_s* g, int* done);
 

@@ -582,16 +582,15 @@ __global__ void __launch_bounds__(kHubThreads) k_move_hub(const int2* __restrict
 // (k_hub_combine).  The reference's tie rule needs ranks over the whole
 // table and uses k_move_hub instead.
 constexpr int kHubSlice = 4096;
-// table slots of one wave of hubs: 4M slots (48 MB of keys and values) leave
-// room in the 126 MB L2 for the streamed adjacency and the gathers
-constexpr int64_t kHubWaveSlots = (int64_t)4 << 20;
+// The table slots of one wave of hubs come from the graph's tier
+// configuration (default 4M slots: 48 MB of keys and values, which leaves
+// room in the 126 MB L2 for the streamed adjacency and the gathers).
 
 __global__ void __launch_bounds__(kHubThreads) k_hub_insert(const int2* __restrict__ items, int64_t n,
                                                             const int32_t* __restrict__ hub_v,
                                                             const int64_t* __restrict__ hub_toff,
                                                             const int32_t* __restrict__ hub_cap, int32_t* gkeys,
-                                                            double* gvals, int32_t* __restrict__ hub_occ,
-                                                            int32_t* __restrict__ hub_nocc, MoveArgs p) {
+                                                            double* gvals, MoveArgs p) {
   const int wid = threadIdx.x >> 5;
   for (int64_t it = blockIdx.x; it < n; it += gridDim.x) {
     const int2 item = items[it];
@@ -600,8 +599,8 @@ __global__ void __launch_bounds__(kHubThreads) k_hub_insert(const int2* __restri
     Table t;
     t.keys = gkeys + hub_toff[h];
     t.vals = gvals + hub_toff[h];
-    t.occ = hub_occ + hub_toff[h];
-    t.nocc = hub_nocc + h;
+    t.occ = nullptr;
+    t.nocc = nullptr;
     t.mask = (unsigned)hub_cap[h] - 1;
     const int64_t s = p.off[v], eend = p.off[v + 1];
     const int64_t s0 = s + (int64_t)item.y * kHubSeg;
@@ -617,16 +616,16 @@ struct SliceResult {
   int pad;
 };
 
-// Slice y of hub x covers entries [y*kHubSlice, (y+1)*kHubSlice) of the
-// hub's occupied-slot list (slices past the hub's count return at once);
-// every listed slot is read and cleared.  The tables of a wave are L2
-// resident, so the scattered slot reads stay on chip.
+// Slice y of hub x covers slots [y*kHubSlice, (y+1)*kHubSlice) of the hub's
+// table, read and cleared in order.  (A per-hub list of occupied slots,
+// appended during the merge, measured twice as slow on R-MAT scale 22: the
+// hub tables are mostly full and the list's counter is one contended
+// address per hub.)
 template <bool kMulti>
 __global__ void __launch_bounds__(kHubThreads) k_hub_slices(const int2* __restrict__ slices, int64_t n,
                                                             const int32_t* __restrict__ hub_v,
                                                             const int64_t* __restrict__ hub_toff,
-                                                            const int32_t* __restrict__ hub_occ,
-                                                            const int32_t* __restrict__ hub_nocc, int32_t* gkeys,
+                                                            const int32_t* __restrict__ hub_cap, int32_t* gkeys,
                                                             double* gvals, MoveArgs p,
                                                             SliceResult* __restrict__ res) {
   __shared__ double sg[32];
@@ -634,15 +633,10 @@ __global__ void __launch_bounds__(kHubThreads) k_hub_slices(const int2* __restri
   __shared__ int sc[32];
   for (int64_t it = blockIdx.x; it < n; it += gridDim.x) {
     const int2 sl = slices[it];
-    const int len = min(kHubSlice, hub_nocc[sl.x] - sl.y * kHubSlice);
-    if (len <= 0) {  // uniform over the block
-      if (threadIdx.x == 0) res[it] = SliceResult{-NIDO_MAX_FLOAT, 0., kNoKey, -1, 0};
-      continue;
-    }
+    const int len = min(kHubSlice, hub_cap[sl.x] - sl.y * kHubSlice);
     const int v = hub_v[sl.x];
-    int* keys = gkeys + hub_toff[sl.x];
-    double* vals = gvals + hub_toff[sl.x];
-    const int32_t* occ = hub_occ + hub_toff[sl.x] + (int64_t)sl.y * kHubSlice;
+    int* keys = gkeys + hub_toff[sl.x] + (int64_t)sl.y * kHubSlice;
+    double* vals = gvals + hub_toff[sl.x] + (int64_t)sl.y * kHubSlice;
     const int own = p.comm[v];
     const double ki = p.k[v];
     const double m = vertex_mass<kMulti>(p, v);
@@ -650,11 +644,11 @@ __global__ void __launch_bounds__(kHubThreads) k_hub_slices(const int2* __restri
     unsigned long long tk = kNoKey;
     int cand = -1;
     for (int i = threadIdx.x; i < len; i += kHubThreads) {
-      const int slot = occ[i];
-      const int cc = keys[slot];
-      const double val = vals[slot];
-      keys[slot] = -1;
-      vals[slot] = 0.;
+      const int cc = keys[i];
+      if (cc < 0) continue;
+      const double val = vals[i];
+      keys[i] = -1;
+      vals[i] = 0.;
       if (cc == own) {
         eown = val;
       } else {
@@ -670,7 +664,7 @@ __global__ void __launch_bounds__(kHubThreads) k_hub_slices(const int2* __restri
 
 template <bool kMulti>
 __global__ void k_hub_combine(int64_t nh, const int32_t* __restrict__ hub_v, const int64_t* __restrict__ slice_first,
-                              const SliceResult* __restrict__ res, int32_t* __restrict__ hub_nocc, MoveArgs p) {
+                              const SliceResult* __restrict__ res, MoveArgs p) {
   const int lane = threadIdx.x & 31;
   const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
@@ -691,7 +685,6 @@ __global__ void k_hub_combine(int64_t nh, const int32_t* __restrict__ hub_v, con
       const int v = hub_v[h];
       const int own = p.comm[v];
       decide(p, vertex_mass<kMulti>(p, v), v, own, p.k[v], p.a[own], eown, g, cand);
-      hub_nocc[h] = 0;  // every slice of this hub has read its count
     }
   }
 }
@@ -755,7 +748,7 @@ int plan_hubs(nido_graph_s* g) {
     hseg[i] = (int32_t)((d + kHubSeg - 1) / kHubSeg);
   }
   // Hubs are listed by batch within the tier.  Each batch's hubs are cut into
-  // waves whose tables together hold at most kHubWaveSlots slots (so they stay
+  // waves whose tables together hold at most cfg.hub_wave_slots slots (so they stay
   // in L2); table offsets are relative to the wave, and every wave reuses the
   // same region because its slice scan clears the tables.  Items and table
   // slices of a hub follow one another.
@@ -769,7 +762,7 @@ int plan_hubs(nido_graph_s* g) {
     const int64_t a1 = g->tier_off[(size_t)kTierHub * nb + b + 1] - h0;
     int64_t wslots = 0;
     for (int64_t i = a0; i < a1; ++i) {
-      if (i == a0 || wslots + hcap[i] > kHubWaveSlots) {
+      if (i == a0 || wslots + hcap[i] > g->cfg.hub_wave_slots) {
         g->hub_waves.push_back({(int64_t)items.size(), 0, (int64_t)slices.size(), 0, i, 0});
         wslots = 0;
       }
@@ -799,19 +792,14 @@ int plan_hubs(nido_graph_s* g) {
   NIDO_TRY(ensure(g, &g->hub_res, &g->hub_cap_res, (int64_t)(slices.size() * sizeof(SliceResult))));
   NIDO_CUDA_TRY(cudaMemcpyAsync(g->hub_slices, slices.data(), sizeof(int2) * slices.size(), cudaMemcpyHostToDevice, s));
   NIDO_CUDA_TRY(cudaMemcpyAsync(g->hub_slice_first, sfirst.data(), sizeof(int64_t) * (nh + 1), cudaMemcpyHostToDevice, s));
-  NIDO_TRY(ensure(g, &g->hub_nocc, &g->hub_cap_nocc, nh));
-  NIDO_CUDA_TRY(cudaMemsetAsync(g->hub_nocc, 0, sizeof(int32_t) * nh, s));
   if (toff > g->gslab) {
     raw_free(g->ctx, g->gkeys);
     raw_free(g->ctx, g->gvals);
-    raw_free(g->ctx, g->hub_occ);
     g->gkeys = nullptr;
     g->gvals = nullptr;
-    g->hub_occ = nullptr;
     g->gslab = 0;
     NIDO_CUDA_TRY(raw_alloc(g->ctx, (void**)&g->gkeys, sizeof(int32_t) * (size_t)toff));
     NIDO_CUDA_TRY(raw_alloc(g->ctx, (void**)&g->gvals, sizeof(double) * (size_t)toff));
-    NIDO_CUDA_TRY(raw_alloc(g->ctx, (void**)&g->hub_occ, sizeof(int32_t) * (size_t)toff));
     NIDO_CUDA_TRY(cudaMemsetAsync(g->gkeys, 0xff, sizeof(int32_t) * (size_t)toff, s));
     NIDO_CUDA_TRY(cudaMemsetAsync(g->gvals, 0, sizeof(double) * (size_t)toff, s));
     g->gslab = toff;
@@ -898,15 +886,14 @@ int launch_tiers(nido_graph_s* g, int batch, int tie, const MoveArgs& p) {
             continue;
           }
           k_hub_insert<<<grid_cap(w.i1 - w.i0, kSMs * 8), kHubThreads, 0, s>>>(
-              items, w.i1 - w.i0, g->hub_v, g->hub_toff, g->hub_capv, g->gkeys, g->gvals, g->hub_occ,
-              g->hub_nocc, p);
+              items, w.i1 - w.i0, g->hub_v, g->hub_toff, g->hub_capv, g->gkeys, g->gvals, p);
           NIDO_LAUNCH_CHECK();
           k_hub_slices<kMulti><<<grid_cap(w.s1 - w.s0, kSMs * 8), kHubThreads, 0, s>>>(
-              g->hub_slices + w.s0, w.s1 - w.s0, g->hub_v, g->hub_toff, g->hub_occ, g->hub_nocc, g->gkeys,
-              g->gvals, p, res + w.s0);
+              g->hub_slices + w.s0, w.s1 - w.s0, g->hub_v, g->hub_toff, g->hub_capv, g->gkeys, g->gvals, p,
+              res + w.s0);
           NIDO_LAUNCH_CHECK();
           k_hub_combine<kMulti><<<grid_cap((w.h1 - w.h0 + 7) / 8, kSMs * 4), 256, 0, s>>>(
-              w.h1 - w.h0, g->hub_v + w.h0, g->hub_slice_first + w.h0, res, g->hub_nocc + w.h0, p);
+              w.h1 - w.h0, g->hub_v + w.h0, g->hub_slice_first + w.h0, res, p);
           NIDO_LAUNCH_CHECK();
         }
         continue;

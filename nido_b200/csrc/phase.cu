@@ -214,15 +214,16 @@ __global__ void k_batch_cuts(const int64_t* __restrict__ off, int64_t nv, int nb
   batch_cuts(off, nv, nb, cuts, parts);
 }
 
-__device__ __forceinline__ int tier_of(int64_t d) {
+// thr = (warp, CTA-S, CTA-M, CTA-L) maximum degrees
+__device__ __forceinline__ int tier_of(int64_t d, int4 thr) {
   if (d <= 4) return kTierG4;
   if (d <= 8) return kTierG8;
   if (d <= 16) return kTierG16;
   if (d <= 32) return kTierG32;
-  if (d <= kWarpMaxDeg) return kTierWarp;
-  if (d <= kCtaSMaxDeg) return kTierCtaS;
-  if (d <= kCtaMMaxDeg) return kTierCtaM;
-  if (d <= kCtaLMaxDeg) return kTierCtaL;
+  if (d <= thr.x) return kTierWarp;
+  if (d <= thr.y) return kTierCtaS;
+  if (d <= thr.z) return kTierCtaM;
+  if (d <= thr.w) return kTierCtaL;
   return kTierHub;
 }
 
@@ -238,7 +239,7 @@ __global__ void k_tier_keys(const int64_t* __restrict__ off, int64_t nv, const i
                             int64_t* __restrict__ counts, unsigned long long* __restrict__ maxdeg,
                             const int32_t* __restrict__ gid, const int64_t* __restrict__ gbase,
                             const int64_t* __restrict__ gcuts, const int32_t* __restrict__ gactive,
-                            int32_t* __restrict__ vbatch) {
+                            int32_t* __restrict__ vbatch, int4 thr) {
   const int lane = threadIdx.x & 31;
   const uint32_t skip = (uint32_t)(kNumTiers * nb);
   unsigned long long md = 0;
@@ -263,7 +264,7 @@ __global__ void k_tier_keys(const int64_t* __restrict__ off, int64_t nv, const i
       }
       if (vbatch) vbatch[v] = lo;
       const int64_t d = off[v + 1] - off[v];
-      key = active ? (uint32_t)(tier_of(d) * nb + lo) : skip;
+      key = active ? (uint32_t)(tier_of(d, thr) * nb + lo) : skip;
       keys[v] = key;
       vals[v] = (uint32_t)v;
       if (active) md = md > (unsigned long long)d ? md : (unsigned long long)d;
@@ -408,7 +409,9 @@ int build_batches(nido_graph_s* g) {
   if (nv > 0) {
     k_tier_keys<<<grid_for(nv, kThreads), kThreads, 0, s>>>(g->off, nv, dcuts, nb, keys, (uint32_t*)g->perm,
                                                            counts, maxdeg, g->gid, g->gbase, g->gcuts,
-                                                           g->gactive, g->vbatch);
+                                                           g->gactive, g->vbatch,
+                                                           make_int4(g->cfg.warp_max, g->cfg.ctas_max,
+                                                                     g->cfg.ctam_max, g->cfg.ctal_max));
     NIDO_LAUNCH_CHECK();
     int bits = 0;
     while (((int64_t)1 << bits) < nkeys + 1) ++bits;

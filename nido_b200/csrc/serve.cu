@@ -119,17 +119,19 @@ void worker_loop(nido_server_s* S, int wid) {
 }  // namespace
 
 // Upload (three CSR copies, per-vertex state, scratch as nido_graph_upload
-// sizes them); the hub-table region, which holds one wave of tables (at most
-// 4M slots, or one table of up to 4*nv slots) at 16 bytes a slot; and an
-// allowance of 20 bytes per edge for the coarsening plan of giant
-// communities, plus the hub work lists.
+// sizes them); the hub-table region, one wave of tables at 12 bytes a slot
+// (at most 8M slots, or one table of up to 4*nv slots); the coarsening
+// plan's region for giant communities, one wave at 16 bytes a slot (at most
+// 4M slots or one table of up to 4*nv), grown by a quarter, plus its
+// per-vertex and per-segment lists; and the hub work lists.
 extern "C" int64_t nido_graph_footprint(int64_t nv, int64_t ne, int32_t nbatches) {
   (void)nbatches;
   const int64_t V = std::max<int64_t>(nv, 1), E = std::max<int64_t>(ne, 1);
   int64_t b = 24 * (V + 1) + 36 * E + 32 * V + 128;
   b += 64 * (V + 1) + (1 << 20) + 8 * (nido::radix_temp_elems(V) + nido::scan_temp_elems(E + 1));
-  b += 16 * std::max<int64_t>((int64_t)4 << 20, 4 * V);
-  b += 20 * E + (16 << 20);
+  b += 12 * std::max<int64_t>((int64_t)8 << 20, 4 * V);
+  b += 20 * std::max<int64_t>((int64_t)4 << 20, 4 * V) + 40 * V + E / 32;
+  b += (int64_t)32 << 20;
   return b;
 }
 

@@ -20,6 +20,24 @@ import numpy as np
 from . import capi
 
 
+def single_graph(name: str) -> capi.Csr:
+    """The one-graph workloads: 'rmat22' (R-MAT scale 22, edge factor 16,
+    (0.57,0.19,0.19,0.05), weights 1.0, seed 2), 'rmat20' (the same at scale
+    20), 'planted' (65,536 vertices in 256 blocks, average degree 32, 80%
+    intra, U[0.5,1.5] weights, seed 1), 'sbm' (16,777,216 vertices, power-law
+    communities 2.5 in 16..65,536, average degree 32, 70% intra, lognormal
+    weights, seed 3)."""
+    if name == "rmat22":
+        return capi.gen_rmat(1 << 22, 16 << 22, wmode=capi.W_ONE, seed=2)
+    if name == "rmat20":
+        return capi.gen_rmat(1 << 20, 16 << 20, wmode=capi.W_ONE, seed=2)
+    if name == "planted":
+        return capi.gen_planted(256, 256, 32.0, 0.8, capi.W_UNIFORM, 1)
+    if name == "sbm":
+        return capi.gen_sbm(1 << 24, 2.5, 16, 65536, 32.0, 0.7, capi.W_LOGNORMAL, True, 3)
+    raise ValueError(f"unknown workload {name}")
+
+
 def many_graph_plan(ngraphs: int = 4096, seed: int = 4, max_edges: float = 1.5e9,
                     vmin: int = 100, vmax: int = 1_000_000):
     """(vertex counts, average degrees, kinds) with kind 0 = SBM, 1 = R-MAT."""

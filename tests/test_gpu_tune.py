@@ -1,0 +1,58 @@
+"""Degree-tier configuration and its autotuner: any valid configuration gives
+the same results on integer weights (bit for bit), the tuner returns a valid
+configuration, and invalid ones are rejected."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def rmat16(nido_lib):
+    return nido_lib.gen_rmat(1 << 16, 16 << 16, wmode=nido_lib.W_INT8, seed=71)
+
+
+def test_lowered_thresholds_same_result(nido_lib, ctx, rmat16):
+    with nido_lib.Graph(ctx, rmat16, 2) as g:
+        want, st0 = g.run()
+        c = g.tier_config()
+        assert (c.warp_max_degree, c.cta_s_max_degree, c.cta_m_max_degree, c.cta_l_max_degree) == (128, 512, 1024, 2048)
+        for warp, ctas, ctam, ctal, wave in ((64, 256, 1024, 1024, 1 << 16), (32, 32, 32, 32, 1 << 16),
+                                             (96, 384, 768, 1536, 8 << 20)):
+            c = nido_lib.TierConfig(warp, ctas, ctam, ctal, wave)
+            g.set_tier_config(c)
+            got, st = g.run()
+            assert np.array_equal(got, want)
+            assert st.final_q == st0.final_q and st.total_loops == st0.total_loops
+
+
+def test_invalid_configs_rejected(nido_lib, ctx, rmat16):
+    with nido_lib.Graph(ctx, rmat16, 2) as g:
+        for bad in ((129, 512, 1024, 2048, 1 << 20), (128, 100, 1024, 2048, 1 << 20),
+                    (64, 512, 1025, 2048, 1 << 20), (64, 512, 1024, 4096, 1 << 20), (64, 512, 1024, 2048, 10)):
+            with pytest.raises(nido_lib.NidoError):
+                g.set_tier_config(nido_lib.TierConfig(*bad))
+
+
+@pytest.mark.parametrize("tie", [0, 1])
+def test_tuned_run_same_result(nido_lib, ctx, rmat16, tie):
+    with nido_lib.Graph(ctx, rmat16, 2) as g:
+        want, _ = g.run(tie=tie)
+    with nido_lib.Graph(ctx, rmat16, 2) as g:
+        got, st = g.run(tie=tie, tune=True)
+        c = g.tier_config()
+        assert 32 <= c.warp_max_degree <= c.cta_s_max_degree <= c.cta_m_max_degree <= c.cta_l_max_degree <= 2048
+        assert st.host_ms[6] > 0
+        assert np.array_equal(got, want)
+        best, ms = g.tune(tie=tie)
+        assert ms > 0
+
+
+def test_tuned_batch_same_result(nido_lib, ctx):
+    gs = [nido_lib.gen_rmat(1 << s, 12 << s, wmode=nido_lib.W_INT8, seed=80 + s) for s in (9, 12, 14, 15)]
+    with nido_lib.Batch(ctx, gs, 2) as b:
+        want = b.run()[0]
+    with nido_lib.Batch(ctx, gs, 2) as b:
+        got = b.run(tune=True)[0]
+    for x, y in zip(want, got):
+        assert np.array_equal(x, y)

@@ -144,3 +144,39 @@ def test_bench_replica_plumbing_gloo():
         assert p.exitcode == 0
     got = sorted(q.get(timeout=10) for _ in range(2))
     assert got == [(0, 2, 11.0), (1, 2, 11.0)]
+
+
+def test_many_graph_plan_rule():
+    """4,096 graphs, log-uniform sizes scaled so the drawn directed edges total
+    1.5e9 (clamped at 100 vertices), 50/50 SBM / R-MAT, degrees in [8, 64]."""
+    from nido_b200 import workloads as W
+    V, d, kind = W.many_graph_plan()
+    assert len(V) == 4096 and V.min() >= 100
+    assert (d >= 8).all() and (d <= 64).all()
+    assert 0.45 < kind.mean() < 0.55
+    assert abs((V * d).sum() / 1.5e9 - 1) < 0.02  # clamping adds a little
+    V2, _, _ = W.many_graph_plan(max_edges=1e15)  # no scaling: the drawn law itself
+    lv = np.log10(V2)
+    assert 2.0 <= lv.min() and lv.max() <= 6.0 and abs(lv.mean() - 4.0) < 0.1
+    assert np.array_equal(W.many_graph_plan()[0], V)  # seeded
+
+
+def test_serving_requests_law():
+    from nido_b200 import workloads as W
+    t, V, kind = W.serving_requests(4000, rate=10.0)
+    gaps = np.diff(np.concatenate([[0.0], t]))
+    assert abs(gaps.mean() - 0.1) < 0.01 and abs(gaps.std() - 0.1) < 0.01  # exponential
+    lv = np.log10(V)
+    assert 3.0 <= lv.min() and lv.max() <= 7.0 and abs(lv.mean() - 5.0) < 0.1
+
+
+def test_many_graphs_packed_small(nido_lib):
+    from nido_b200 import workloads as W
+    vbase, u, (V, d, kind) = W.many_graphs_packed(24, max_edges=2e5)
+    assert vbase[-1] == u.nv and len(vbase) == 25 and np.array_equal(np.diff(vbase), V)
+    src = np.repeat(np.arange(u.nv), np.diff(u.off))
+    g_of = np.searchsorted(vbase, src, side="right") - 1
+    assert (u.adj >= vbase[g_of]).all() and (u.adj < vbase[g_of + 1]).all()
+    assert (u.w >= 1).all() and (u.w == np.round(u.w)).all()  # integer weights (duplicates summed)
+    g5 = W.unpack(vbase, u, 5)
+    assert g5.nv == V[5] and g5.off[0] == 0 and (g5.adj < V[5]).all()
