@@ -205,8 +205,8 @@ __device__ __forceinline__ int table_add(const Table& t, int c, double e, bool& 
   unsigned h = hash_slot(c, t.mask);
   volatile int* vk = t.keys;
   isnew = false;
-  if (kGlobal) {
-    for (unsigned probe = 0; probe <= t.mask; ++probe) {
+  for (unsigned probe = 0; probe <= t.mask; ++probe) {
+    if constexpr (kGlobal) {
       const int old = atomicCAS(&t.keys[h], -1, c);
       if (old == -1 || old == c) {
         isnew = old == -1;
@@ -214,11 +214,8 @@ __device__ __forceinline__ int table_add(const Table& t, int c, double e, bool& 
         return (int)h;
       }
       h = (h + 1) & t.mask;
+      continue;
     }
-    atomicAdd(err, 1ull);
-    return -1;
-  }
-  for (unsigned probe = 0; probe <= t.mask; ++probe) {
     const int kk = vk[h];
     bool hit = kk == c;
     if (!hit && kk == -1) {
@@ -295,6 +292,61 @@ __device__ __forceinline__ void accumulate_edges(const MoveArgs& p, int v, int64
       occ_append(t, isnew, slot);
       if (!kAtomicVals) __syncwarp();
     }
+  }
+}
+
+// Hub segments (smallest-id rule): like accumulate_edges into a global
+// table, but every lane keeps the compare-and-swaps of its kUnroll chunks in
+// flight together instead of finishing one chunk's probe before the next.
+// Equal communities within a chunk are still folded onto one lane first.
+template <int kUnroll>
+__device__ __forceinline__ void merge_edges_global(const MoveArgs& p, int v, int64_t first, int64_t eend,
+                                                   int64_t stride, int* keys, double* vals, unsigned mask) {
+  const int lane = threadIdx.x & 31;
+  for (int64_t base = first; base < eend; base += kUnroll * stride) {
+    int u[kUnroll], c[kUnroll];
+    double wt[kUnroll];
+    unsigned h[kUnroll];
+#pragma unroll
+    for (int k = 0; k < kUnroll; ++k) {
+      const int64_t j = base + k * stride + lane;
+      u[k] = -1;
+      wt[k] = 0.;
+      if (j < eend) {
+        u[k] = p.adj[j];
+        wt[k] = p.w[j];
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < kUnroll; ++k) {
+      c[k] = u[k] >= 0 ? p.comm[u[k]] : -1;
+      if (u[k] == v) wt[k] = 0.;
+    }
+    unsigned pending = 0u;
+#pragma unroll
+    for (int k = 0; k < kUnroll; ++k) {
+      const bool ok = u[k] >= 0;
+      const unsigned peers = __match_any_sync(NIDO_FULL_MASK, c[k]);
+      wt[k] = fold_peers(peers, ok, wt[k]);
+      if (ok && lane == __ffs(peers) - 1) pending |= 1u << k;
+      h[k] = ok ? hash_slot(c[k], mask) : 0u;
+    }
+    for (unsigned probe = 0; pending != 0u && probe <= mask; ++probe) {
+      int old[kUnroll];
+#pragma unroll
+      for (int k = 0; k < kUnroll; ++k) old[k] = (pending >> k & 1u) ? atomicCAS(&keys[h[k]], -1, c[k]) : 0;
+#pragma unroll
+      for (int k = 0; k < kUnroll; ++k) {
+        if (!(pending >> k & 1u)) continue;
+        if (old[k] == -1 || old[k] == c[k]) {
+          atomicAdd(&vals[h[k]], wt[k]);
+          pending &= ~(1u << k);
+        } else {
+          h[k] = (h[k] + 1) & mask;
+        }
+      }
+    }
+    if (pending != 0u) atomicAdd(p.err, 1ull);
   }
 }
 
@@ -596,15 +648,10 @@ __global__ void __launch_bounds__(kHubThreads) k_hub_insert(const int2* __restri
     const int2 item = items[it];
     const int h = item.x;
     const int v = hub_v[h];
-    Table t;
-    t.keys = gkeys + hub_toff[h];
-    t.vals = gvals + hub_toff[h];
-    t.occ = nullptr;
-    t.nocc = nullptr;
-    t.mask = (unsigned)hub_cap[h] - 1;
     const int64_t s = p.off[v], eend = p.off[v + 1];
     const int64_t s0 = s + (int64_t)item.y * kHubSeg;
-    accumulate_edges<true, 4, true>(p, v, s0 + (int64_t)wid * 32, min(eend, s0 + kHubSeg), kHubThreads, t);
+    merge_edges_global<4>(p, v, s0 + (int64_t)wid * 32, min(eend, s0 + kHubSeg), kHubThreads, gkeys + hub_toff[h],
+                          gvals + hub_toff[h], (unsigned)hub_cap[h] - 1);
   }
 }
 
@@ -643,17 +690,34 @@ __global__ void __launch_bounds__(kHubThreads) k_hub_slices(const int2* __restri
     double g = -NIDO_MAX_FLOAT, eown = 0.;
     unsigned long long tk = kNoKey;
     int cand = -1;
-    for (int i = threadIdx.x; i < len; i += kHubThreads) {
-      const int cc = keys[i];
-      if (cc < 0) continue;
-      const double val = vals[i];
-      keys[i] = -1;
-      vals[i] = 0.;
-      if (cc == own) {
-        eown = val;
-      } else {
-        const double gg = gain_of(val, ki, p.a[cc], m);
-        if (better(gg, (unsigned)cc, g, tk)) { g = gg; tk = (unsigned)cc; cand = cc; }
+    // four slots per thread at a time, so their a_c gathers are in flight together
+    constexpr int U = 4;
+    for (int i0 = threadIdx.x; i0 < len; i0 += U * kHubThreads) {
+      int cc[U];
+      double val[U], ac[U];
+#pragma unroll
+      for (int k = 0; k < U; ++k) {
+        const int i = i0 + k * kHubThreads;
+        cc[k] = -1;
+        if (i < len) {
+          cc[k] = keys[i];
+          val[k] = vals[i];
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < U; ++k) ac[k] = (cc[k] >= 0 && cc[k] != own) ? p.a[cc[k]] : 0.;
+#pragma unroll
+      for (int k = 0; k < U; ++k) {
+        if (cc[k] < 0) continue;
+        const int i = i0 + k * kHubThreads;
+        keys[i] = -1;
+        vals[i] = 0.;
+        if (cc[k] == own) {
+          eown = val[k];
+        } else {
+          const double gg = gain_of(val[k], ki, ac[k], m);
+          if (better(gg, (unsigned)cc[k], g, tk)) { g = gg; tk = (unsigned)cc[k]; cand = cc[k]; }
+        }
       }
     }
     eown = block_sum(eown, sg);
