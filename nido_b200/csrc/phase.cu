@@ -120,6 +120,34 @@ __global__ void k_commit(int64_t v0, int64_t v1, const double* __restrict__ k,
 }
 
 // ---- modularity -------------------------------------------------------------------
+// Sum of w[j] over j = j0, j0+step, ... < e with comm[adj[j]] == own, added in
+// that order; four edges' loads are issued before any is added, so four
+// dependent gathers are in flight per lane.
+__device__ __forceinline__ double own_weight(const int32_t* __restrict__ adj, const double* __restrict__ w,
+                                             const int32_t* __restrict__ comm, int32_t own, int64_t j0,
+                                             int64_t e, int step) {
+  double x = 0.;
+  int64_t j = j0;
+  for (; j + 3 * (int64_t)step < e; j += 4 * (int64_t)step) {
+    int u[4];
+    double wt[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      u[k] = adj[j + k * step];
+      wt[k] = w[j + k * step];
+    }
+    int c[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) c[k] = comm[u[k]];
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+      if (c[k] == own) x += wt[k];
+  }
+  for (; j < e; j += step)
+    if (comm[adj[j]] == own) x += w[j];
+  return x;
+}
+
 // Stage 1: per-vertex in-community weight (self-loops included), one group of
 // G lanes per vertex; lane l sums edges l, l+G, ... then a fixed tree.
 template <int G>
@@ -137,10 +165,7 @@ __global__ void k_q_self_group(const int32_t* __restrict__ list, int64_t n,
     int v = 0;
     if (idx < n) {
       v = list[idx];
-      const int32_t own = comm[v];
-      const int64_t e = off[v + 1];
-      for (int64_t j = off[v] + gl; j < e; j += G)
-        if (comm[adj[j]] == own) x += w[j];
+      x = own_weight(adj, w, comm, comm[v], off[v] + gl, off[v + 1], G);
     }
 #pragma unroll
     for (int o = G / 2; o > 0; o >>= 1) x += __shfl_down_sync(NIDO_FULL_MASK, x, o, G);
@@ -158,11 +183,7 @@ __global__ void __launch_bounds__(T) k_q_self_cta(const int32_t* __restrict__ li
   __shared__ double ws[T / 32];
   for (int64_t idx = blockIdx.x; idx < n; idx += gridDim.x) {
     const int v = list[idx];
-    const int32_t own = comm[v];
-    const int64_t e = off[v + 1];
-    double x = 0.;
-    for (int64_t j = off[v] + threadIdx.x; j < e; j += T)
-      if (comm[adj[j]] == own) x += w[j];
+    double x = own_weight(adj, w, comm, comm[v], off[v] + threadIdx.x, off[v + 1], T);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(NIDO_FULL_MASK, x, o);
     if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = x;
