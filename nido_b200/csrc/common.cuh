@@ -29,6 +29,7 @@
 // Follows every kernel launch: counts it and reports a launch error (bad
 // configuration) without a sync.
 extern "C" void nido_count_launch(void);
+extern "C" void nido_count_launches(uint64_t n);  // kernels of a replayed CUDA graph
 #define NIDO_LAUNCH_CHECK()                     \
   do {                                          \
     nido_count_launch();                        \

@@ -190,6 +190,8 @@ extern "C" int nido_graph_free(nido_graph g) {
                   (void*)g->hub_nseg, (void*)g->hub_toff, (void*)g->hub_done, (void*)g->hub_slices,
                   (void*)g->hub_slice_first, (void*)g->hub_res, (void*)g->agg_buf})
     nido::raw_free(ctx, p);
+  for (nido_graph_s::MoveGraph& mg : g->move_graphs)
+    if (mg.exec) cudaGraphExecDestroy(mg.exec);
   delete g;
   return NIDO_OK;
 }

@@ -149,6 +149,19 @@ struct nido_graph_s {
   int64_t max_degree = 0;
   TierConfig cfg;
   bool tuned = false;
+  // the move sweep of every batch captured as a CUDA graph, replayed for the
+  // later sweeps of a phase (plan_epoch changes whenever the tier lists or
+  // the hub plan are rebuilt)
+  struct MoveGraph {
+    cudaGraphExec_t exec = nullptr;
+    int tie = -1;
+    int64_t epoch = -1;
+    int uses = 0;
+    uint64_t kernels = 0;
+  };
+  std::vector<MoveGraph> move_graphs;
+  int64_t plan_epoch = 0;
+  bool use_graphs = true;
   double host_pinned_dummy = 0;
 };
 

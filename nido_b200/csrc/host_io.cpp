@@ -21,6 +21,7 @@ static thread_local char g_err[512] = "";
 static unsigned long long g_launches = 0;
 
 extern "C" void nido_count_launch(void) { __atomic_fetch_add(&g_launches, 1ull, __ATOMIC_RELAXED); }
+extern "C" void nido_count_launches(uint64_t n) { __atomic_fetch_add(&g_launches, (unsigned long long)n, __ATOMIC_RELAXED); }
 extern "C" uint64_t nido_launch_count(void) { return __atomic_load_n(&g_launches, __ATOMIC_RELAXED); }
 
 extern "C" int nido_set_error(int code, const char* fmt, ...) {

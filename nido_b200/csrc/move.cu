@@ -982,7 +982,48 @@ int launch_move(nido_graph_s* g, int batch, int tie, cudaEvent_t ev_start, cudaE
   MoveArgs p{g->off, g->adj, g->w, g->comm, g->k, g->a, g->newc, g->m, tie,
              reinterpret_cast<unsigned long long*>(g->dcount + 1), g->gid, g->mg};
   if (ev_start) NIDO_CUDA_TRY(cudaEventRecord(ev_start, s));
-  NIDO_TRY(g->gid ? launch_tiers<true>(g, batch, tie, p) : launch_tiers<false>(g, batch, tie, p));
+  auto direct = [&]() { return g->gid ? launch_tiers<true>(g, batch, tie, p) : launch_tiers<false>(g, batch, tie, p); };
+  if (!g->use_graphs) {
+    NIDO_TRY(direct());
+  } else {
+    // The launches of a batch are fixed for a phase: the first sweep runs them
+    // directly, the second captures them into a CUDA graph, later sweeps
+    // replay it (the arguments are all device pointers that live for the
+    // phase).
+    if (g->move_graphs.size() < (size_t)g->nbatches) g->move_graphs.resize(g->nbatches);
+    nido_graph_s::MoveGraph& mg = g->move_graphs[batch];
+    if (mg.epoch != g->plan_epoch || mg.tie != tie) {
+      if (mg.exec) cudaGraphExecDestroy(mg.exec);
+      mg = nido_graph_s::MoveGraph();
+      mg.epoch = g->plan_epoch;
+      mg.tie = tie;
+    }
+    if (mg.exec) {
+      NIDO_CUDA_TRY(cudaGraphLaunch(mg.exec, s));
+      nido_count_launches(mg.kernels);
+    } else if (mg.uses++ == 0) {
+      NIDO_TRY(direct());
+    } else {
+      const uint64_t l0 = nido_launch_count();
+      cudaGraph_t graph = nullptr;
+      NIDO_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+      const int st = direct();
+      const cudaError_t ce = cudaStreamEndCapture(s, &graph);
+      if (st != NIDO_OK) {
+        if (graph) cudaGraphDestroy(graph);
+        return st;
+      }
+      if (ce != cudaSuccess) return nido_set_error(NIDO_E_CUDA, "move-sweep capture failed: %s", cudaGetErrorString(ce));
+      mg.kernels = nido_launch_count() - l0;
+      const cudaError_t ie = cudaGraphInstantiate(&mg.exec, graph, 0);
+      cudaGraphDestroy(graph);
+      if (ie != cudaSuccess) {
+        mg.exec = nullptr;
+        return nido_set_error(NIDO_E_CUDA, "move-sweep graph instantiation failed: %s", cudaGetErrorString(ie));
+      }
+      NIDO_CUDA_TRY(cudaGraphLaunch(mg.exec, s));
+    }
+  }
   if (ev_end) NIDO_CUDA_TRY(cudaEventRecord(ev_end, s));
   return NIDO_OK;
 }

@@ -449,6 +449,7 @@ int build_batches(nido_graph_s* g) {
   NIDO_CUDA_TRY(cudaStreamSynchronize(s));
   g->max_degree = (int64_t)md;
   g->bins_valid = true;
+  ++g->plan_epoch;
   return plan_hubs(g);
 }
 
