@@ -46,6 +46,7 @@ struct AggArgs {
   int64_t* __restrict__ degp;           // coarse degree
   int64_t nvp;                          // coarse vertex count
   unsigned long long* err;              // probe-limit failures (never expected)
+  const int32_t* __restrict__ pm32;     // member holding position 32*b, for every b
 };
 
 inline unsigned grid_for(int64_t work, int per_block, int max_blocks) {
@@ -136,6 +137,14 @@ __device__ __forceinline__ int64_t find_member(const int64_t* __restrict__ medge
   return lo;
 }
 
+// pm32[b] = the member whose positions include 32*b (positions run over the
+// members' edge lists in member order; medge has nv+1 entries)
+__global__ void k_member_blocks(const int64_t* __restrict__ medge, int64_t nv, int32_t* __restrict__ pm32) {
+  const int64_t nb = (medge[nv] + 31) >> 5;
+  for (int64_t b = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; b < nb; b += (int64_t)gridDim.x * blockDim.x)
+    pm32[b] = (int32_t)find_member(medge, 0, nv, 32 * b);
+}
+
 // Slot of key X, inserting it if absent (*isnew reports the insert); at most
 // mask+1 probes, -1 when the table is full (tables are sized to at least
 // twice the number of keys, so this never happens).
@@ -173,9 +182,20 @@ __device__ __forceinline__ unsigned cap_for(int64_t D, int64_t nvp) {
 }
 
 // neighbour of list position P: new id and weight
+// Member holding list position P: start from the member of P's 32-position
+// block and step forward (a binary search over [m0, m1) only after 32 steps,
+// i.e. across a run of members without edges).
+__device__ __forceinline__ int64_t member_of(const AggArgs& q, int64_t m1, int64_t P) {
+  int64_t i = q.pm32[P >> 5];
+  for (int k = 0; k < 32 && q.medge[i + 1] <= P; ++k) ++i;
+  if (q.medge[i + 1] <= P) i = find_member(q.medge, i, m1, P);
+  return i;
+}
+
 __device__ __forceinline__ void load_pos(const AggArgs& q, int64_t m0, int64_t m1, int64_t P, int& X,
                                          double& wt) {
-  const int64_t i = find_member(q.medge, m0, m1, P);
+  (void)m0;
+  const int64_t i = member_of(q, m1, P);
   const uint32_t v = q.member[i];
   const int64_t e = q.off[v] + (P - q.medge[i]);
   X = q.newid[q.adj[e]];
@@ -536,6 +556,19 @@ int launch_aggregation(nido_graph_s* g, int* done) {
   k_member_bounds<<<gv, 256, 0, s>>>(rk, rv, nv, nvp, g->off, mo, medge);
   NIDO_LAUNCH_CHECK();
   NIDO_TRY(scan_exclusive_i64(medge, medge, nv, temp, s));
+  {  // member of every 32-position block of the member-edge lists
+    const int64_t nblk = (g->ne + 31) / 32 + 1;
+    if (nblk > g->pm32_cap) {
+      NIDO_CUDA_TRY(cudaStreamSynchronize(s));
+      raw_free(g->ctx, g->pm32);
+      g->pm32 = nullptr;
+      g->pm32_cap = 0;
+      NIDO_CUDA_TRY(raw_alloc(g->ctx, (void**)&g->pm32, sizeof(int32_t) * (size_t)nblk));
+      g->pm32_cap = nblk;
+    }
+    k_member_blocks<<<grid_for(nblk, 256, kSMs * 16), 256, 0, s>>>(medge, nv, g->pm32);
+    NIDO_LAUNCH_CHECK();
+  }
   NIDO_CUDA_TRY(cudaMemsetAsync(counts, 0, sizeof(int64_t) * 4, s));
   // coarse-vertex tiers (rk2/rv2 are free after the member sort)
   uint32_t* tk = rk2;
@@ -550,7 +583,7 @@ int launch_aggregation(nido_graph_s* g, int* done) {
   NIDO_CUDA_TRY(cudaStreamSynchronize(s));
 
   AggArgs q{g->off, g->adj, g->w, newid, rv, mo, medge, g->adj2, g->w2, degp, nvp,
-            reinterpret_cast<unsigned long long*>(g->dcount + 1)};
+            reinterpret_cast<unsigned long long*>(g->dcount + 1), g->pm32};
   const int32_t* list = reinterpret_cast<const int32_t*>(tv);
   if (cnt[0] > 0) {
     const int capmax = 2 * kAggWarpMaxD;

@@ -130,6 +130,8 @@ struct nido_graph_s {
   // so runs after the first allocate nothing)
   char* agg_buf = nullptr;
   size_t agg_buf_bytes = 0;
+  int32_t* pm32 = nullptr;   // member of every 32-position block of the member-edge lists
+  int64_t pm32_cap = 0;
 
   // many-graph mode (null / empty for one graph): the graph of every current
   // vertex, the mass of every graph, and the batch of every vertex relative to

@@ -553,25 +553,53 @@ __global__ void __launch_bounds__(kThreads) k_move_cta(const int32_t* __restrict
   if (threadIdx.x == 0) nocc_s = 0;
   __syncthreads();
   const int wid = threadIdx.x >> 5;
-  for (int64_t task = blockIdx.x; task < n; task += gridDim.x) {
-    const int v = list[task];
-    const int64_t s = p.off[v], eend = p.off[v + 1];
+  // The next vertex's header (id, offsets, community, k, a_own) is loaded
+  // while the current one is evaluated, so its dependent round trips overlap.
+  int64_t task = blockIdx.x;
+  int v = 0, own = 0;
+  int64_t s = 0, eend = 0;
+  double ki = 0., aown = 0.;
+  if (task < n) {
+    v = list[task];
+    s = p.off[v];
+    eend = p.off[v + 1];
+    own = p.comm[v];
+    ki = p.k[v];
+    aown = p.a[own];
+  }
+  for (; task < n; task += gridDim.x) {
+    const int64_t nt = task + gridDim.x;
+    const int vn = nt < n ? list[nt] : 0;
     t.mask = min((unsigned)kCap, next_pow2_cap(eend - s)) - 1;
-    const int own = p.comm[v];
-    const double ki = p.k[v], aown = p.a[own];
     accumulate_edges<true, 4>(p, v, s + (int64_t)wid * 32, eend, kThreads, t);
     __syncthreads();
     const int nu = nocc_s;
+    int64_t sn = 0, en = 0;
+    int ownn = 0;
+    double kin = 0.;
+    if (nt < n) {
+      sn = p.off[vn];
+      en = p.off[vn + 1];
+      ownn = p.comm[vn];
+      kin = p.k[vn];
+    }
     // block_evaluate ends with a barrier that every thread reaches after
     // reading nu, so the count can be reset right after it
     block_evaluate(p, vertex_mass<kMulti>(p, v), t, nu, false, v, own, ki, aown, sg, stk, sc);
     if (threadIdx.x == 0) nocc_s = 0;
+    const double aownn = nt < n ? p.a[ownn] : 0.;
     for (int i = threadIdx.x; i < nu; i += kThreads) {
       const int slot = t.occ[i];
       t.keys[slot] = -1;
       t.vals[slot] = 0.;
     }
     __syncthreads();
+    v = vn;
+    s = sn;
+    eend = en;
+    own = ownn;
+    ki = kin;
+    aown = aownn;
   }
 }
 
