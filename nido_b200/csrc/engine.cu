@@ -142,6 +142,11 @@ extern "C" int nido_ctx_create(int device, size_t hbm_budget_bytes, nido_ctx* ou
   NIDO_CUDA_TRY(cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking));
   NIDO_CUDA_TRY(cudaEventCreate(&ctx->ev0));
   NIDO_CUDA_TRY(cudaEventCreate(&ctx->ev1));
+  for (int i = 0; i < 2; ++i) {
+    NIDO_CUDA_TRY(cudaStreamCreateWithFlags(&ctx->aux[i], cudaStreamNonBlocking));
+    NIDO_CUDA_TRY(cudaEventCreateWithFlags(&ctx->join_ev[i], cudaEventDisableTiming));
+  }
+  NIDO_CUDA_TRY(cudaEventCreateWithFlags(&ctx->fork_ev, cudaEventDisableTiming));
   *out = ctx;
   return NIDO_OK;
 }
@@ -153,6 +158,14 @@ extern "C" int nido_ctx_destroy(nido_ctx ctx) {
   cudaEventDestroy(ctx->ev0);
   cudaEventDestroy(ctx->ev1);
   for (cudaEvent_t e : ctx->move_ev) cudaEventDestroy(e);
+  for (int i = 0; i < 2; ++i) {
+    if (ctx->aux[i]) {
+      cudaStreamSynchronize(ctx->aux[i]);
+      cudaStreamDestroy(ctx->aux[i]);
+    }
+    if (ctx->join_ev[i]) cudaEventDestroy(ctx->join_ev[i]);
+  }
+  if (ctx->fork_ev) cudaEventDestroy(ctx->fork_ev);
   cudaStreamDestroy(ctx->stream);
   delete ctx;
   return NIDO_OK;

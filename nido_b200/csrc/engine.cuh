@@ -56,6 +56,12 @@ struct nido_ctx_s {
   size_t used = 0;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   std::vector<cudaEvent_t> move_ev;  // 2 per batch, for per-iteration move timing
+  // side streams of the move sweep: the degree tiers of one batch touch
+  // disjoint vertices, so the hub chain and the CTA tiers run beside the
+  // small-degree tiers (fork and join events on the context's stream)
+  cudaStream_t aux[2] = {nullptr, nullptr};
+  cudaEvent_t fork_ev = nullptr;
+  cudaEvent_t join_ev[2] = {nullptr, nullptr};
   // stream-ordered allocation (cudaMallocAsync / cudaFreeAsync on the
   // context's stream): allocating or freeing then does not wait for the work
   // of other contexts on the same GPU

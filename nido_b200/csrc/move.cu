@@ -929,12 +929,19 @@ int set_smem_mode() {
   return NIDO_OK;
 }
 
-// the tier kernels of one batch; kMulti: many graphs (per-vertex mass)
+// the tier kernels of one batch; kMulti: many graphs (per-vertex mass).  The
+// tiers cover disjoint vertices and only read comm and a, so they run on
+// three streams: the hub chain and the CTA tiers on the context's side
+// streams, the rest on its stream, joined before the function returns.
 template <bool kMulti>
 int launch_tiers(nido_graph_s* g, int batch, int tie, const MoveArgs& p) {
-  cudaStream_t s = g->ctx->stream;
+  nido_ctx_s* ctx = g->ctx;
+  const cudaStream_t main_s = ctx->stream;
+  NIDO_CUDA_TRY(cudaEventRecord(ctx->fork_ev, main_s));
+  for (int i = 0; i < 2; ++i) NIDO_CUDA_TRY(cudaStreamWaitEvent(ctx->aux[i], ctx->fork_ev, 0));
   const int nb = g->nbatches;
-  for (int t = 0; t < kNumTiers; ++t) {
+  for (int t = kNumTiers - 1; t >= 0; --t) {  // longest chains first
+    const cudaStream_t s = t == kTierHub ? ctx->aux[0] : (t >= kTierCtaS ? ctx->aux[1] : main_s);
     const int64_t b0 = g->tier_off[(size_t)t * nb + batch], b1 = g->tier_off[(size_t)t * nb + batch + 1];
     const int64_t n = b1 - b0;
     if (n <= 0) continue;
@@ -992,6 +999,10 @@ int launch_tiers(nido_graph_s* g, int batch, int tie, const MoveArgs& p) {
       }
     }
     NIDO_LAUNCH_CHECK();
+  }
+  for (int i = 0; i < 2; ++i) {
+    NIDO_CUDA_TRY(cudaEventRecord(ctx->join_ev[i], ctx->aux[i]));
+    NIDO_CUDA_TRY(cudaStreamWaitEvent(main_s, ctx->join_ev[i], 0));
   }
   return NIDO_OK;
 }
