@@ -493,7 +493,8 @@ namespace {
 bool config_ok(const TierConfig& c) {
   return c.warp_max >= 32 && c.warp_max <= kWarpMaxDeg && c.ctas_max >= c.warp_max && c.ctas_max <= kCtaSMaxDeg &&
          c.ctam_max >= c.ctas_max && c.ctam_max <= kCtaMMaxDeg && c.ctal_max >= c.ctam_max &&
-         c.ctal_max <= kCtaLMaxDeg && c.hub_wave_slots >= 4096;
+         c.ctal_max <= kCtaLMaxDeg && c.ctax_max >= c.ctal_max && c.ctax_max <= kCtaXMaxDeg &&
+         c.hub_wave_slots >= 4096;
 }
 
 // one move sweep over every batch, timed on the device (ms)
@@ -529,10 +530,11 @@ int tune_tiers(nido_graph_s* g, int tie, int sweeps, double* best_ms) {
     g->cfg = best;
     return NIDO_OK;
   };
+  for (int32_t v : {4096, 2048}) { TierConfig c = best; c.ctax_max = std::max(v, best.ctal_max); NIDO_TRY(try_cfg(c)); }
   for (int32_t v : {1024, 1536}) { TierConfig c = best; c.ctal_max = v; NIDO_TRY(try_cfg(c)); }
   for (int32_t v : {384, 256}) { TierConfig c = best; c.ctas_max = v; NIDO_TRY(try_cfg(c)); }
   for (int32_t v : {96, 64}) { TierConfig c = best; c.warp_max = v; NIDO_TRY(try_cfg(c)); }
-  if (g->max_degree > best.ctal_max)
+  if (g->max_degree > best.ctax_max)
     for (int64_t v : {(int64_t)2 << 20, (int64_t)8 << 20}) { TierConfig c = best; c.hub_wave_slots = v; NIDO_TRY(try_cfg(c)); }
   g->cfg = best;
   g->bins_valid = false;
@@ -545,7 +547,8 @@ int tune_tiers(nido_graph_s* g, int tie, int sweeps, double* best_ms) {
 
 extern "C" int nido_get_tier_config(nido_graph g, nido_tier_config* c) {
   if (!g || !c) return nido_set_error(NIDO_E_INVALID, "null argument");
-  *c = nido_tier_config{g->cfg.warp_max, g->cfg.ctas_max, g->cfg.ctam_max, g->cfg.ctal_max, g->cfg.hub_wave_slots};
+  *c = nido_tier_config{g->cfg.warp_max, g->cfg.ctas_max, g->cfg.ctam_max, g->cfg.ctal_max, g->cfg.ctax_max, 0,
+                        g->cfg.hub_wave_slots};
   return NIDO_OK;
 }
 
@@ -556,6 +559,7 @@ extern "C" int nido_set_tier_config(nido_graph g, const nido_tier_config* c) {
   t.ctas_max = c->cta_s_max_degree;
   t.ctam_max = c->cta_m_max_degree;
   t.ctal_max = c->cta_l_max_degree;
+  t.ctax_max = c->cta_x_max_degree;
   t.hub_wave_slots = c->hub_wave_slots;
   if (!nido::config_ok(t)) return nido_set_error(NIDO_E_INVALID, "tier thresholds out of range or decreasing");
   g->cfg = t;

@@ -28,6 +28,7 @@ enum Tier {
   kTierCtaS,    // d <= 512  : one 128-thread CTA, shared-memory hash (1024 slots)
   kTierCtaM,    // d <= 1024 : one 256-thread CTA, shared-memory hash (2048 slots)
   kTierCtaL,    // d <= 2048 : one 256-thread CTA, shared-memory hash (4096 slots)
+  kTierCtaX,    // d <= 8192 : one 1024-thread CTA, shared-memory hash (16384 slots, 192 KB)
   kTierHub,     // larger    : 2048-edge segments on many CTAs, hash in global memory (L2)
   kNumTiers
 };
@@ -37,6 +38,7 @@ constexpr int kWarpMaxDeg = 128;
 constexpr int kCtaSMaxDeg = 512;
 constexpr int kCtaMMaxDeg = 1024;
 constexpr int kCtaLMaxDeg = 2048;
+constexpr int kCtaXMaxDeg = 8192;
 
 // Degree thresholds of the shared-memory tiers and the hub wave size.  The
 // defaults are the kernels' capacities; the tuner (engine.cu) may lower the
@@ -46,6 +48,7 @@ struct TierConfig {
   int32_t ctas_max = kCtaSMaxDeg;
   int32_t ctam_max = kCtaMMaxDeg;
   int32_t ctal_max = kCtaLMaxDeg;
+  int32_t ctax_max = kCtaXMaxDeg;
   int64_t hub_wave_slots = (int64_t)4 << 20;
 };
 

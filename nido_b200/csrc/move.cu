@@ -537,7 +537,10 @@ __device__ __forceinline__ void block_evaluate(const MoveArgs& p, double m, cons
 }
 
 // ---- 256 < degree <= 2048: one CTA per vertex, table in shared memory ----------
-template <int kThreads, int kCap, bool kMulti>
+// kOcc: keep a list of occupied slots (16 bytes a slot) so evaluation and
+// clearing touch only used slots; without it (12 bytes a slot, for the
+// largest table) both walk the vertex's whole table.
+template <int kThreads, int kCap, bool kMulti, bool kOcc = true>
 __global__ void __launch_bounds__(kThreads) k_move_cta(const int32_t* __restrict__ list, int64_t n, MoveArgs p) {
   extern __shared__ double smem[];
   __shared__ double sg[32];
@@ -547,7 +550,7 @@ __global__ void __launch_bounds__(kThreads) k_move_cta(const int32_t* __restrict
   Table t;
   t.vals = smem;
   t.keys = reinterpret_cast<int*>(smem + kCap);
-  t.occ = t.keys + kCap;
+  t.occ = kOcc ? t.keys + kCap : nullptr;
   t.nocc = &nocc_s;
   for (int i = threadIdx.x; i < kCap; i += kThreads) { t.keys[i] = -1; t.vals[i] = 0.; }
   if (threadIdx.x == 0) nocc_s = 0;
@@ -573,7 +576,7 @@ __global__ void __launch_bounds__(kThreads) k_move_cta(const int32_t* __restrict
     t.mask = min((unsigned)kCap, next_pow2_cap(eend - s)) - 1;
     accumulate_edges<true, 4>(p, v, s + (int64_t)wid * 32, eend, kThreads, t);
     __syncthreads();
-    const int nu = nocc_s;
+    const int nu = kOcc ? nocc_s : (int)(t.mask + 1);
     int64_t sn = 0, en = 0;
     int ownn = 0;
     double kin = 0.;
@@ -589,7 +592,7 @@ __global__ void __launch_bounds__(kThreads) k_move_cta(const int32_t* __restrict
     if (threadIdx.x == 0) nocc_s = 0;
     const double aownn = nt < n ? p.a[ownn] : 0.;
     for (int i = threadIdx.x; i < nu; i += kThreads) {
-      const int slot = t.occ[i];
+      const int slot = kOcc ? t.occ[i] : i;
       t.keys[slot] = -1;
       t.vals[slot] = 0.;
     }
@@ -911,6 +914,7 @@ constexpr int kWarpCap = 256;     // warp tier: degree <= 128
 constexpr int kCtaSCap = 1024;    // 128-thread CTA tier: degree <= 512
 constexpr int kCtaMCap = 2048;    // 256-thread CTA tier: degree <= 1024
 constexpr int kCtaLCap = 4096;    // 256-thread CTA tier: degree <= 2048
+constexpr int kCtaXCap = 16384;   // 1024-thread CTA tier: degree <= 8192 (no occupied list)
 
 template <typename K>
 int set_smem(K kernel, size_t bytes) {
@@ -926,6 +930,7 @@ int set_smem_mode() {
   NIDO_TRY(set_smem(k_move_cta<128, kCtaSCap, kMulti>, (size_t)kCtaSCap * 16));
   NIDO_TRY(set_smem(k_move_cta<256, kCtaMCap, kMulti>, (size_t)kCtaMCap * 16));
   NIDO_TRY(set_smem(k_move_cta<256, kCtaLCap, kMulti>, (size_t)kCtaLCap * 16));
+  NIDO_TRY(set_smem(k_move_cta<1024, kCtaXCap, kMulti, false>, (size_t)kCtaXCap * 12));
   return NIDO_OK;
 }
 
@@ -971,6 +976,9 @@ int launch_tiers(nido_graph_s* g, int batch, int tie, const MoveArgs& p) {
         break;
       case kTierCtaL:
         k_move_cta<256, kCtaLCap, kMulti><<<grid_cap(n, kSMs * 3), 256, (size_t)kCtaLCap * 16, s>>>(list, n, p);
+        break;
+      case kTierCtaX:
+        k_move_cta<1024, kCtaXCap, kMulti, false><<<grid_cap(n, kSMs), 1024, (size_t)kCtaXCap * 12, s>>>(list, n, p);
         break;
       default: {
         SliceResult* res = reinterpret_cast<SliceResult*>(g->hub_res);

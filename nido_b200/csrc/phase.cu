@@ -235,16 +235,21 @@ __global__ void k_batch_cuts(const int64_t* __restrict__ off, int64_t nv, int nb
   batch_cuts(off, nv, nb, cuts, parts);
 }
 
-// thr = (warp, CTA-S, CTA-M, CTA-L) maximum degrees
-__device__ __forceinline__ int tier_of(int64_t d, int4 thr) {
+// maximum degrees of the warp, CTA-S, CTA-M, CTA-L and CTA-XL tiers
+struct TierThresholds {
+  int warp, ctas, ctam, ctal, ctax;
+};
+
+__device__ __forceinline__ int tier_of(int64_t d, const TierThresholds& thr) {
   if (d <= 4) return kTierG4;
   if (d <= 8) return kTierG8;
   if (d <= 16) return kTierG16;
   if (d <= 32) return kTierG32;
-  if (d <= thr.x) return kTierWarp;
-  if (d <= thr.y) return kTierCtaS;
-  if (d <= thr.z) return kTierCtaM;
-  if (d <= thr.w) return kTierCtaL;
+  if (d <= thr.warp) return kTierWarp;
+  if (d <= thr.ctas) return kTierCtaS;
+  if (d <= thr.ctam) return kTierCtaM;
+  if (d <= thr.ctal) return kTierCtaL;
+  if (d <= thr.ctax) return kTierCtaX;
   return kTierHub;
 }
 
@@ -260,7 +265,7 @@ __global__ void k_tier_keys(const int64_t* __restrict__ off, int64_t nv, const i
                             int64_t* __restrict__ counts, unsigned long long* __restrict__ maxdeg,
                             const int32_t* __restrict__ gid, const int64_t* __restrict__ gbase,
                             const int64_t* __restrict__ gcuts, const int32_t* __restrict__ gactive,
-                            int32_t* __restrict__ vbatch, int4 thr) {
+                            int32_t* __restrict__ vbatch, TierThresholds thr) {
   const int lane = threadIdx.x & 31;
   const uint32_t skip = (uint32_t)(kNumTiers * nb);
   unsigned long long md = 0;
@@ -431,8 +436,9 @@ int build_batches(nido_graph_s* g) {
     k_tier_keys<<<grid_for(nv, kThreads), kThreads, 0, s>>>(g->off, nv, dcuts, nb, keys, (uint32_t*)g->perm,
                                                            counts, maxdeg, g->gid, g->gbase, g->gcuts,
                                                            g->gactive, g->vbatch,
-                                                           make_int4(g->cfg.warp_max, g->cfg.ctas_max,
-                                                                     g->cfg.ctam_max, g->cfg.ctal_max));
+                                                           TierThresholds{g->cfg.warp_max, g->cfg.ctas_max,
+                                                                          g->cfg.ctam_max, g->cfg.ctal_max,
+                                                                          g->cfg.ctax_max});
     NIDO_LAUNCH_CHECK();
     int bits = 0;
     while (((int64_t)1 << bits) < nkeys + 1) ++bits;
