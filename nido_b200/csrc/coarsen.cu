@@ -272,8 +272,7 @@ __global__ void __launch_bounds__(kAggThreads) k_agg_cta(const int32_t* __restri
                                                          int capmax, int32_t* gkeys, double* gvals,
                                                          int32_t* gfpos, int64_t gslab) {
   extern __shared__ double smem[];
-  __shared__ int wsum[kAggThreads / 32];
-  __shared__ int running_s;
+  __shared__ int wsum[2][kAggThreads / 32];
   int *keys, *fpos;
   double* vals;
   if (kGlobal) {
@@ -324,9 +323,11 @@ __global__ void __launch_bounds__(kAggThreads) k_agg_cta(const int32_t* __restri
         }
       }
     }
-    if (threadIdx.x == 0) running_s = 0;
+    // emit in list order: per 256 positions one barrier, the warps' counts
+    // double-buffered, every thread carrying the running total
     __syncthreads();
-    for (int64_t base = P0; base < P1; base += blockDim.x) {
+    int running = 0, par = 0;
+    for (int64_t base = P0; base < P1; base += blockDim.x, par ^= 1) {
       const int64_t P = base + threadIdx.x;
       const bool ok = P < P1;
       int X = -1;
@@ -339,24 +340,23 @@ __global__ void __launch_bounds__(kAggThreads) k_agg_cta(const int32_t* __restri
         first = h >= 0 && fpos[h] == (int)(P - P0);
       }
       const unsigned bal = __ballot_sync(NIDO_FULL_MASK, first);
-      if (lane == 0) wsum[wid] = __popc(bal);
+      if (lane == 0) wsum[par][wid] = __popc(bal);
       __syncthreads();
-      int pre = running_s;
-      for (int i = 0; i < wid; ++i) pre += wsum[i];
+      int pre = running, tot = 0;
+      for (int i = 0; i < nwarp; ++i) {
+        const int c = wsum[par][i];
+        if (i < wid) pre += c;
+        tot += c;
+      }
+      running += tot;
       if (first) {
         const int idx = pre + __popc(bal & lanemask_lt());
         q.tadj[P0 + idx] = X;
         q.tw[P0 + idx] = vals[h];
       }
-      __syncthreads();
-      if (threadIdx.x == 0) {
-        int t = 0;
-        for (int i = 0; i < nwarp; ++i) t += wsum[i];
-        running_s += t;
-      }
-      __syncthreads();
     }
-    if (threadIdx.x == 0) q.degp[cp] = running_s;
+    if (threadIdx.x == 0) q.degp[cp] = running;
+    __syncthreads();  // every warp is done reading the table before it is cleared
     for (unsigned i = threadIdx.x; i < cap; i += blockDim.x) { keys[i] = -1; vals[i] = 0.; fpos[i] = INT_MAX; }
     __syncthreads();
   }
@@ -440,8 +440,7 @@ __global__ void __launch_bounds__(256) k_agg_seg_insert(int64_t it0, int64_t n, 
 template <bool kEmit>
 __global__ void __launch_bounds__(256) k_agg_seg_scan(int64_t it0, int64_t n, AggArgs q, SegArgs a,
                                                       int64_t* segcnt) {
-  __shared__ int wsum[8];
-  __shared__ int64_t running_s;
+  __shared__ int wsum[2][8];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   for (int64_t it = it0 + blockIdx.x; it < it0 + n; it += gridDim.x) {
     const int2 item = a.items[it];
@@ -453,9 +452,11 @@ __global__ void __launch_bounds__(256) k_agg_seg_scan(int64_t it0, int64_t n, Ag
     const int* fpos = a.fpos + a.toff[item.x];
     const unsigned mask = (unsigned)a.caps[item.x] - 1;
     const int64_t base_out = kEmit ? segcnt[it] - segcnt[a.first[item.x]] : 0;
-    if (threadIdx.x == 0) running_s = 0;
+    // one barrier per 256 positions (counts double-buffered, as in k_agg_cta)
     __syncthreads();
-    for (int64_t base = s0; base < s1; base += blockDim.x) {
+    int64_t running = 0;
+    int par = 0;
+    for (int64_t base = s0; base < s1; base += blockDim.x, par ^= 1) {
       const int64_t P = base + threadIdx.x;
       int X = -1;
       double wt = 0.;
@@ -467,23 +468,23 @@ __global__ void __launch_bounds__(256) k_agg_seg_scan(int64_t it0, int64_t n, Ag
         firstocc = h >= 0 && fpos[h] == (int)(P - P0);
       }
       const unsigned bal = __ballot_sync(NIDO_FULL_MASK, firstocc);
-      if (lane == 0) wsum[wid] = __popc(bal);
+      if (lane == 0) wsum[par][wid] = __popc(bal);
       __syncthreads();
+      int64_t pre = running;
+      int tot = 0;
+      for (int i = 0; i < (int)(blockDim.x >> 5); ++i) {
+        const int c = wsum[par][i];
+        if (i < wid) pre += c;
+        tot += c;
+      }
+      running += tot;
       if (kEmit && firstocc) {
-        int64_t idx = base_out + running_s + __popc(bal & lanemask_lt());
-        for (int i = 0; i < wid; ++i) idx += wsum[i];
+        const int64_t idx = base_out + pre + __popc(bal & lanemask_lt());
         q.tadj[P0 + idx] = X;
         q.tw[P0 + idx] = vals[h];
       }
-      __syncthreads();
-      if (threadIdx.x == 0) {
-        int t = 0;
-        for (int i = 0; i < (int)(blockDim.x >> 5); ++i) t += wsum[i];
-        running_s += t;
-      }
-      __syncthreads();
     }
-    if (!kEmit && threadIdx.x == 0) segcnt[it] = running_s;
+    if (!kEmit && threadIdx.x == 0) segcnt[it] = running;
     __syncthreads();
   }
 }
