@@ -13,8 +13,9 @@
 //   - the loop control: per-graph dQ, loop counters and convergence flags
 //     live on the device; graphs that stop iterating are no longer committed
 //     and drop out of the degree-tier lists once enough of them stopped;
-//     graphs that finish keep their vertices as singletons, so coarsening
-//     the union leaves their clustering unchanged.
+//     a graph that finishes has its clustering written out at once and its
+//     vertices dropped from the union at the next coarsening, so later
+//     phases carry only the graphs still running.
 // Given integer weights (exact FP64 sums) every graph's clustering equals the
 // one nido_run produces for that graph alone.
 #include <string.h>
@@ -67,6 +68,8 @@ struct nido_batch_s {
   int64_t* counters = nullptr; // [0] iterating graphs [1] restoring [2] iterating vertices [3] aggregating
   int32_t* gid = nullptr;
   int32_t* vbatch = nullptr;
+  int64_t* outc = nullptr;     // final clustering of every original vertex (ids within its graph)
+  int32_t* elist = nullptr;    // graphs whose clustering is written out now
   int64_t cap_part = 0, cap_modv = 0;
   size_t bytes = 0;            // budgeted bytes of the arrays above
 };
@@ -279,14 +282,26 @@ __global__ void k_control(const int32_t* __restrict__ gl, int n, const double* _
   }
 }
 
-// k_commit of the one-graph driver for the vertices of batch b (all
-// vertices for b < 0) of the graphs whose flag is set.
-__global__ void k_commit_multi(int64_t nv, int b, const int32_t* __restrict__ vbatch,
-                               const int32_t* __restrict__ gid, const int32_t* __restrict__ flag,
-                               const double* __restrict__ k, int32_t* __restrict__ comm,
-                               int32_t* __restrict__ newc, double* __restrict__ a) {
-  for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < nv; v += (int64_t)gridDim.x * blockDim.x) {
-    if ((b >= 0 && vbatch[v] != b) || !flag[gid[v]]) continue;
+// The listed vertices of one batch: the perm ranges of its (tier, batch)
+// keys, which are not contiguous (the keys are tier-major).
+struct PermRanges {
+  int64_t start[kNumTiers];
+  int64_t pre[kNumTiers + 1];  // prefix of the range lengths
+};
+
+// k_commit of the one-graph driver for the listed vertices of a batch (or,
+// for restore, for every listed vertex: one range) of the graphs whose flag
+// is set.
+__global__ void k_commit_listed(PermRanges r, int nr, const int32_t* __restrict__ perm,
+                                const int32_t* __restrict__ gid, const int32_t* __restrict__ flag,
+                                const double* __restrict__ k, int32_t* __restrict__ comm,
+                                int32_t* __restrict__ newc, double* __restrict__ a) {
+  const int64_t total = r.pre[nr];
+  for (int64_t x = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; x < total; x += (int64_t)gridDim.x * blockDim.x) {
+    int t = 0;
+    while (r.pre[t + 1] <= x) ++t;
+    const int v = perm[r.start[t] + (x - r.pre[t])];
+    if (!flag[gid[v]]) continue;
     const int32_t src = comm[v], dst = newc[v];
     if (src != dst) {
       const double kv = k[v];
@@ -316,12 +331,23 @@ __global__ void k_phase_end(const int32_t* __restrict__ gl, int n, const double*
   }
 }
 
-// graphs that do not aggregate keep every vertex as its own community, so
-// the union's coarsening only renumbers them
-__global__ void k_identity(int64_t nv, const int32_t* __restrict__ gid, const int32_t* __restrict__ gagg,
-                           int32_t* __restrict__ comm) {
+// graphs that do not aggregate are finished (their clustering is written
+// out already): community -1 drops their vertices from the coarse union
+__global__ void k_drop(int64_t nv, const int32_t* __restrict__ gid, const int32_t* __restrict__ gagg,
+                       int32_t* __restrict__ comm) {
   for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < nv; v += (int64_t)gridDim.x * blockDim.x)
-    if (!gagg[gid[v]]) comm[v] = (int32_t)v;
+    if (!gagg[gid[v]]) comm[v] = -1;
+}
+
+// final clustering of the listed graphs: clus of their original vertices,
+// renumbered within each graph (one block per graph)
+__global__ void k_emit(const int32_t* __restrict__ gl, int n, const int64_t* __restrict__ gbase0,
+                       const int64_t* __restrict__ gbase, const int32_t* __restrict__ clus, int64_t* __restrict__ outc) {
+  for (int i = blockIdx.x; i < n; i += gridDim.x) {
+    const int g = gl[i];
+    const int64_t b = gbase[g];
+    for (int64_t v = gbase0[g] + threadIdx.x; v < gbase0[g + 1]; v += blockDim.x) outc[v] = (int64_t)clus[v] - b;
+  }
 }
 
 // a graph whose coarsening kept its vertex count or left one vertex is
@@ -335,13 +361,6 @@ __global__ void k_post_agg(const int32_t* __restrict__ gl, int n, const int64_t*
     const int64_t nvo = gold[g + 1] - gold[g], nvp = gnew[g + 1] - gnew[g];
     if (nvp == nvo || nvp == 1) gfin[g] = 1;
   }
-}
-
-__global__ void k_final_clus(int64_t nv0, const int64_t* __restrict__ gbase0, int ng,
-                             const int64_t* __restrict__ gbase, const int32_t* __restrict__ clus,
-                             int64_t* __restrict__ out) {
-  for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < nv0; v += (int64_t)gridDim.x * blockDim.x)
-    out[v] = (int64_t)clus[v] - gbase[find_item(gbase0, ng, v)];
 }
 
 __global__ void k_iota32(int32_t* __restrict__ x, int64_t n) {
@@ -472,7 +491,8 @@ extern "C" int nido_batch_free(nido_batch B) {
                     (void*)B->gfin, (void*)B->loops_phase, (void*)B->loops_total, (void*)B->phases, (void*)B->Q,
                     (void*)B->Qold, (void*)B->qnew, (void*)B->mg, (void*)B->plist, (void*)B->llist,
                     (void*)B->moff, (void*)B->qoff, (void*)B->part, (void*)B->modv, (void*)B->selfv,
-                    (void*)B->counters, (void*)B->gid, (void*)B->vbatch})
+                    (void*)B->counters, (void*)B->gid, (void*)B->vbatch, (void*)B->outc,
+                    (void*)B->elist})
       raw_free(ctx, p);
     ctx->used -= std::min(ctx->used, B->bytes);
     nido_graph_free(B->g);
@@ -519,6 +539,7 @@ extern "C" int nido_batch_upload(nido_ctx ctx, int32_t ngraphs, const int64_t* v
   take(&B->plist, G); take(&B->llist, G); take(&B->moff, G + 1); take(&B->qoff, G + 1);
   take(&B->part, B->cap_part); take(&B->modv, B->cap_modv); take(&B->selfv, V);
   take(&B->counters, 4); take(&B->gid, V); take(&B->vbatch, V);
+  take(&B->outc, V); take(&B->elist, G);
   if (st != NIDO_OK) {
     // device_alloc counted only what it allocated; nido_batch_free subtracts B->bytes
     nido_batch_free(B);
@@ -583,6 +604,18 @@ extern "C" int nido_batch_run(nido_batch B, const nido_params* p, int64_t* out_c
   const double tau = p->tau;
   std::vector<int64_t> base(B->vbase), edges(ng);
   std::vector<int32_t> fin(ng, 0), flags(ng);
+  // graphs whose final clustering is written to outc (empty graphs have none)
+  std::vector<char> emitted(ng, 0);
+  for (int32_t i = 0; i < ng; ++i) emitted[i] = B->vbase[i + 1] == B->vbase[i];
+  auto emit = [&](const std::vector<int32_t>& em) -> int {
+    if (em.empty()) return NIDO_OK;
+    NIDO_CUDA_TRY(cudaMemcpyAsync(B->elist, em.data(), sizeof(int32_t) * em.size(), cudaMemcpyHostToDevice, s));
+    k_emit<<<grid_for((int64_t)em.size(), 1, kSMs * 8), 256, 0, s>>>(B->elist, (int)em.size(), B->gbase0, g->gbase,
+                                                                 g->clus, B->outc);
+    NIDO_LAUNCH_CHECK();
+    NIDO_CUDA_TRY(cudaStreamSynchronize(s));  // em is a local vector
+    return NIDO_OK;
+  };
   unsigned long long cnt[4];
   int64_t phase = 0;
   bool first = true;
@@ -638,9 +671,19 @@ extern "C" int nido_batch_run(nido_batch B, const nido_params* p, int64_t* out_c
       NIDO_CUDA_TRY(cudaEventRecord(ev[0], s));
       for (int b = 0; b < nb; ++b) {
         NIDO_TRY(launch_move(g, b, p->tie_mode, nullptr, nullptr));
-        k_commit_multi<<<grid_for(g->nv, kThreads), kThreads, 0, s>>>(g->nv, b, B->vbatch, B->gid, B->giter, g->k,
-                                                                      g->comm, g->newc, g->a);
-        NIDO_LAUNCH_CHECK();
+        PermRanges r{};
+        int64_t tot = 0;
+        for (int t = 0; t < kNumTiers; ++t) {
+          r.start[t] = g->tier_off[(size_t)t * nb + b];
+          r.pre[t] = tot;
+          tot += g->tier_off[(size_t)t * nb + b + 1] - r.start[t];
+        }
+        r.pre[kNumTiers] = tot;
+        if (tot > 0) {
+          k_commit_listed<<<grid_for(tot, kThreads), kThreads, 0, s>>>(r, kNumTiers, g->perm, B->gid, B->giter, g->k,
+                                                                        g->comm, g->newc, g->a);
+          NIDO_LAUNCH_CHECK();
+        }
       }
       NIDO_CUDA_TRY(cudaEventRecord(ev[1], s));
       st.move_launches += nb;
@@ -659,8 +702,12 @@ extern "C" int nido_batch_run(nido_batch B, const nido_params* p, int64_t* out_c
       NIDO_CUDA_TRY(cudaEventElapsedTime(&ms, ev[0], ev[1]));
       st.move_ms += ms;
       if (cnt[1]) {
-        k_commit_multi<<<grid_for(g->nv, kThreads), kThreads, 0, s>>>(g->nv, -1, B->vbatch, B->gid, B->grest, g->k,
-                                                                      g->comm, g->newc, g->a);
+        PermRanges r{};
+        r.start[0] = 0;
+        r.pre[0] = 0;
+        r.pre[1] = g->tier_off[(size_t)kNumTiers * nb];  // every listed vertex
+        k_commit_listed<<<grid_for(r.pre[1], kThreads), kThreads, 0, s>>>(r, 1, g->perm, B->gid, B->grest, g->k,
+                                                                           g->comm, g->newc, g->a);
         NIDO_LAUNCH_CHECK();
         NIDO_CUDA_TRY(cudaMemsetAsync(B->grest, 0, sizeof(int32_t) * ng, s));
       }
@@ -689,15 +736,40 @@ extern "C" int nido_batch_run(nido_batch B, const nido_params* p, int64_t* out_c
       st.nv_phase[phase - 1] = listed_v;
       st.ne_phase[phase - 1] = g->ne;
     }
+    // graphs that do not aggregate are finished: their clustering is final
+    NIDO_CUDA_TRY(cudaMemcpyAsync(flags.data(), B->gagg, sizeof(int32_t) * ng, cudaMemcpyDeviceToHost, s));
+    NIDO_CUDA_TRY(cudaStreamSynchronize(s));
+    {
+      std::vector<int32_t> em;
+      for (int32_t i = 0; i < ng; ++i)
+        if (!emitted[i] && !flags[i]) { em.push_back(i); emitted[i] = 1; }
+      NIDO_TRY(emit(em));
+    }
     if (cnt[3] == 0) break;
-    k_identity<<<grid_for(g->nv, kThreads), kThreads, 0, s>>>(g->nv, B->gid, B->gagg, g->comm);
+    k_drop<<<grid_for(g->nv, kThreads), kThreads, 0, s>>>(g->nv, B->gid, B->gagg, g->comm);
     NIDO_LAUNCH_CHECK();
     int done = 0;
     NIDO_TRY(launch_aggregation(g, &done));
     std::swap(g->gbase, g->gbase2);  // the clustering is in the new numbering either way
     k_post_agg<<<grid_for(np, 128), 128, 0, s>>>(B->plist, np, g->gbase2, g->gbase, B->gagg, B->gfin);
     NIDO_LAUNCH_CHECK();
+    // graphs whose coarsening kept their size or left one vertex are
+    // finished too (their vertices leave the union at the next coarsening)
+    NIDO_CUDA_TRY(cudaMemcpyAsync(flags.data(), B->gfin, sizeof(int32_t) * ng, cudaMemcpyDeviceToHost, s));
+    NIDO_CUDA_TRY(cudaStreamSynchronize(s));
+    {
+      std::vector<int32_t> em;
+      for (int32_t i = 0; i < ng; ++i)
+        if (!emitted[i] && flags[i]) { em.push_back(i); emitted[i] = 1; }
+      NIDO_TRY(emit(em));
+    }
     if (done) break;  // every graph kept its size or collapsed: all finished
+  }
+  {  // graphs still running when the phase cap ended the loop
+    std::vector<int32_t> em;
+    for (int32_t i = 0; i < ng; ++i)
+      if (!emitted[i]) { em.push_back(i); emitted[i] = 1; }
+    NIDO_TRY(emit(em));
   }
   NIDO_CUDA_TRY(cudaEventRecord(t1, s));
   NIDO_CUDA_TRY(cudaEventSynchronize(t1));
@@ -711,14 +783,7 @@ extern "C" int nido_batch_run(nido_batch B, const nido_params* p, int64_t* out_c
   if (nerr) return nido_set_error(NIDO_E_CUDA, "hash table overflow in %lld probes", (long long)nerr);
   st.total_ms = tot;
   st.phases = phase;
-  if (out_comm) {
-    Arena ar(g->scratch, g->scratch_bytes);
-    int64_t* tmp = ar.take<int64_t>(g->nv0);
-    if (!tmp) return nido_set_error(NIDO_E_NOMEM, "scratch arena too small");
-    k_final_clus<<<grid_for(g->nv0, kThreads), kThreads, 0, s>>>(g->nv0, B->gbase0, ng, g->gbase, g->clus, tmp);
-    NIDO_LAUNCH_CHECK();
-    NIDO_CUDA_TRY(cudaMemcpyAsync(out_comm, tmp, sizeof(int64_t) * g->nv0, cudaMemcpyDeviceToHost, s));
-  }
+  if (out_comm) NIDO_CUDA_TRY(cudaMemcpyAsync(out_comm, B->outc, sizeof(int64_t) * g->nv0, cudaMemcpyDeviceToHost, s));
   if (out_q) NIDO_CUDA_TRY(cudaMemcpyAsync(out_q, B->Q, sizeof(double) * ng, cudaMemcpyDeviceToHost, s));
   if (out_phases) NIDO_CUDA_TRY(cudaMemcpyAsync(out_phases, B->phases, sizeof(int64_t) * ng, cudaMemcpyDeviceToHost, s));
   if (out_loops) NIDO_CUDA_TRY(cudaMemcpyAsync(out_loops, B->loops_total, sizeof(int64_t) * ng, cudaMemcpyDeviceToHost, s));

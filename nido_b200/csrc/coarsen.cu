@@ -56,17 +56,23 @@ inline unsigned grid_for(int64_t work, int per_block, int max_blocks) {
   return (unsigned)b;
 }
 
+// A negative community drops the vertex from the coarse graph (the
+// many-graph driver drops finished graphs this way; one-graph runs never do).
 __global__ void k_mark_used(const int32_t* __restrict__ comm, int64_t nv, int32_t* __restrict__ used) {
-  for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < nv; v += (int64_t)gridDim.x * blockDim.x)
-    used[comm[v]] = 1;
+  for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < nv; v += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t c = comm[v];
+    if (c >= 0) used[c] = 1;
+  }
 }
 
 __global__ void k_newid(const int32_t* __restrict__ comm, const int64_t* __restrict__ cid, int64_t nv,
                         int32_t* __restrict__ newid, uint32_t* __restrict__ keys, uint32_t* __restrict__ vals) {
+  const uint32_t dropped = (uint32_t)cid[nv];  // nvp: dropped vertices sort after every member
   for (int64_t v = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < nv; v += (int64_t)gridDim.x * blockDim.x) {
-    const int32_t x = (int32_t)cid[comm[v]];
+    const int32_t c = comm[v];
+    const int32_t x = c >= 0 ? (int32_t)cid[c] : -1;
     newid[v] = x;
-    keys[v] = (uint32_t)x;
+    keys[v] = c >= 0 ? (uint32_t)x : dropped;
     vals[v] = (uint32_t)v;
   }
 }
@@ -80,20 +86,24 @@ __global__ void k_graph_bases(const int64_t* __restrict__ gbase, int ng, const i
 }
 
 __global__ void k_compose(int32_t* __restrict__ clus, int64_t n0, const int32_t* __restrict__ newid) {
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n0; i += (int64_t)gridDim.x * blockDim.x)
-    clus[i] = newid[clus[i]];
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n0; i += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t c = clus[i];
+    if (c >= 0) clus[i] = newid[c];
+  }
 }
 
-// member offsets from the sorted keys (every id in [0, nvp) occurs) and the
-// member degrees
+// member offsets from the sorted keys (every id in [0, nvp) occurs; dropped
+// vertices carry key nvp and come last, with no member edges) and the member
+// degrees
 __global__ void k_member_bounds(const uint32_t* __restrict__ keys, const uint32_t* __restrict__ member,
                                 int64_t nv, int64_t nvp, const int64_t* __restrict__ off,
                                 int64_t* __restrict__ mo, int64_t* __restrict__ mdeg) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nv; i += (int64_t)gridDim.x * blockDim.x) {
-    if (i == 0 || keys[i] != keys[i - 1]) mo[keys[i]] = i;
-    if (i == 0) mo[nvp] = nv;
+    const uint32_t key = keys[i];
+    if (i == 0 || key != keys[i - 1]) mo[key] = i;
+    if (i == nv - 1 && key < (uint32_t)nvp) mo[nvp] = nv;
     const uint32_t v = member[i];
-    mdeg[i] = off[v + 1] - off[v];
+    mdeg[i] = key < (uint32_t)nvp ? off[v + 1] - off[v] : 0;
   }
 }
 
@@ -552,7 +562,7 @@ int launch_aggregation(nido_graph_s* g, int* done) {
   if (nvp == nv || nvp == 1) return NIDO_OK;  // graph_gpu.cpp:1391-1392
   *done = 0;
   int bits = 0;
-  while (((int64_t)1 << bits) < nvp) ++bits;
+  while (((int64_t)1 << bits) < nvp + 1) ++bits;  // keys run to nvp (dropped vertices)
   NIDO_TRY(radix_sort_pairs(rk, rv, rk2, rv2, nv, bits, temp, s));
   k_member_bounds<<<gv, 256, 0, s>>>(rk, rv, nv, nvp, g->off, mo, medge);
   NIDO_LAUNCH_CHECK();
