@@ -924,6 +924,25 @@ int set_smem(K kernel, size_t bytes) {
 }  // namespace
 
 namespace {
+// CTAs of every move kernel that fit on the GPU at once (SMs x resident CTAs
+// per SM, from the occupancy calculator): grid-stride kernels launched with
+// more would leave a partial wave at the end.
+struct Resident {
+  int64_t g4 = kSMs, g8 = kSMs, g16 = kSMs, g32 = kSMs, warp = kSMs, ctas = kSMs, ctam = kSMs, ctal = kSMs,
+          ctax = kSMs, hubmv = kSMs, hubins = kSMs, hubsl = kSMs;
+};
+Resident g_resident[2];
+
+template <typename K>
+int64_t resident(K kernel, int threads, size_t smem, int sms) {
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem) != cudaSuccess) {
+    cudaGetLastError();
+    per_sm = 1;
+  }
+  return (int64_t)std::max(per_sm, 1) * sms;
+}
+
 template <bool kMulti>
 int set_smem_mode() {
   NIDO_TRY(set_smem(k_move_warp<kWarpCap, kMulti>, (size_t)8 * kWarpCap * 16));
@@ -931,6 +950,22 @@ int set_smem_mode() {
   NIDO_TRY(set_smem(k_move_cta<256, kCtaMCap, kMulti>, (size_t)kCtaMCap * 16));
   NIDO_TRY(set_smem(k_move_cta<256, kCtaLCap, kMulti>, (size_t)kCtaLCap * 16));
   NIDO_TRY(set_smem(k_move_cta<1024, kCtaXCap, kMulti, false>, (size_t)kCtaXCap * 12));
+  int dev = 0, sms = kSMs;
+  NIDO_CUDA_TRY(cudaGetDevice(&dev));
+  NIDO_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  Resident& R = g_resident[kMulti ? 1 : 0];
+  R.g4 = resident(k_move_group<4, kMulti>, 256, 0, sms);
+  R.g8 = resident(k_move_group<8, kMulti>, 256, 0, sms);
+  R.g16 = resident(k_move_group<16, kMulti>, 256, 0, sms);
+  R.g32 = resident(k_move_group<32, kMulti>, 256, 0, sms);
+  R.warp = resident(k_move_warp<kWarpCap, kMulti>, 256, (size_t)8 * kWarpCap * 16, sms);
+  R.ctas = resident(k_move_cta<128, kCtaSCap, kMulti>, 128, (size_t)kCtaSCap * 16, sms);
+  R.ctam = resident(k_move_cta<256, kCtaMCap, kMulti>, 256, (size_t)kCtaMCap * 16, sms);
+  R.ctal = resident(k_move_cta<256, kCtaLCap, kMulti>, 256, (size_t)kCtaLCap * 16, sms);
+  R.ctax = resident(k_move_cta<1024, kCtaXCap, kMulti, false>, 1024, (size_t)kCtaXCap * 12, sms);
+  R.hubmv = resident(k_move_hub<kMulti>, kHubThreads, 0, sms);
+  R.hubins = resident(k_hub_insert, kHubThreads, 0, sms);
+  R.hubsl = resident(k_hub_slices<kMulti>, kHubThreads, 0, sms);
   return NIDO_OK;
 }
 
@@ -941,6 +976,7 @@ int set_smem_mode() {
 template <bool kMulti>
 int launch_tiers(nido_graph_s* g, int batch, int tie, const MoveArgs& p) {
   nido_ctx_s* ctx = g->ctx;
+  const Resident& R = g_resident[kMulti ? 1 : 0];
   const cudaStream_t main_s = ctx->stream;
   NIDO_CUDA_TRY(cudaEventRecord(ctx->fork_ev, main_s));
   for (int i = 0; i < 2; ++i) NIDO_CUDA_TRY(cudaStreamWaitEvent(ctx->aux[i], ctx->fork_ev, 0));
@@ -953,32 +989,32 @@ int launch_tiers(nido_graph_s* g, int batch, int tie, const MoveArgs& p) {
     const int32_t* list = g->perm + b0;
     switch (t) {
       case kTierG4:
-        k_move_group<4, kMulti><<<grid_cap((n + 63) / 64, kSMs * 16), 256, 0, s>>>(list, n, p);
+        k_move_group<4, kMulti><<<grid_cap((n + 63) / 64, R.g4), 256, 0, s>>>(list, n, p);
         break;
       case kTierG8:
-        k_move_group<8, kMulti><<<grid_cap((n + 31) / 32, kSMs * 16), 256, 0, s>>>(list, n, p);
+        k_move_group<8, kMulti><<<grid_cap((n + 31) / 32, R.g8), 256, 0, s>>>(list, n, p);
         break;
       case kTierG16:
-        k_move_group<16, kMulti><<<grid_cap((n + 15) / 16, kSMs * 16), 256, 0, s>>>(list, n, p);
+        k_move_group<16, kMulti><<<grid_cap((n + 15) / 16, R.g16), 256, 0, s>>>(list, n, p);
         break;
       case kTierG32:
-        k_move_group<32, kMulti><<<grid_cap((n + 7) / 8, kSMs * 16), 256, 0, s>>>(list, n, p);
+        k_move_group<32, kMulti><<<grid_cap((n + 7) / 8, R.g32), 256, 0, s>>>(list, n, p);
         break;
       case kTierWarp:
-        k_move_warp<kWarpCap, kMulti><<<grid_cap((n + 7) / 8, kSMs * 7), 256, (size_t)8 * kWarpCap * 16, s>>>(
+        k_move_warp<kWarpCap, kMulti><<<grid_cap((n + 7) / 8, R.warp), 256, (size_t)8 * kWarpCap * 16, s>>>(
             list, n, p);
         break;
       case kTierCtaS:
-        k_move_cta<128, kCtaSCap, kMulti><<<grid_cap(n, kSMs * 14), 128, (size_t)kCtaSCap * 16, s>>>(list, n, p);
+        k_move_cta<128, kCtaSCap, kMulti><<<grid_cap(n, R.ctas), 128, (size_t)kCtaSCap * 16, s>>>(list, n, p);
         break;
       case kTierCtaM:
-        k_move_cta<256, kCtaMCap, kMulti><<<grid_cap(n, kSMs * 7), 256, (size_t)kCtaMCap * 16, s>>>(list, n, p);
+        k_move_cta<256, kCtaMCap, kMulti><<<grid_cap(n, R.ctam), 256, (size_t)kCtaMCap * 16, s>>>(list, n, p);
         break;
       case kTierCtaL:
-        k_move_cta<256, kCtaLCap, kMulti><<<grid_cap(n, kSMs * 3), 256, (size_t)kCtaLCap * 16, s>>>(list, n, p);
+        k_move_cta<256, kCtaLCap, kMulti><<<grid_cap(n, R.ctal), 256, (size_t)kCtaLCap * 16, s>>>(list, n, p);
         break;
       case kTierCtaX:
-        k_move_cta<1024, kCtaXCap, kMulti, false><<<grid_cap(n, kSMs), 1024, (size_t)kCtaXCap * 12, s>>>(list, n, p);
+        k_move_cta<1024, kCtaXCap, kMulti, false><<<grid_cap(n, R.ctax), 1024, (size_t)kCtaXCap * 12, s>>>(list, n, p);
         break;
       default: {
         SliceResult* res = reinterpret_cast<SliceResult*>(g->hub_res);
@@ -986,16 +1022,16 @@ int launch_tiers(nido_graph_s* g, int batch, int tie, const MoveArgs& p) {
           const nido_graph_s::HubWave& w = g->hub_waves[wv];
           const int2* items = g->hub_items + w.i0;
           if (tie == NIDO_TIE_NIDO) {
-            k_move_hub<kMulti><<<grid_cap(w.i1 - w.i0, kSMs * 8), kHubThreads, 0, s>>>(
+            k_move_hub<kMulti><<<grid_cap(w.i1 - w.i0, R.hubmv), kHubThreads, 0, s>>>(
                 items, w.i1 - w.i0, g->hub_v, g->hub_toff, g->hub_capv, g->hub_nseg, g->hub_done, g->gkeys,
                 g->gvals, p);
             NIDO_LAUNCH_CHECK();
             continue;
           }
-          k_hub_insert<<<grid_cap(w.i1 - w.i0, kSMs * 8), kHubThreads, 0, s>>>(
+          k_hub_insert<<<grid_cap(w.i1 - w.i0, R.hubins), kHubThreads, 0, s>>>(
               items, w.i1 - w.i0, g->hub_v, g->hub_toff, g->hub_capv, g->gkeys, g->gvals, p);
           NIDO_LAUNCH_CHECK();
-          k_hub_slices<kMulti><<<grid_cap(w.s1 - w.s0, kSMs * 8), kHubThreads, 0, s>>>(
+          k_hub_slices<kMulti><<<grid_cap(w.s1 - w.s0, R.hubsl), kHubThreads, 0, s>>>(
               g->hub_slices + w.s0, w.s1 - w.s0, g->hub_v, g->hub_toff, g->hub_capv, g->gkeys, g->gvals, p,
               res + w.s0);
           NIDO_LAUNCH_CHECK();
