@@ -21,6 +21,7 @@
 // shuffle tree picks: among tied entries of rank r in the id-sorted list of
 // the vertex's neighbour communities, the smallest (bitrev3(r mod 8), r).
 #include <algorithm>
+#include <mutex>
 
 #include "common.cuh"
 #include "engine.cuh"
@@ -953,6 +954,8 @@ int set_smem_mode() {
   int dev = 0, sms = kSMs;
   NIDO_CUDA_TRY(cudaGetDevice(&dev));
   NIDO_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  static std::mutex mu;  // contexts may be created from several threads
+  std::lock_guard<std::mutex> lk(mu);
   Resident& R = g_resident[kMulti ? 1 : 0];
   R.g4 = resident(k_move_group<4, kMulti>, 256, 0, sms);
   R.g8 = resident(k_move_group<8, kMulti>, 256, 0, sms);

@@ -352,35 +352,81 @@ int launch_commit(nido_graph_s* g, int64_t v0, int64_t v1) {
 
 // Per-vertex in-community weight (self-loops included) of every listed
 // vertex, over all tiers of the current tier lists.
+// CTAs of the self-sum kernels resident on the GPU at once (grids are capped
+// there: grid-stride kernels launched with more leave a partial last wave)
+struct QResident {
+  int g4 = 148 * 8, g8 = 148 * 8, g16 = 148 * 8, g32 = 148 * 8, cta = 148 * 8;
+};
+
+template <typename K>
+int q_resident(K kernel, int threads, int sms) {
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, 0) != cudaSuccess) {
+    cudaGetLastError();
+    per_sm = 1;
+  }
+  return std::max(per_sm, 1) * sms;
+}
+
+QResident q_resident_all() {
+  QResident r;
+  int dev = 0, sms = 148;
+  if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+    cudaGetLastError();
+    return r;
+  }
+  r.g4 = q_resident(k_q_self_group<4>, kThreads, sms);
+  r.g8 = q_resident(k_q_self_group<8>, kThreads, sms);
+  r.g16 = q_resident(k_q_self_group<16>, kThreads, sms);
+  r.g32 = q_resident(k_q_self_group<32>, kThreads, sms);
+  r.cta = q_resident(k_q_self_cta<256>, 256, sms);
+  return r;
+}
+
+// The tiers' self-sums touch disjoint vertices: the large-degree tiers run
+// on the context's side streams beside the small ones (joined on return).
 int launch_q_self(nido_graph_s* g, double* selfv) {
-  cudaStream_t s = g->ctx->stream;
+  nido_ctx_s* ctx = g->ctx;
+  static const QResident g_qres = q_resident_all();  // once per process (thread-safe)
+  const cudaStream_t main_s = ctx->stream;
+  NIDO_CUDA_TRY(cudaEventRecord(ctx->fork_ev, main_s));
+  for (int i = 0; i < 2; ++i) NIDO_CUDA_TRY(cudaStreamWaitEvent(ctx->aux[i], ctx->fork_ev, 0));
   const int nb = g->nbatches;
-  for (int t = 0; t < kNumTiers; ++t) {
+  for (int t = kNumTiers - 1; t >= 0; --t) {
     const int64_t b0 = g->tier_off[(size_t)t * nb], b1 = g->tier_off[(size_t)(t + 1) * nb];
     const int64_t n = b1 - b0;
     if (n == 0) continue;
     const int32_t* list = g->perm + b0;
+    const cudaStream_t s = t >= kTierCtaL ? ctx->aux[0] : (t >= kTierG32 ? ctx->aux[1] : main_s);
     switch (t) {
       case kTierG4:
-        k_q_self_group<4><<<grid_for(n, kThreads / 4 * 8), kThreads, 0, s>>>(list, n, g->off, g->adj, g->w, g->comm, selfv);
+        k_q_self_group<4><<<grid_for(n, kThreads / 4 * 8, g_qres.g4), kThreads, 0, s>>>(list, n, g->off, g->adj, g->w,
+                                                                                       g->comm, selfv);
         break;
       case kTierG8:
-        k_q_self_group<8><<<grid_for(n, kThreads / 8 * 4), kThreads, 0, s>>>(list, n, g->off, g->adj, g->w, g->comm, selfv);
+        k_q_self_group<8><<<grid_for(n, kThreads / 8 * 4, g_qres.g8), kThreads, 0, s>>>(list, n, g->off, g->adj, g->w,
+                                                                                       g->comm, selfv);
         break;
       case kTierG16:
-        k_q_self_group<16><<<grid_for(n, kThreads / 16 * 2), kThreads, 0, s>>>(list, n, g->off, g->adj, g->w, g->comm, selfv);
+        k_q_self_group<16><<<grid_for(n, kThreads / 16 * 2, g_qres.g16), kThreads, 0, s>>>(list, n, g->off, g->adj,
+                                                                                           g->w, g->comm, selfv);
         break;
       case kTierG32:
       case kTierWarp:
       case kTierCtaS:
       case kTierCtaM:
-        k_q_self_group<32><<<grid_for(n, kThreads / 32), kThreads, 0, s>>>(list, n, g->off, g->adj, g->w, g->comm, selfv);
+        k_q_self_group<32><<<grid_for(n, kThreads / 32, g_qres.g32), kThreads, 0, s>>>(list, n, g->off, g->adj, g->w,
+                                                                                      g->comm, selfv);
         break;
       default:
-        k_q_self_cta<256><<<grid_for(n, 1, 148 * 8), 256, 0, s>>>(list, n, g->off, g->adj, g->w, g->comm, selfv);
+        k_q_self_cta<256><<<grid_for(n, 1, g_qres.cta), 256, 0, s>>>(list, n, g->off, g->adj, g->w, g->comm, selfv);
         break;
     }
     NIDO_LAUNCH_CHECK();
+  }
+  for (int i = 0; i < 2; ++i) {
+    NIDO_CUDA_TRY(cudaEventRecord(ctx->join_ev[i], ctx->aux[i]));
+    NIDO_CUDA_TRY(cudaStreamWaitEvent(main_s, ctx->join_ev[i], 0));
   }
   return NIDO_OK;
 }
