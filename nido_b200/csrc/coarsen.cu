@@ -596,19 +596,25 @@ int launch_aggregation(nido_graph_s* g, int* done) {
   AggArgs q{g->off, g->adj, g->w, newid, rv, mo, medge, g->adj2, g->w2, degp, nvp,
             reinterpret_cast<unsigned long long*>(g->dcount + 1), g->pm32};
   const int32_t* list = reinterpret_cast<const int32_t*>(tv);
+  // the three tiers write disjoint coarse vertices: the warp and CTA tiers
+  // run on the context's side streams while the giant path (which plans on
+  // the host) runs on its stream; all join before the offsets are scanned
+  nido_ctx_s* ctx = g->ctx;
+  NIDO_CUDA_TRY(cudaEventRecord(ctx->fork_ev, s));
+  for (int i = 0; i < 2; ++i) NIDO_CUDA_TRY(cudaStreamWaitEvent(ctx->aux[i], ctx->fork_ev, 0));
   if (cnt[0] > 0) {
     const int capmax = 2 * kAggWarpMaxD;
     const size_t sm = (size_t)8 * capmax * (sizeof(double) + 2 * sizeof(int));
     NIDO_CUDA_TRY(cudaFuncSetAttribute(k_agg_warp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    k_agg_warp<<<grid_for(cnt[0], 8, kSMs * 8), 256, sm, s>>>(list, cnt[0], q, capmax);
+    k_agg_warp<<<grid_for(cnt[0], 8, kSMs * 8), 256, sm, ctx->aux[0]>>>(list, cnt[0], q, capmax);
     NIDO_LAUNCH_CHECK();
   }
   if (cnt[1] > 0) {
     const int capmax = kAggCtaMaxCap;
     const size_t sm = (size_t)capmax * (sizeof(double) + 2 * sizeof(int));
     NIDO_CUDA_TRY(cudaFuncSetAttribute(k_agg_cta<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    k_agg_cta<false><<<grid_for(cnt[1], 1, kSMs * 2), kAggThreads, sm, s>>>(list + cnt[0], cnt[1], q, capmax,
-                                                                          nullptr, nullptr, nullptr, 0);
+    k_agg_cta<false><<<grid_for(cnt[1], 1, kSMs * 2), kAggThreads, sm, ctx->aux[1]>>>(
+        list + cnt[0], cnt[1], q, capmax, nullptr, nullptr, nullptr, 0);
     NIDO_LAUNCH_CHECK();
   }
   if (cnt[2] > 0) {
@@ -698,6 +704,10 @@ int launch_aggregation(nido_graph_s* g, int* done) {
       NIDO_LAUNCH_CHECK();
     }
     NIDO_CUDA_TRY(cudaStreamSynchronize(s));  // the host plan vectors go out of scope
+  }
+  for (int i = 0; i < 2; ++i) {
+    NIDO_CUDA_TRY(cudaEventRecord(ctx->join_ev[i], ctx->aux[i]));
+    NIDO_CUDA_TRY(cudaStreamWaitEvent(s, ctx->join_ev[i], 0));
   }
   // coarse offsets into off2, then the entries into the work CSR (when the
   // current graph is the work CSR, its lists are dead once pass 1 is done)
