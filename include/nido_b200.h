@@ -175,7 +175,7 @@ typedef struct {
   int32_t cta_s_max_degree;  /* 128-thread CTA, 1024 slots; <= 512 */
   int32_t cta_m_max_degree;  /* 256-thread CTA, 2048 slots; <= 1024 */
   int32_t cta_l_max_degree;  /* 256-thread CTA, 4096 slots; <= 2048 */
-  int32_t cta_x_max_degree;  /* 1024-thread CTA, 16384 slots; <= 8192; above: hub tier */
+  int32_t cta_x_max_degree;  /* 1024-thread CTA, 16384 slots; <= 12288; above: hub tier */
   int32_t reserved;
   int64_t hub_wave_slots;    /* hub-table slots processed together (L2 residency) */
 } nido_tier_config;

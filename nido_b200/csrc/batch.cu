@@ -67,7 +67,6 @@ struct nido_batch_s {
   double* selfv = nullptr;
   int64_t* counters = nullptr; // [0] iterating graphs [1] restoring [2] iterating vertices [3] aggregating
   int32_t* gid = nullptr;
-  int32_t* vbatch = nullptr;
   int64_t* outc = nullptr;     // final clustering of every original vertex (ids within its graph)
   int32_t* elist = nullptr;    // graphs whose clustering is written out now
   int64_t cap_part = 0, cap_modv = 0;
@@ -491,7 +490,7 @@ extern "C" int nido_batch_free(nido_batch B) {
                     (void*)B->gfin, (void*)B->loops_phase, (void*)B->loops_total, (void*)B->phases, (void*)B->Q,
                     (void*)B->Qold, (void*)B->qnew, (void*)B->mg, (void*)B->plist, (void*)B->llist,
                     (void*)B->moff, (void*)B->qoff, (void*)B->part, (void*)B->modv, (void*)B->selfv,
-                    (void*)B->counters, (void*)B->gid, (void*)B->vbatch, (void*)B->outc,
+                    (void*)B->counters, (void*)B->gid, (void*)B->outc,
                     (void*)B->elist})
       raw_free(ctx, p);
     ctx->used -= std::min(ctx->used, B->bytes);
@@ -538,7 +537,7 @@ extern "C" int nido_batch_upload(nido_ctx ctx, int32_t ngraphs, const int64_t* v
   take(&B->Q, G); take(&B->Qold, G); take(&B->qnew, G); take(&B->mg, G);
   take(&B->plist, G); take(&B->llist, G); take(&B->moff, G + 1); take(&B->qoff, G + 1);
   take(&B->part, B->cap_part); take(&B->modv, B->cap_modv); take(&B->selfv, V);
-  take(&B->counters, 4); take(&B->gid, V); take(&B->vbatch, V);
+  take(&B->counters, 4); take(&B->gid, V);
   take(&B->outc, V); take(&B->elist, G);
   if (st != NIDO_OK) {
     // device_alloc counted only what it allocated; nido_batch_free subtracts B->bytes
@@ -563,7 +562,6 @@ extern "C" int nido_batch_upload(nido_ctx ctx, int32_t ngraphs, const int64_t* v
   }
   g->gid = B->gid;
   g->mg = B->mg;
-  g->vbatch = B->vbatch;
   g->gcuts = B->gcuts;
   g->gactive = B->gactive;
   g->gbase = B->gbA;

@@ -530,7 +530,7 @@ int tune_tiers(nido_graph_s* g, int tie, int sweeps, double* best_ms) {
     g->cfg = best;
     return NIDO_OK;
   };
-  for (int32_t v : {4096, 2048}) { TierConfig c = best; c.ctax_max = std::max(v, best.ctal_max); NIDO_TRY(try_cfg(c)); }
+  for (int32_t v : {8192, 4096, 2048}) { TierConfig c = best; c.ctax_max = std::max(v, best.ctal_max); NIDO_TRY(try_cfg(c)); }
   for (int32_t v : {1024, 1536}) { TierConfig c = best; c.ctal_max = v; NIDO_TRY(try_cfg(c)); }
   for (int32_t v : {384, 256}) { TierConfig c = best; c.ctas_max = v; NIDO_TRY(try_cfg(c)); }
   for (int32_t v : {96, 64}) { TierConfig c = best; c.warp_max = v; NIDO_TRY(try_cfg(c)); }

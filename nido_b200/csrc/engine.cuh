@@ -28,7 +28,7 @@ enum Tier {
   kTierCtaS,    // d <= 512  : one 128-thread CTA, shared-memory hash (1024 slots)
   kTierCtaM,    // d <= 1024 : one 256-thread CTA, shared-memory hash (2048 slots)
   kTierCtaL,    // d <= 2048 : one 256-thread CTA, shared-memory hash (4096 slots)
-  kTierCtaX,    // d <= 8192 : one 1024-thread CTA, shared-memory hash (16384 slots, 192 KB)
+  kTierCtaX,    // d <= 12288: one 1024-thread CTA, shared-memory hash (16384 slots, 192 KB, load <= 3/4)
   kTierHub,     // larger    : 2048-edge segments on many CTAs, hash in global memory (L2)
   kNumTiers
 };
@@ -38,7 +38,7 @@ constexpr int kWarpMaxDeg = 128;
 constexpr int kCtaSMaxDeg = 512;
 constexpr int kCtaMMaxDeg = 1024;
 constexpr int kCtaLMaxDeg = 2048;
-constexpr int kCtaXMaxDeg = 8192;
+constexpr int kCtaXMaxDeg = 12288;  // table load up to 3/4 in the 16384 slots
 
 // Degree thresholds of the shared-memory tiers and the hub wave size.  The
 // defaults are the kernels' capacities; the tuner (engine.cu) may lower the
@@ -143,8 +143,8 @@ struct nido_graph_s {
   int64_t pm32_cap = 0;
 
   // many-graph mode (null / empty for one graph): the graph of every current
-  // vertex, the mass of every graph, and the batch of every vertex relative to
-  // its own graph's -b cuts
+  // vertex and the mass of every graph; vbatch (optional) receives every
+  // vertex's batch relative to its own graph's -b cuts
   int32_t* gid = nullptr;
   double* mg = nullptr;
   int32_t* vbatch = nullptr;
