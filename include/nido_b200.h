@@ -171,10 +171,10 @@ int nido_modularity_noalloc(void* stream, int64_t nv, const int64_t* d_off, cons
 /* ---- degree tiers and their autotuner (no reference counterpart: the reference
  * bins by fixed degree bounds, graph_gpu.cpp:602-624) -------------------------- */
 typedef struct {
-  int32_t warp_max_degree;   /* one warp, 256-slot shared table; <= 128 */
-  int32_t cta_s_max_degree;  /* 128-thread CTA, 1024 slots; <= 512 */
-  int32_t cta_m_max_degree;  /* 256-thread CTA, 2048 slots; <= 1024 */
-  int32_t cta_l_max_degree;  /* 256-thread CTA, 4096 slots; <= 2048 */
+  int32_t warp_max_degree;   /* one warp, 256-slot shared table; <= 192 */
+  int32_t cta_s_max_degree;  /* 128-thread CTA, 1024 slots; <= 768 */
+  int32_t cta_m_max_degree;  /* 256-thread CTA, 2048 slots; <= 1536 */
+  int32_t cta_l_max_degree;  /* 256-thread CTA, 4096 slots; <= 3072 */
   int32_t cta_x_max_degree;  /* 1024-thread CTA, 16384 slots; <= 12288; above: hub tier */
   int32_t reserved;
   int64_t hub_wave_slots;    /* hub-table slots processed together (L2 residency) */

@@ -530,10 +530,10 @@ int tune_tiers(nido_graph_s* g, int tie, int sweeps, double* best_ms) {
     g->cfg = best;
     return NIDO_OK;
   };
-  for (int32_t v : {8192, 4096, 2048}) { TierConfig c = best; c.ctax_max = std::max(v, best.ctal_max); NIDO_TRY(try_cfg(c)); }
-  for (int32_t v : {1024, 1536}) { TierConfig c = best; c.ctal_max = v; NIDO_TRY(try_cfg(c)); }
-  for (int32_t v : {384, 256}) { TierConfig c = best; c.ctas_max = v; NIDO_TRY(try_cfg(c)); }
-  for (int32_t v : {96, 64}) { TierConfig c = best; c.warp_max = v; NIDO_TRY(try_cfg(c)); }
+  for (int32_t v : {8192, 4096}) { TierConfig c = best; c.ctax_max = v; NIDO_TRY(try_cfg(c)); }
+  for (int32_t v : {2048, 1536}) { TierConfig c = best; c.ctal_max = v; NIDO_TRY(try_cfg(c)); }
+  for (int32_t v : {512, 384}) { TierConfig c = best; c.ctas_max = v; NIDO_TRY(try_cfg(c)); }
+  for (int32_t v : {128, 64}) { TierConfig c = best; c.warp_max = v; NIDO_TRY(try_cfg(c)); }
   if (g->max_degree > best.ctax_max)
     for (int64_t v : {(int64_t)2 << 20, (int64_t)8 << 20}) { TierConfig c = best; c.hub_wave_slots = v; NIDO_TRY(try_cfg(c)); }
   g->cfg = best;

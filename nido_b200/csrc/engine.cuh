@@ -24,20 +24,21 @@ enum Tier {
   kTierG8,      // d <= 8   : 8-lane group
   kTierG16,     // d <= 16  : 16-lane group
   kTierG32,     // d <= 32  : one warp, registers
-  kTierWarp,    // d <= 128  : one warp, shared-memory hash (256 slots)
-  kTierCtaS,    // d <= 512  : one 128-thread CTA, shared-memory hash (1024 slots)
-  kTierCtaM,    // d <= 1024 : one 256-thread CTA, shared-memory hash (2048 slots)
-  kTierCtaL,    // d <= 2048 : one 256-thread CTA, shared-memory hash (4096 slots)
+  kTierWarp,    // d <= 192  : one warp, shared-memory hash (256 slots)
+  kTierCtaS,    // d <= 768  : one 128-thread CTA, shared-memory hash (1024 slots)
+  kTierCtaM,    // d <= 1536 : one 256-thread CTA, shared-memory hash (2048 slots)
+  kTierCtaL,    // d <= 3072 : one 256-thread CTA, shared-memory hash (4096 slots)
   kTierCtaX,    // d <= 12288: one 1024-thread CTA, shared-memory hash (16384 slots, 192 KB, load <= 3/4)
   kTierHub,     // larger    : 2048-edge segments on many CTAs, hash in global memory (L2)
   kNumTiers
 };
 
-// degree bounds of the tiers (the shared-memory table sizes are fixed by them)
-constexpr int kWarpMaxDeg = 128;
-constexpr int kCtaSMaxDeg = 512;
-constexpr int kCtaMMaxDeg = 1024;
-constexpr int kCtaLMaxDeg = 2048;
+// largest degree each shared-memory tier accepts: its table (256 / 1024 /
+// 2048 / 4096 / 16384 slots) filled to at most 3/4
+constexpr int kWarpMaxDeg = 192;
+constexpr int kCtaSMaxDeg = 768;
+constexpr int kCtaMMaxDeg = 1536;
+constexpr int kCtaLMaxDeg = 3072;
 constexpr int kCtaXMaxDeg = 12288;  // table load up to 3/4 in the 16384 slots
 
 // Degree thresholds of the shared-memory tiers and the hub wave size.  The

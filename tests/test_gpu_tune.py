@@ -17,10 +17,11 @@ def test_lowered_thresholds_same_result(nido_lib, ctx, rmat16):
         want, st0 = g.run()
         c = g.tier_config()
         assert (c.warp_max_degree, c.cta_s_max_degree, c.cta_m_max_degree, c.cta_l_max_degree,
-                c.cta_x_max_degree) == (128, 512, 1024, 2048, 12288)
+                c.cta_x_max_degree) == (192, 768, 1536, 3072, 12288)
         for warp, ctas, ctam, ctal, ctax, wave in ((64, 256, 1024, 1024, 1024, 1 << 16), (32, 32, 32, 32, 32, 1 << 16),
                                                    (96, 384, 768, 1536, 4096, 8 << 20), (128, 512, 1024, 2048, 2048, 4 << 20),
-                                                   (128, 512, 1024, 2048, 12288, 4 << 20)):
+                                                   (128, 512, 1024, 2048, 12288, 4 << 20),
+                                                   (192, 768, 1536, 3072, 12288, 4 << 20)):
             c = nido_lib.TierConfig(warp, ctas, ctam, ctal, ctax, 0, wave)
             g.set_tier_config(c)
             got, st = g.run()
@@ -30,8 +31,8 @@ def test_lowered_thresholds_same_result(nido_lib, ctx, rmat16):
 
 def test_invalid_configs_rejected(nido_lib, ctx, rmat16):
     with nido_lib.Graph(ctx, rmat16, 2) as g:
-        for bad in ((129, 512, 1024, 2048, 8192, 1 << 20), (128, 100, 1024, 2048, 8192, 1 << 20),
-                    (64, 512, 1025, 2048, 8192, 1 << 20), (64, 512, 1024, 4096, 8192, 1 << 20),
+        for bad in ((193, 512, 1024, 2048, 8192, 1 << 20), (128, 100, 1024, 2048, 8192, 1 << 20),
+                    (64, 512, 1537, 2048, 8192, 1 << 20), (64, 512, 1024, 4096, 8192, 1 << 20),
                     (64, 512, 1024, 2048, 1024, 1 << 20), (64, 512, 1024, 2048, 12289, 1 << 20),
                     (64, 512, 1024, 2048, 8192, 10)):
             w, s, m, l, x, wave = bad
@@ -46,7 +47,7 @@ def test_tuned_run_same_result(nido_lib, ctx, rmat16, tie):
     with nido_lib.Graph(ctx, rmat16, 2) as g:
         got, st = g.run(tie=tie, tune=True)
         c = g.tier_config()
-        assert 32 <= c.warp_max_degree <= c.cta_s_max_degree <= c.cta_m_max_degree <= c.cta_l_max_degree <= 2048
+        assert 32 <= c.warp_max_degree <= c.cta_s_max_degree <= c.cta_m_max_degree <= c.cta_l_max_degree <= 3072
         assert c.cta_l_max_degree <= c.cta_x_max_degree <= 12288
         assert st.host_ms[6] > 0
         assert np.array_equal(got, want)
