@@ -37,9 +37,9 @@ PEAKS_FALLBACK = {"hbm_gbs": 6650.0}
 
 # DRAM bytes the move kernels move per algorithmic byte (16 B per edge +
 # 32 B per vertex per sweep): ncu dram__bytes_read.sum + dram__bytes_write.sum
-# over every move kernel of one whole R-MAT scale 20 run (84 sweeps), 38.09 GB
+# over every move kernel of one whole R-MAT scale 20 run (84 sweeps), 26.19 GB
 # against 20.71 GB algorithmic, cold cache per kernel (an upper bound).
-MOVE_TRAFFIC_PER_ALGO_BYTE = 1.84
+MOVE_TRAFFIC_PER_ALGO_BYTE = 1.26
 
 
 def peaks():

@@ -912,10 +912,14 @@ int plan_hubs(nido_graph_s* g) {
 
 namespace {
 constexpr int kWarpCap = 256;     // warp tier: degree <= 128
-constexpr int kCtaSCap = 1024;    // 128-thread CTA tier: degree <= 512
-constexpr int kCtaMCap = 2048;    // 256-thread CTA tier: degree <= 1024
-constexpr int kCtaLCap = 4096;    // 256-thread CTA tier: degree <= 2048
-constexpr int kCtaXCap = 16384;   // 1024-thread CTA tier: degree <= 8192 (no occupied list)
+// threads per CTA and table slots of the CTA tiers
+constexpr int kCtaSThreads = 128;
+constexpr int kCtaMThreads = 256;
+constexpr int kCtaLThreads = 256;
+constexpr int kCtaSCap = 1024;
+constexpr int kCtaMCap = 2048;
+constexpr int kCtaLCap = 4096;
+constexpr int kCtaXCap = 16384;   // 1024-thread CTA-XL tier (no occupied list)
 
 template <typename K>
 int set_smem(K kernel, size_t bytes) {
@@ -947,9 +951,9 @@ int64_t resident(K kernel, int threads, size_t smem, int sms) {
 template <bool kMulti>
 int set_smem_mode() {
   NIDO_TRY(set_smem(k_move_warp<kWarpCap, kMulti>, (size_t)8 * kWarpCap * 16));
-  NIDO_TRY(set_smem(k_move_cta<128, kCtaSCap, kMulti>, (size_t)kCtaSCap * 16));
-  NIDO_TRY(set_smem(k_move_cta<256, kCtaMCap, kMulti>, (size_t)kCtaMCap * 16));
-  NIDO_TRY(set_smem(k_move_cta<256, kCtaLCap, kMulti>, (size_t)kCtaLCap * 16));
+  NIDO_TRY(set_smem(k_move_cta<kCtaSThreads, kCtaSCap, kMulti>, (size_t)kCtaSCap * 16));
+  NIDO_TRY(set_smem(k_move_cta<kCtaMThreads, kCtaMCap, kMulti>, (size_t)kCtaMCap * 16));
+  NIDO_TRY(set_smem(k_move_cta<kCtaLThreads, kCtaLCap, kMulti>, (size_t)kCtaLCap * 16));
   NIDO_TRY(set_smem(k_move_cta<1024, kCtaXCap, kMulti, false>, (size_t)kCtaXCap * 12));
   int dev = 0, sms = kSMs;
   NIDO_CUDA_TRY(cudaGetDevice(&dev));
@@ -962,9 +966,9 @@ int set_smem_mode() {
   R.g16 = resident(k_move_group<16, kMulti>, 256, 0, sms);
   R.g32 = resident(k_move_group<32, kMulti>, 256, 0, sms);
   R.warp = resident(k_move_warp<kWarpCap, kMulti>, 256, (size_t)8 * kWarpCap * 16, sms);
-  R.ctas = resident(k_move_cta<128, kCtaSCap, kMulti>, 128, (size_t)kCtaSCap * 16, sms);
-  R.ctam = resident(k_move_cta<256, kCtaMCap, kMulti>, 256, (size_t)kCtaMCap * 16, sms);
-  R.ctal = resident(k_move_cta<256, kCtaLCap, kMulti>, 256, (size_t)kCtaLCap * 16, sms);
+  R.ctas = resident(k_move_cta<kCtaSThreads, kCtaSCap, kMulti>, kCtaSThreads, (size_t)kCtaSCap * 16, sms);
+  R.ctam = resident(k_move_cta<kCtaMThreads, kCtaMCap, kMulti>, kCtaMThreads, (size_t)kCtaMCap * 16, sms);
+  R.ctal = resident(k_move_cta<kCtaLThreads, kCtaLCap, kMulti>, kCtaLThreads, (size_t)kCtaLCap * 16, sms);
   R.ctax = resident(k_move_cta<1024, kCtaXCap, kMulti, false>, 1024, (size_t)kCtaXCap * 12, sms);
   R.hubmv = resident(k_move_hub<kMulti>, kHubThreads, 0, sms);
   R.hubins = resident(k_hub_insert, kHubThreads, 0, sms);
@@ -1008,13 +1012,13 @@ int launch_tiers(nido_graph_s* g, int batch, int tie, const MoveArgs& p) {
             list, n, p);
         break;
       case kTierCtaS:
-        k_move_cta<128, kCtaSCap, kMulti><<<grid_cap(n, R.ctas), 128, (size_t)kCtaSCap * 16, s>>>(list, n, p);
+        k_move_cta<kCtaSThreads, kCtaSCap, kMulti><<<grid_cap(n, R.ctas), kCtaSThreads, (size_t)kCtaSCap * 16, s>>>(list, n, p);
         break;
       case kTierCtaM:
-        k_move_cta<256, kCtaMCap, kMulti><<<grid_cap(n, R.ctam), 256, (size_t)kCtaMCap * 16, s>>>(list, n, p);
+        k_move_cta<kCtaMThreads, kCtaMCap, kMulti><<<grid_cap(n, R.ctam), kCtaMThreads, (size_t)kCtaMCap * 16, s>>>(list, n, p);
         break;
       case kTierCtaL:
-        k_move_cta<256, kCtaLCap, kMulti><<<grid_cap(n, R.ctal), 256, (size_t)kCtaLCap * 16, s>>>(list, n, p);
+        k_move_cta<kCtaLThreads, kCtaLCap, kMulti><<<grid_cap(n, R.ctal), kCtaLThreads, (size_t)kCtaLCap * 16, s>>>(list, n, p);
         break;
       case kTierCtaX:
         k_move_cta<1024, kCtaXCap, kMulti, false><<<grid_cap(n, R.ctax), 1024, (size_t)kCtaXCap * 12, s>>>(list, n, p);
