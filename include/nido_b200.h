@@ -98,6 +98,11 @@ int nido_ctx_destroy(nido_ctx ctx);
 int nido_ctx_sync(nido_ctx ctx);
 /* the ctx's cudaStream_t, for callers that order their own work with it */
 int nido_ctx_stream(nido_ctx ctx, void** stream);
+/* Device blocks freed by this context's graphs stay with the context and are
+ * reused by its later uploads and runs (no cudaMalloc / cudaFree between
+ * graphs).  This returns the free ones to the driver; released_bytes (may be
+ * null) receives their size.  Destroying the context does the same. */
+int nido_ctx_trim(nido_ctx ctx, size_t* released_bytes);
 
 /* ---- graphs ----------------------------------------------------------------- */
 /* Upload a CSR and compute k_v and m.  Replaces the GraphGPU constructor

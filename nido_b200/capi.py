@@ -84,6 +84,7 @@ def lib() -> C.CDLL:
             "nido_ctx_destroy": (C.c_int, [vp]),
             "nido_ctx_sync": (C.c_int, [vp]),
             "nido_ctx_stream": (C.c_int, [vp, C.POINTER(vp)]),
+            "nido_ctx_trim": (C.c_int, [vp, C.POINTER(C.c_size_t)]),
             "nido_graph_upload": (C.c_int, [vp, C.c_int64, C.c_int64, _i64p, _i64p, _f64p, C.c_int32,
                                             C.POINTER(vp)]),
             "nido_graph_free": (C.c_int, [vp]),
@@ -246,6 +247,13 @@ class Context:
         s = C.c_void_p()
         _check(lib().nido_ctx_stream(self.h, C.byref(s)))
         return s.value or 0
+
+    def trim(self) -> int:
+        """Return the device blocks cached from freed graphs to the driver;
+        the number of bytes released."""
+        n = C.c_size_t()
+        _check(lib().nido_ctx_trim(self.h, C.byref(n)))
+        return n.value
 
     def close(self):
         if self.h:

@@ -17,13 +17,65 @@
 using nido::Arena;
 
 namespace nido {
-cudaError_t raw_alloc(nido_ctx_s* ctx, void** p, size_t bytes) {
-  return ctx->async_alloc ? cudaMallocAsync(p, bytes, ctx->stream) : cudaMalloc(p, bytes);
+// Blocks of a context that is not stream-ordered: cudaMalloc maps new memory
+// (tens to hundreds of ms for the few GB of a large graph) and cudaFree waits
+// for the whole device, so freed blocks stay with the context and later
+// requests reuse them: the smallest free block of at least the request and at
+// most twice it.  Sizes are rounded (512 B; 2 MiB from 1 MiB up).  Every use
+// of a block is on the context's stream or on side streams joined back to it,
+// so a reused block's new work is ordered after its old work.  When cudaMalloc
+// fails the free blocks are released and the call retried; destroying the
+// context releases them.
+namespace {
+size_t block_size(size_t bytes) {
+  const size_t g = bytes >= ((size_t)1 << 20) ? ((size_t)2 << 20) : (size_t)512;
+  return (std::max<size_t>(bytes, 1) + g - 1) / g * g;
 }
+}  // namespace
+
+cudaError_t raw_alloc(nido_ctx_s* ctx, void** p, size_t bytes) {
+  if (ctx->async_alloc) return cudaMallocAsync(p, bytes, ctx->stream);
+  const size_t b = block_size(bytes);
+  auto it = ctx->free_blocks.lower_bound(b);
+  if (it != ctx->free_blocks.end() && it->first <= 2 * b) {
+    *p = it->second;
+    ctx->live_blocks[it->second] = it->first;
+    ctx->cached_bytes -= it->first;
+    ctx->free_blocks.erase(it);
+    return cudaSuccess;
+  }
+  cudaError_t e = cudaMalloc(p, b);
+  if (e == cudaErrorMemoryAllocation && !ctx->free_blocks.empty()) {
+    cudaGetLastError();
+    release_cached(ctx);
+    e = cudaMalloc(p, b);
+  }
+  if (e == cudaSuccess) ctx->live_blocks[*p] = b;
+  return e;
+}
+
 void raw_free(nido_ctx_s* ctx, void* p) {
   if (!p) return;
-  if (ctx->async_alloc) cudaFreeAsync(p, ctx->stream);
-  else cudaFree(p);
+  if (ctx->async_alloc) {
+    cudaFreeAsync(p, ctx->stream);
+    return;
+  }
+  auto it = ctx->live_blocks.find(p);
+  if (it == ctx->live_blocks.end()) {  // not from raw_alloc
+    cudaFree(p);
+    return;
+  }
+  ctx->free_blocks.emplace(it->second, p);
+  ctx->cached_bytes += it->second;
+  ctx->live_blocks.erase(it);
+}
+
+void release_cached(nido_ctx_s* ctx) {
+  if (ctx->free_blocks.empty()) return;
+  cudaStreamSynchronize(ctx->stream);
+  for (auto& kv : ctx->free_blocks) cudaFree(kv.second);
+  ctx->free_blocks.clear();
+  ctx->cached_bytes = 0;
 }
 }  // namespace nido
 
@@ -166,8 +218,17 @@ extern "C" int nido_ctx_destroy(nido_ctx ctx) {
     if (ctx->join_ev[i]) cudaEventDestroy(ctx->join_ev[i]);
   }
   if (ctx->fork_ev) cudaEventDestroy(ctx->fork_ev);
+  nido::release_cached(ctx);
   cudaStreamDestroy(ctx->stream);
   delete ctx;
+  return NIDO_OK;
+}
+
+extern "C" int nido_ctx_trim(nido_ctx ctx, size_t* released_bytes) {
+  if (!ctx) return nido_set_error(NIDO_E_INVALID, "null context");
+  NIDO_CUDA_TRY(cudaSetDevice(ctx->device));
+  if (released_bytes) *released_bytes = ctx->cached_bytes;
+  nido::release_cached(ctx);
   return NIDO_OK;
 }
 
@@ -201,7 +262,8 @@ extern "C" int nido_graph_free(nido_graph g) {
   // hub-tier buffers are sized per phase outside the budget accounting
   for (void* p : {(void*)g->gkeys, (void*)g->gvals, (void*)g->hub_items, (void*)g->hub_v, (void*)g->hub_capv,
                   (void*)g->hub_nseg, (void*)g->hub_toff, (void*)g->hub_done, (void*)g->hub_slices,
-                  (void*)g->hub_slice_first, (void*)g->hub_res, (void*)g->agg_buf, (void*)g->pm32})
+                  (void*)g->hub_slice_first, (void*)g->hub_res, (void*)g->hub_item_first,
+                  (void*)g->hub_part, (void*)g->agg_buf, (void*)g->pm32})
     nido::raw_free(ctx, p);
   for (nido_graph_s::MoveGraph& mg : g->move_graphs)
     if (mg.exec) cudaGraphExecDestroy(mg.exec);

@@ -14,6 +14,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <map>
+#include <unordered_map>
 #include <vector>
 
 #include "common.cuh"
@@ -40,6 +42,7 @@ constexpr int kCtaSMaxDeg = 768;
 constexpr int kCtaMMaxDeg = 1536;
 constexpr int kCtaLMaxDeg = 3072;
 constexpr int kCtaXMaxDeg = 12288;  // table load up to 3/4 in the 16384 slots
+constexpr int kHubSeg = 2048;        // edges of one hub segment (move and modularity)
 
 // Degree thresholds of the shared-memory tiers and the hub wave size.  The
 // defaults are the kernels' capacities; the tuner (engine.cu) may lower the
@@ -70,6 +73,12 @@ struct nido_ctx_s {
   // context's stream): allocating or freeing then does not wait for the work
   // of other contexts on the same GPU
   bool async_alloc = false;
+  // otherwise blocks come from cudaMalloc and are kept for reuse when freed
+  // (raw_alloc / raw_free): free blocks by size, the size of every block in
+  // use, and the bytes held in free blocks
+  std::multimap<size_t, void*> free_blocks;
+  std::unordered_map<void*, size_t> live_blocks;
+  size_t cached_bytes = 0;
 };
 
 struct nido_graph_s {
@@ -136,6 +145,11 @@ struct nido_graph_s {
   int64_t* hub_slice_first = nullptr;
   char* hub_res = nullptr;
   int64_t hub_cap_slices = 0, hub_cap_first = 0, hub_cap_res = 0;
+  // first segment item of every hub (nhubs + 1; items run in hub order) and
+  // the per-item partial in-community sums of the modularity
+  int64_t* hub_item_first = nullptr;
+  double* hub_part = nullptr;
+  int64_t hub_cap_ifirst = 0, hub_cap_part = 0, hub_nitems = 0;
   // coarsening plan and tables of giant coarse vertices (grows, never shrinks,
   // so runs after the first allocate nothing)
   char* agg_buf = nullptr;
@@ -207,6 +221,7 @@ int graph_prepare_phase(nido_graph_s* g);               // k, m, tier lists (eng
 // device memory of a context: stream-ordered when ctx->async_alloc (engine.cu)
 cudaError_t raw_alloc(nido_ctx_s* ctx, void** p, size_t bytes);
 void raw_free(nido_ctx_s* ctx, void* p);  // null is a no-op
+void release_cached(nido_ctx_s* ctx);     // cudaFree every cached free block
 // device memory counted against the context's HBM budget (engine.cu)
 int device_alloc(nido_ctx_s* ctx, void** p, size_t bytes);
 void device_free(nido_ctx_s* ctx, void* p, size_t bytes);

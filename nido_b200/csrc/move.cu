@@ -611,7 +611,6 @@ __global__ void __launch_bounds__(kThreads) k_move_cta(const int32_t* __restrict
 // Each CTA takes one (hub, segment) item and merges its edges into the hub's
 // table in global memory (L2-resident); the CTA that finishes a hub's last
 // segment (an atomic ticket; nobody waits) evaluates and clears the table.
-constexpr int kHubSeg = 2048;
 constexpr int kHubThreads = 256;
 
 template <bool kMulti>
@@ -821,6 +820,7 @@ int plan_hubs(nido_graph_s* g) {
   g->hub_waves.clear();
   g->hub_wave_off.assign(nb + 1, 0);
   g->nhubs = nh;
+  g->hub_nitems = 0;
   if (nh == 0) return NIDO_OK;
   cudaStream_t s = g->ctx->stream;
   Arena ar(g->scratch, g->scratch_bytes);
@@ -850,6 +850,7 @@ int plan_hubs(nido_graph_s* g) {
   // slices of a hub follow one another.
   std::vector<int2> slices;
   std::vector<int64_t> sfirst(nh + 1, 0);
+  std::vector<int64_t> ifirst(nh + 1, 0);
   g->hub_waves.clear();
   g->hub_wave_off.assign(nb + 1, 0);
   int64_t maxslots = 0;
@@ -865,6 +866,7 @@ int plan_hubs(nido_graph_s* g) {
       htoff[i] = wslots;
       wslots += hcap[i];
       maxslots = std::max(maxslots, wslots);
+      ifirst[i] = (int64_t)items.size();
       for (int sgi = 0; sgi < hseg[i]; ++sgi) items.push_back(make_int2((int)i, sgi));
       sfirst[i] = (int64_t)slices.size();
       for (int sl = 0; sl * kHubSlice < hcap[i]; ++sl) slices.push_back(make_int2((int)i, sl));
@@ -876,6 +878,8 @@ int plan_hubs(nido_graph_s* g) {
     }
     g->hub_wave_off[b + 1] = (int64_t)g->hub_waves.size();
   }
+  ifirst[nh] = (int64_t)items.size();
+  g->hub_nitems = (int64_t)items.size();
   const int64_t toff = maxslots;
   NIDO_TRY(ensure(g, &g->hub_v, &g->hub_cap_hubs_v, nh));
   NIDO_TRY(ensure(g, &g->hub_capv, &g->hub_cap_hubs_c, nh));
@@ -886,6 +890,9 @@ int plan_hubs(nido_graph_s* g) {
   NIDO_TRY(ensure(g, &g->hub_slices, &g->hub_cap_slices, (int64_t)slices.size()));
   NIDO_TRY(ensure(g, &g->hub_slice_first, &g->hub_cap_first, nh + 1));
   NIDO_TRY(ensure(g, &g->hub_res, &g->hub_cap_res, (int64_t)(slices.size() * sizeof(SliceResult))));
+  NIDO_TRY(ensure(g, &g->hub_item_first, &g->hub_cap_ifirst, nh + 1));
+  NIDO_TRY(ensure(g, &g->hub_part, &g->hub_cap_part, (int64_t)items.size()));
+  NIDO_CUDA_TRY(cudaMemcpyAsync(g->hub_item_first, ifirst.data(), sizeof(int64_t) * (nh + 1), cudaMemcpyHostToDevice, s));
   NIDO_CUDA_TRY(cudaMemcpyAsync(g->hub_slices, slices.data(), sizeof(int2) * slices.size(), cudaMemcpyHostToDevice, s));
   NIDO_CUDA_TRY(cudaMemcpyAsync(g->hub_slice_first, sfirst.data(), sizeof(int64_t) * (nh + 1), cudaMemcpyHostToDevice, s));
   if (toff > g->gslab) {

@@ -197,6 +197,50 @@ __global__ void __launch_bounds__(T) k_q_self_cta(const int32_t* __restrict__ li
   }
 }
 
+// Hub tier: one CTA per kHubSeg-edge segment of the hub plan (a partial sum
+// per item), then one warp per hub adds its items' partials (lane-strided,
+// then a fixed tree), so a hub's sum is spread over many CTAs instead of
+// running its whole edge list on one.
+__global__ void __launch_bounds__(256) k_q_self_seg(const int2* __restrict__ items, int64_t n,
+                                                    const int32_t* __restrict__ hub_v,
+                                                    const int64_t* __restrict__ off,
+                                                    const int32_t* __restrict__ adj,
+                                                    const double* __restrict__ w,
+                                                    const int32_t* __restrict__ comm,
+                                                    double* __restrict__ part) {
+  __shared__ double ws[8];
+  for (int64_t idx = blockIdx.x; idx < n; idx += gridDim.x) {
+    const int2 it = items[idx];
+    const int v = hub_v[it.x];
+    const int64_t e0 = off[v] + (int64_t)it.y * kHubSeg;
+    const int64_t e1 = min(off[v + 1], e0 + kHubSeg);
+    double x = own_weight(adj, w, comm, comm[v], e0 + threadIdx.x, e1, 256);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(NIDO_FULL_MASK, x, o);
+    if ((threadIdx.x & 31) == 0) ws[threadIdx.x >> 5] = x;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double s = 0.;
+      for (int i = 0; i < 8; ++i) s += ws[i];
+      part[idx] = s;
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void k_q_hub_sum(int64_t nh, const int32_t* __restrict__ hub_v, const int64_t* __restrict__ first,
+                            const double* __restrict__ part, double* __restrict__ selfv) {
+  const int lane = threadIdx.x & 31;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t h = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; h < nh; h += nw) {
+    double x = 0.;
+    for (int64_t i = first[h] + lane; i < first[h + 1]; i += 32) x += part[i];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(NIDO_FULL_MASK, x, o);
+    if (lane == 0) selfv[hub_v[h]] = x;
+  }
+}
+
 // Stage 2: the reference's thread slots and 16-lane groups
 // (compute_modularity_reduce_kernel<128,16>, graph_cuda.cu:2096-2134, grid
 // min(ceil(nv/8), 65535)): slot t takes vertices t, t+S, ...; ac folds
@@ -355,7 +399,7 @@ int launch_commit(nido_graph_s* g, int64_t v0, int64_t v1) {
 // CTAs of the self-sum kernels resident on the GPU at once (grids are capped
 // there: grid-stride kernels launched with more leave a partial last wave)
 struct QResident {
-  int g4 = 148 * 8, g8 = 148 * 8, g16 = 148 * 8, g32 = 148 * 8, cta = 148 * 8;
+  int g4 = 148 * 8, g8 = 148 * 8, g16 = 148 * 8, g32 = 148 * 8, cta = 148 * 8, seg = 148 * 8;
 };
 
 template <typename K>
@@ -380,6 +424,7 @@ QResident q_resident_all() {
   r.g16 = q_resident(k_q_self_group<16>, kThreads, sms);
   r.g32 = q_resident(k_q_self_group<32>, kThreads, sms);
   r.cta = q_resident(k_q_self_cta<256>, 256, sms);
+  r.seg = q_resident(k_q_self_seg, 256, sms);
   return r;
 }
 
@@ -417,6 +462,17 @@ int launch_q_self(nido_graph_s* g, double* selfv) {
       case kTierCtaM:
         k_q_self_group<32><<<grid_for(n, kThreads / 32, g_qres.g32), kThreads, 0, s>>>(list, n, g->off, g->adj, g->w,
                                                                                       g->comm, selfv);
+        break;
+      case kTierHub:
+        if (g->nhubs == n && g->hub_nitems > 0) {  // the hub plan covers this list
+          k_q_self_seg<<<grid_for(g->hub_nitems, 1, g_qres.seg), 256, 0, s>>>(
+              g->hub_items, g->hub_nitems, g->hub_v, g->off, g->adj, g->w, g->comm, g->hub_part);
+          NIDO_LAUNCH_CHECK();
+          k_q_hub_sum<<<grid_for(n * 32, 256, kSMs * 8), 256, 0, s>>>(n, g->hub_v, g->hub_item_first, g->hub_part,
+                                                                     selfv);
+          break;
+        }
+        k_q_self_cta<256><<<grid_for(n, 1, g_qres.cta), 256, 0, s>>>(list, n, g->off, g->adj, g->w, g->comm, selfv);
         break;
       default:
         k_q_self_cta<256><<<grid_for(n, 1, g_qres.cta), 256, 0, s>>>(list, n, g->off, g->adj, g->w, g->comm, selfv);

@@ -269,3 +269,22 @@ def test_full_size_rmat_properties(nido_lib, ctx, orc):
     # communities are dense ids 0..n-1
     u = np.unique(cl)
     assert u[0] == 0 and u[-1] == len(u) - 1
+
+
+def test_freed_blocks_reused_and_trimmed(nido_lib):
+    """A context keeps the blocks of a freed graph and its next upload of the
+    same sizes reuses them (the cache does not grow); results are unchanged;
+    nido_ctx_trim hands the cached bytes back to the driver."""
+    G = nido_lib.gen_rmat(1 << 15, 16 << 15, wmode=nido_lib.W_INT8, seed=5)
+    with nido_lib.Context(0) as c:
+        with nido_lib.Graph(c, G, 2) as g:
+            want, st0 = g.run()
+            used = g.device_bytes()
+        held = c.trim()
+        assert held >= used * 0.9
+        assert c.trim() == 0
+        for _ in range(3):
+            with nido_lib.Graph(c, G, 2) as g:
+                got, st = g.run()
+            assert np.array_equal(got, want) and st.final_q == st0.final_q
+        assert c.trim() == held  # three uploads, one set of blocks
