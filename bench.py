@@ -208,6 +208,12 @@ def run_ours(args, world, rank, local):
     ms_max = reduce_max(ms, world)
     move_ms = sum(s.move_ms for s in stats)
     move_bytes = sum(s.move_bytes for s in stats)
+    # device time per run by section (CUDA events; the rest is batching,
+    # commits, per-phase preparation and host round trips)
+    n = len(stats)
+    breakdown = {"move": move_ms / n, "modularity": sum(s.q_ms for s in stats) / n,
+                 "aggregation": sum(s.agg_ms for s in stats) / n}
+    breakdown["other"] = sum(s.total_ms for s in stats) / n - sum(breakdown.values())
     sweeps = sum(s.total_loops for s in stats)
     edges_per_run = stats[0].edges_scanned
     # edges a whole run visits in the CPU oracle's count (one modularity sweep
@@ -268,6 +274,7 @@ def run_ours(args, world, rank, local):
                    "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (CSR 12 B/edge)"},
         "edges_scanned_per_s": world * edges_per_run * args.steps / sec,
         "move_sweeps_per_run": sweeps / args.steps, "final_q": final_q,
+        "breakdown_ms_per_run": breakdown,
         "e2e": {"value": world * args.steps / (e2e_ms * 1e-3), "unit": "graphs/s",
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",

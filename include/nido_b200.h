@@ -83,6 +83,8 @@ typedef struct {
   int64_t loops_phase[200];
   int64_t nv_phase[200];
   int64_t ne_phase[200];
+  double q_ms;         /* device time of the modularity evaluations */
+  double agg_ms;       /* device time of the aggregations (coarsening) */
 } nido_run_stats;
 
 /* ---- library ---------------------------------------------------------------- */

@@ -30,6 +30,7 @@ def main():
             _, st = g.run(tau=a.t, max_iter=a.i, tie=tie, tune=a.tune)
             print(json.dumps({"run": r, "nv": G.nv, "ne": G.ne, "phases": st.phases, "loops": st.total_loops,
                               "final_q": st.final_q, "total_ms": st.total_ms, "move_ms": st.move_ms,
+                              "q_ms": st.q_ms, "agg_ms": st.agg_ms,
                               "move_gbs": st.move_bytes / (st.move_ms * 1e6) if st.move_ms else 0.0,
                               "kernel_launches": st.kernel_launches,
                               "tiers": g.tier_config().as_dict()}), flush=True)

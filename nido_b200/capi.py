@@ -45,7 +45,7 @@ class RunStats(C.Structure):
                 ("edges_scanned", C.c_double), ("move_launches", C.c_int64),
                 ("kernel_launches", C.c_int64), ("host_ms", C.c_double * 8), ("q_phase", C.c_double * 200),
                 ("loops_phase", C.c_int64 * 200), ("nv_phase", C.c_int64 * 200),
-                ("ne_phase", C.c_int64 * 200)]
+                ("ne_phase", C.c_int64 * 200), ("q_ms", C.c_double), ("agg_ms", C.c_double)]
 
 
 _lib = None

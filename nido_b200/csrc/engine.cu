@@ -639,6 +639,51 @@ extern "C" int nido_tune(nido_graph g, int32_t tie_mode, int32_t sweeps, nido_ti
   return NIDO_OK;
 }
 
+namespace {
+// Device time of a section that runs many times per run (modularity,
+// aggregation): event pairs in two slots, each pair read back once a later
+// stream synchronisation has certainly passed it, so timing adds no wait.
+struct SectionTimer {
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  bool pending[2] = {false, false};
+  int slot = 0;
+  double ms = 0.;
+  int init() {
+    for (cudaEvent_t& e : ev) NIDO_CUDA_TRY(cudaEventCreate(&e));
+    return NIDO_OK;
+  }
+  ~SectionTimer() {
+    for (cudaEvent_t e : ev)
+      if (e) cudaEventDestroy(e);
+  }
+  int begin(cudaStream_t s) {
+    if (pending[slot]) NIDO_TRY(harvest(slot));
+    NIDO_CUDA_TRY(cudaEventRecord(ev[2 * slot], s));
+    return NIDO_OK;
+  }
+  int end(cudaStream_t s) {
+    NIDO_CUDA_TRY(cudaEventRecord(ev[2 * slot + 1], s));
+    pending[slot] = true;
+    slot ^= 1;
+    return NIDO_OK;
+  }
+  // after a synchronisation of the stream: read the other slot's pair
+  int synced() { return pending[slot] ? harvest(slot) : NIDO_OK; }
+  int harvest(int i) {
+    float t = 0.f;
+    NIDO_CUDA_TRY(cudaEventElapsedTime(&t, ev[2 * i], ev[2 * i + 1]));
+    ms += t;
+    pending[i] = false;
+    return NIDO_OK;
+  }
+  int finish() {  // the stream is idle
+    for (int i = 0; i < 2; ++i)
+      if (pending[i]) NIDO_TRY(harvest(i));
+    return NIDO_OK;
+  }
+};
+}  // namespace
+
 // LouvainGPU::run (louvain_gpu.cpp:28-124): phases of singleton start,
 // iterations of batched moves until dQ <= tau or max_iter, undo of an
 // iteration that lowered Q, and aggregation when the phase gained more
@@ -658,6 +703,16 @@ extern "C" int nido_run(nido_graph g, const nido_params* p, int64_t* out_comm, n
   NIDO_CUDA_TRY(cudaEventCreate(&t1));
   auto now_ms = [] {
     return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
+  };
+  SectionTimer qt, at;  // modularity and aggregation device time
+  NIDO_TRY(qt.init());
+  NIDO_TRY(at.init());
+  auto modularity = [&](double* q) -> int {
+    NIDO_TRY(qt.begin(s));
+    NIDO_TRY(nido::launch_modularity(g, q));  // ends with a stream synchronisation
+    NIDO_TRY(qt.end(s));
+    NIDO_TRY(qt.synced());
+    return at.synced();
   };
   const uint64_t launches0 = nido_launch_count();
   double tm = now_ms();
@@ -682,7 +737,7 @@ extern "C" int nido_run(nido_graph g, const nido_params* p, int64_t* out_comm, n
     }
     NIDO_TRY(nido::launch_singleton(g));
     double Q;
-    NIDO_TRY(nido::launch_modularity(g, &Q));
+    NIDO_TRY(modularity(&Q));
     lap(2);
     const double Q_old = Q;
     if (p->verbose) printf("LOOP# \tQ \t\tdQ\n----------------------------------------\n0 \t%g \t0\n", Q);
@@ -704,7 +759,7 @@ extern "C" int nido_run(nido_graph g, const nido_params* p, int64_t* out_comm, n
       st.move_bytes += 16.0 * (double)g->ne + 32.0 * (double)g->nv;
       lap(1);
       double Qtmp;
-      NIDO_TRY(nido::launch_modularity(g, &Qtmp));
+      NIDO_TRY(modularity(&Qtmp));
       lap(2);
       dQ = Qtmp - Q;
       ++loops;
@@ -732,7 +787,9 @@ extern "C" int nido_run(nido_graph g, const nido_params* p, int64_t* out_comm, n
     if (Q - Q_old > tau) {
       int d = 0;
       lap(1);
+      NIDO_TRY(at.begin(s));
       NIDO_TRY(nido::launch_aggregation(g, &d));
+      NIDO_TRY(at.end(s));
       lap(3);
       done = d != 0;
       if (!done) NIDO_TRY(prepare_phase(g));
@@ -751,6 +808,10 @@ extern "C" int nido_run(nido_graph g, const nido_params* p, int64_t* out_comm, n
   cudaEventDestroy(t1);
   st.total_ms = tot;
   st.phases = phases;
+  NIDO_TRY(qt.finish());
+  NIDO_TRY(at.finish());
+  st.q_ms = qt.ms;
+  st.agg_ms = at.ms;
   int64_t nerr = 0;
   NIDO_CUDA_TRY(cudaMemcpyAsync(&nerr, g->dcount + 1, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
   NIDO_CUDA_TRY(cudaStreamSynchronize(s));
