@@ -15,9 +15,11 @@
 //    concatenated list (compress_edges, graph_gpu.cpp:1224-1304).
 //    Coarse vertices with at most 256 member edges are handled by one warp
 //    that walks the list in order and folds each weight onto its entry in
-//    edge order, which is the reference's summation order.  Larger ones use a
-//    CTA with atomic first-position tracking and an ordered second pass; their
-//    weight sums are exact for integer weights.
+//    edge order, which is the reference's summation order.  Up to 4096 use a
+//    CTA (256 threads up to 1024) with atomic first-position tracking and an
+//    ordered second pass over the slots recorded in the first; larger ones
+//    are cut into segments on many CTAs.  Weight sums beyond the warp tier are
+//    exact for integer weights.
 #include <limits.h>
 
 #include <algorithm>
@@ -30,8 +32,14 @@ namespace nido {
 namespace {
 
 constexpr int kAggWarpMaxD = 256;   // member edges handled by one warp
-constexpr int kAggCtaMaxCap = 8192; // shared-memory table slots of the CTA tier
-constexpr int kAggThreads = 512;
+// CTA tiers: threads, shared-memory table slots and list positions (member
+// edges) of one coarse vertex; a table holds at least twice the positions
+constexpr int kAggSThreads = 256;
+constexpr int kAggSCap = 2048;
+constexpr int kAggSMaxD = 1024;
+constexpr int kAggLThreads = 512;
+constexpr int kAggLCap = 8192;
+constexpr int kAggLMaxD = 4096;
 
 struct AggArgs {
   const int64_t* __restrict__ off;
@@ -48,6 +56,18 @@ struct AggArgs {
   unsigned long long* err;              // probe-limit failures (never expected)
   const int32_t* __restrict__ pm32;     // member holding position 32*b, for every b
 };
+
+// CTAs of a kernel resident on the whole GPU at once (at least one per SM)
+template <typename K>
+int agg_resident(K kernel, int threads, size_t smem) {
+  int per_sm = 0, dev = 0, sms = kSMs;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, smem) != cudaSuccess ||
+      cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) {
+    cudaGetLastError();
+    per_sm = 1;
+  }
+  return std::max(per_sm, 1) * sms;
+}
 
 inline unsigned grid_for(int64_t work, int per_block, int max_blocks) {
   int64_t b = (work + per_block - 1) / per_block;
@@ -116,16 +136,15 @@ __global__ void k_agg_tiers(const int64_t* __restrict__ mo, const int64_t* __res
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   for (int64_t base = blockIdx.x * (int64_t)blockDim.x; base < nvp; base += stride) {
     const int64_t c = base + threadIdx.x;
-    uint32_t t = 3u;
+    uint32_t t = 4u;
     if (c < nvp) {
       const int64_t D = medge[mo[c + 1]] - medge[mo[c]];
-      const int64_t U = D < nvp ? D : nvp;
-      t = D <= kAggWarpMaxD ? 0u : (2 * U <= kAggCtaMaxCap ? 1u : 2u);
+      t = D <= kAggWarpMaxD ? 0u : (D <= kAggSMaxD ? 1u : (D <= kAggLMaxD ? 2u : 3u));
       keys[c] = t;
       vals[c] = (uint32_t)c;
     }
     const unsigned peers = __match_any_sync(NIDO_FULL_MASK, t);
-    if (t < 3u && lane == __ffs(peers) - 1) atomicAdd((unsigned long long*)&counts[t], (unsigned long long)__popc(peers));
+    if (t < 4u && lane == __ffs(peers) - 1) atomicAdd((unsigned long long*)&counts[t], (unsigned long long)__popc(peers));
   }
 }
 
@@ -274,44 +293,36 @@ __global__ void __launch_bounds__(256) k_agg_warp(const int32_t* __restrict__ li
   }
 }
 
-// CTA tier: one CTA per coarse vertex; pass 1 merges with atomics and keeps
-// the first list position of every new id, pass 2 walks the list in order and
-// emits each id at its first position.
-template <bool kGlobal>
-__global__ void __launch_bounds__(kAggThreads) k_agg_cta(const int32_t* __restrict__ list, int64_t n, AggArgs q,
-                                                         int capmax, int32_t* gkeys, double* gvals,
-                                                         int32_t* gfpos, int64_t gslab) {
+// CTA tiers: one CTA per coarse vertex of at most kMaxD list positions.
+// Pass 1 merges with atomics, keeps the first list position of every new id
+// and records the slot of every position in shared memory; pass 2 walks the
+// positions in order from those slots (no second walk through members,
+// offsets and the new-id gather) and emits each id at its first position.
+template <int kThreads, int kCap, int kMaxD>
+__global__ void __launch_bounds__(kThreads) k_agg_cta(const int32_t* __restrict__ list, int64_t n, AggArgs q) {
   extern __shared__ double smem[];
-  __shared__ int wsum[2][kAggThreads / 32];
-  int *keys, *fpos;
-  double* vals;
-  if (kGlobal) {
-    keys = gkeys + (size_t)blockIdx.x * gslab;
-    fpos = gfpos + (size_t)blockIdx.x * gslab;
-    vals = gvals + (size_t)blockIdx.x * gslab;
-  } else {
-    vals = smem;
-    keys = reinterpret_cast<int*>(smem + capmax);
-    fpos = keys + capmax;
-    for (int i = threadIdx.x; i < capmax; i += blockDim.x) { keys[i] = -1; vals[i] = 0.; fpos[i] = INT_MAX; }
-    __syncthreads();
-  }
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+  __shared__ int wsum[2][kThreads / 32];
+  double* vals = smem;
+  int* keys = reinterpret_cast<int*>(smem + kCap);
+  int* fpos = keys + kCap;
+  int* hpos = fpos + kCap;
+  for (int i = threadIdx.x; i < kCap; i += kThreads) { keys[i] = -1; vals[i] = 0.; fpos[i] = INT_MAX; }
+  __syncthreads();
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   for (int64_t task = blockIdx.x; task < n; task += gridDim.x) {
     const int cp = list[task];
     const int64_t m0 = q.mo[cp], m1 = q.mo[cp + 1];
     const int64_t P0 = q.medge[m0], P1 = q.medge[m1];
-    unsigned cap = cap_for(P1 - P0, q.nvp);
-    if (!kGlobal) cap = min(cap, (unsigned)capmax);
-    const unsigned mask = cap - 1;
-    for (int64_t base = P0 + (int64_t)wid * 32; base < P1; base += blockDim.x) {
+    const unsigned cap = min(cap_for(P1 - P0, q.nvp), (unsigned)kCap), mask = cap - 1;
+    for (int64_t base = P0 + (int64_t)wid * 32; base < P1; base += kThreads) {
       const int64_t P = base + lane;
       const bool ok = P < P1;
       int X = -1;
       double wt = 0.;
       if (ok) load_pos(q, m0, m1, P, X, wt);
       const unsigned peers = __match_any_sync(NIDO_FULL_MASK, X);
-      const bool lead = ok && lane == __ffs(peers) - 1;
+      const int leader = __ffs(peers) - 1;
+      const bool lead = ok && lane == leader;
       double e = 0.;
       {
         unsigned rem = ok ? peers : 0u;
@@ -322,9 +333,10 @@ __global__ void __launch_bounds__(kAggThreads) k_agg_cta(const int32_t* __restri
           if (rem) { e += x; rem &= rem - 1; }
         }
       }
+      int h = -1;
       if (lead) {
         bool isnew;
-        const int h = find_or_insert(keys, mask, X, &isnew);
+        h = find_or_insert(keys, mask, X, &isnew);
         if (h >= 0) {
           atomicAdd(&vals[h], e);
           atomicMin(&fpos[h], (int)(P - P0));
@@ -332,44 +344,44 @@ __global__ void __launch_bounds__(kAggThreads) k_agg_cta(const int32_t* __restri
           atomicAdd(q.err, 1ull);
         }
       }
+      h = __shfl_sync(NIDO_FULL_MASK, h, leader);
+      if (ok) hpos[P - P0] = h;
     }
-    // emit in list order: per 256 positions one barrier, the warps' counts
-    // double-buffered, every thread carrying the running total
+    // emit in list order: per kThreads positions one barrier, the warps'
+    // counts double-buffered, every thread carrying the running total
     __syncthreads();
     int running = 0, par = 0;
-    for (int64_t base = P0; base < P1; base += blockDim.x, par ^= 1) {
-      const int64_t P = base + threadIdx.x;
-      const bool ok = P < P1;
-      int X = -1;
-      double wt = 0.;
-      int h = -1;
-      bool first = false;
-      if (ok) {
-        load_pos(q, m0, m1, P, X, wt);
-        h = find_slot(keys, mask, X);
-        first = h >= 0 && fpos[h] == (int)(P - P0);
-      }
+    for (int64_t base = 0; base < P1 - P0; base += kThreads, par ^= 1) {
+      const int i = (int)base + threadIdx.x;
+      const int h = i < P1 - P0 ? hpos[i] : -1;
+      const bool first = h >= 0 && fpos[h] == i;
       const unsigned bal = __ballot_sync(NIDO_FULL_MASK, first);
       if (lane == 0) wsum[par][wid] = __popc(bal);
       __syncthreads();
       int pre = running, tot = 0;
-      for (int i = 0; i < nwarp; ++i) {
-        const int c = wsum[par][i];
-        if (i < wid) pre += c;
+#pragma unroll
+      for (int k = 0; k < kThreads / 32; ++k) {
+        const int c = wsum[par][k];
+        if (k < wid) pre += c;
         tot += c;
       }
       running += tot;
       if (first) {
         const int idx = pre + __popc(bal & lanemask_lt());
-        q.tadj[P0 + idx] = X;
+        q.tadj[P0 + idx] = keys[h];
         q.tw[P0 + idx] = vals[h];
       }
     }
     if (threadIdx.x == 0) q.degp[cp] = running;
     __syncthreads();  // every warp is done reading the table before it is cleared
-    for (unsigned i = threadIdx.x; i < cap; i += blockDim.x) { keys[i] = -1; vals[i] = 0.; fpos[i] = INT_MAX; }
+    for (unsigned i = threadIdx.x; i < cap; i += kThreads) { keys[i] = -1; vals[i] = 0.; fpos[i] = INT_MAX; }
     __syncthreads();
   }
+}
+
+template <int kThreads, int kCap, int kMaxD>
+constexpr size_t agg_cta_smem() {
+  return (size_t)kCap * (sizeof(double) + 2 * sizeof(int)) + (size_t)kMaxD * sizeof(int);
 }
 
 // ---- giant coarse vertices: kAggSeg-position segments on many CTAs ----------
@@ -446,56 +458,73 @@ __global__ void __launch_bounds__(256) k_agg_seg_insert(int64_t it0, int64_t n, 
   }
 }
 
-// count (kEmit false) or emit (kEmit true) first occurrences of a segment
-template <bool kEmit>
-__global__ void __launch_bounds__(256) k_agg_seg_scan(int64_t it0, int64_t n, AggArgs q, SegArgs a,
-                                                      int64_t* segcnt) {
-  __shared__ int wsum[2][8];
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-  for (int64_t it = it0 + blockIdx.x; it < it0 + n; it += gridDim.x) {
-    const int2 item = a.items[it];
-    int cp;
-    int64_t m0, m1, P0, s0, s1;
-    seg_range(q, a, item, cp, m0, m1, P0, s0, s1);
-    const int* keys = a.keys + a.toff[item.x];
-    const double* vals = a.vals + a.toff[item.x];
-    const int* fpos = a.fpos + a.toff[item.x];
-    const unsigned mask = (unsigned)a.caps[item.x] - 1;
-    const int64_t base_out = kEmit ? segcnt[it] - segcnt[a.first[item.x]] : 0;
-    // one barrier per 256 positions (counts double-buffered, as in k_agg_cta)
-    __syncthreads();
-    int64_t running = 0;
-    int par = 0;
-    for (int64_t base = s0; base < s1; base += blockDim.x, par ^= 1) {
-      const int64_t P = base + threadIdx.x;
-      int X = -1;
-      double wt = 0.;
-      int h = -1;
-      bool firstocc = false;
-      if (P < s1) {
-        load_pos(q, m0, m1, P, X, wt);
-        h = find_slot(keys, mask, X);
-        firstocc = h >= 0 && fpos[h] == (int)(P - P0);
-      }
-      const unsigned bal = __ballot_sync(NIDO_FULL_MASK, firstocc);
-      if (lane == 0) wsum[par][wid] = __popc(bal);
-      __syncthreads();
-      int64_t pre = running;
-      int tot = 0;
-      for (int i = 0; i < (int)(blockDim.x >> 5); ++i) {
-        const int c = wsum[par][i];
-        if (i < wid) pre += c;
-        tot += c;
-      }
-      running += tot;
-      if (kEmit && firstocc) {
-        const int64_t idx = base_out + pre + __popc(bal & lanemask_lt());
-        q.tadj[P0 + idx] = X;
-        q.tw[P0 + idx] = vals[h];
-      }
+// Giants of a wave hold the table slots [toff[i], toff[i] + caps[i]) of the
+// wave's region, in giant order: the giant holding slot h.
+__device__ __forceinline__ int64_t giant_of_slot(const int64_t* __restrict__ toff, int64_t g0, int64_t g1,
+                                                 int64_t h) {
+  int64_t lo = g0, hi = g1;
+  while (hi - lo > 1) {
+    const int64_t mid = lo + (hi - lo) / 2;
+    if (toff[mid] <= h) lo = mid; else hi = mid;
+  }
+  return lo;
+}
+
+constexpr int kSegWords = kAggSeg / 32;  // bitmap words of one segment item
+
+// After the inserts of a wave: every occupied slot sets the bit of its id's
+// first list position in the bitmap of the segment item holding it.
+__global__ void k_agg_mark(int64_t g0, int64_t g1, int64_t ws, int64_t i0, SegArgs a, uint32_t* __restrict__ bm) {
+  for (int64_t h = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; h < ws; h += (int64_t)gridDim.x * blockDim.x) {
+    if (a.keys[h] < 0) continue;
+    const int64_t i = giant_of_slot(a.toff, g0, g1, h);
+    const int f = a.fpos[h];
+    const int64_t li = a.first[i] + f / kAggSeg - i0;
+    const int b = f % kAggSeg;
+    atomicOr(&bm[li * kSegWords + (b >> 5)], 1u << (b & 31));
+  }
+}
+
+// Per segment item of a wave (one warp each): its count of first
+// occurrences and the exclusive prefix count of every bitmap word.
+__global__ void k_agg_seg_count(int64_t i0, int64_t n, const uint32_t* __restrict__ bm, int32_t* __restrict__ wpre,
+                                int64_t* __restrict__ segcnt) {
+  static_assert(kSegWords == 128, "four bitmap words per lane");
+  const int lane = threadIdx.x & 31;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t li = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; li < n; li += nw) {
+    const uint4 w4 = reinterpret_cast<const uint4*>(bm + li * kSegWords)[lane];
+    const int c0 = __popc(w4.x), c1 = __popc(w4.y), c2 = __popc(w4.z), c3 = __popc(w4.w);
+    const int tot = c0 + c1 + c2 + c3;
+    int inc = tot;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(NIDO_FULL_MASK, inc, o);
+      if (lane >= o) inc += y;
     }
-    if (!kEmit && threadIdx.x == 0) segcnt[it] = running;
-    __syncthreads();
+    const int ex = inc - tot;
+    reinterpret_cast<int4*>(wpre + li * kSegWords)[lane] = make_int4(ex, ex + c0, ex + c0 + c1, ex + c0 + c1 + c2);
+    if (lane == 31) segcnt[i0 + li] = inc;
+  }
+}
+
+// After the scan of the wave's counts: every occupied slot writes its id and
+// summed weight at its rank among the first occurrences of its giant's list.
+__global__ void k_agg_emit(int64_t g0, int64_t g1, int64_t ws, int64_t i0, AggArgs q, SegArgs a,
+                           const uint32_t* __restrict__ bm, const int32_t* __restrict__ wpre,
+                           const int64_t* __restrict__ segcnt) {
+  for (int64_t h = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; h < ws; h += (int64_t)gridDim.x * blockDim.x) {
+    const int key = a.keys[h];
+    if (key < 0) continue;
+    const int64_t i = giant_of_slot(a.toff, g0, g1, h);
+    const int f = a.fpos[h];
+    const int64_t it = a.first[i] + f / kAggSeg, li = it - i0;
+    const int b = f % kAggSeg, w = b >> 5;
+    const int64_t idx = (segcnt[it] - segcnt[a.first[i]]) + wpre[li * kSegWords + w] +
+                        __popc(bm[li * kSegWords + w] & ((1u << (b & 31)) - 1u));
+    const int64_t P0 = q.medge[q.mo[a.cids[i]]];
+    q.tadj[P0 + idx] = key;
+    q.tw[P0 + idx] = a.vals[h];
   }
 }
 
@@ -610,19 +639,27 @@ int launch_aggregation(nido_graph_s* g, int* done) {
     NIDO_LAUNCH_CHECK();
   }
   if (cnt[1] > 0) {
-    const int capmax = kAggCtaMaxCap;
-    const size_t sm = (size_t)capmax * (sizeof(double) + 2 * sizeof(int));
-    NIDO_CUDA_TRY(cudaFuncSetAttribute(k_agg_cta<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    k_agg_cta<false><<<grid_for(cnt[1], 1, kSMs * 2), kAggThreads, sm, ctx->aux[1]>>>(
-        list + cnt[0], cnt[1], q, capmax, nullptr, nullptr, nullptr, 0);
+    constexpr size_t sm = agg_cta_smem<kAggSThreads, kAggSCap, kAggSMaxD>();
+    auto k = k_agg_cta<kAggSThreads, kAggSCap, kAggSMaxD>;
+    NIDO_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    k<<<grid_for(cnt[1], 1, agg_resident(k, kAggSThreads, sm)), kAggSThreads, sm, ctx->aux[1]>>>(list + cnt[0],
+                                                                                             cnt[1], q);
     NIDO_LAUNCH_CHECK();
   }
   if (cnt[2] > 0) {
+    constexpr size_t sm = agg_cta_smem<kAggLThreads, kAggLCap, kAggLMaxD>();
+    auto k = k_agg_cta<kAggLThreads, kAggLCap, kAggLMaxD>;
+    NIDO_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    k<<<grid_for(cnt[2], 1, agg_resident(k, kAggLThreads, sm)), kAggLThreads, sm, ctx->aux[0]>>>(
+        list + cnt[0] + cnt[1], cnt[2], q);
+    NIDO_LAUNCH_CHECK();
+  }
+  if (cnt[3] > 0) {
     // plan: per giant coarse vertex a table of >= 2*min(D, nvp) slots and
     // ceil(D / kAggSeg) segment items; giants go in waves whose tables share
     // one region of at most kAggWaveSlots slots (or one larger table)
-    const int64_t n2 = cnt[2];
-    const int32_t* list2 = list + cnt[0] + cnt[1];
+    const int64_t n2 = cnt[3];
+    const int32_t* list2 = list + cnt[0] + cnt[1] + cnt[2];
     int64_t* dsz = ar.take<int64_t>(n2);
     if (!dsz) return nido_set_error(NIDO_E_NOMEM, "scratch arena too small (aggregation plan)");
     k_agg_sizes<<<grid_for(n2, 256, kSMs * 4), 256, 0, s>>>(list2, n2, mo, medge, dsz);
@@ -654,9 +691,13 @@ int launch_aggregation(nido_graph_s* g, int* done) {
     wave_g.push_back(n2);
     first[n2] = (int64_t)items.size();
     const int64_t ni = (int64_t)items.size();
+    int64_t wave_items = 0;  // most segment items in one wave
+    for (size_t wv = 0; wv + 1 < wave_g.size(); ++wv)
+      wave_items = std::max(wave_items, first[wave_g[wv + 1]] - first[wave_g[wv]]);
     const size_t bytes = sizeof(int2) * ni + sizeof(int32_t) * 2 * n2 + sizeof(int64_t) * (2 * n2 + 1) +
                          sizeof(int64_t) * (ni + 1) + sizeof(int64_t) * scan_temp_elems(ni) +
-                         (sizeof(int32_t) * 2 + sizeof(double)) * slots + 16 * 256;
+                         (sizeof(int32_t) * 2 + sizeof(double)) * slots +
+                         2 * sizeof(uint32_t) * kSegWords * wave_items + 16 * 256;
     if (bytes > g->agg_buf_bytes) {
       NIDO_CUDA_TRY(cudaStreamSynchronize(s));
       raw_free(g->ctx, g->agg_buf);
@@ -677,6 +718,8 @@ int launch_aggregation(nido_graph_s* g, int* done) {
     int32_t* tkeys = pa.take<int32_t>(slots);
     int32_t* tfpos = pa.take<int32_t>(slots);
     double* tvals = pa.take<double>(slots);
+    uint32_t* bm = pa.take<uint32_t>(kSegWords * wave_items);
+    int32_t* wpre = pa.take<int32_t>(kSegWords * wave_items);
     NIDO_CUDA_TRY(cudaMemcpyAsync(ditems, items.data(), sizeof(int2) * ni, cudaMemcpyHostToDevice, s));
     NIDO_CUDA_TRY(cudaMemcpyAsync(dcids, cids.data(), sizeof(int32_t) * n2, cudaMemcpyHostToDevice, s));
     NIDO_CUDA_TRY(cudaMemcpyAsync(dcaps, caps.data(), sizeof(int32_t) * n2, cudaMemcpyHostToDevice, s));
@@ -690,15 +733,19 @@ int launch_aggregation(nido_graph_s* g, int* done) {
       NIDO_CUDA_TRY(cudaMemsetAsync(tkeys, 0xff, sizeof(int32_t) * ws, s));
       NIDO_CUDA_TRY(cudaMemsetAsync(tfpos, 0x7f, sizeof(int32_t) * ws, s));
       NIDO_CUDA_TRY(cudaMemsetAsync(tvals, 0, sizeof(double) * ws, s));
+      NIDO_CUDA_TRY(cudaMemsetAsync(bm, 0, sizeof(uint32_t) * kSegWords * nw, s));
       const unsigned gi = grid_for(nw, 1, kSMs * 8);
       k_agg_seg_insert<<<gi, 256, 0, s>>>(i0, nw, q, sa);
       NIDO_LAUNCH_CHECK();
-      k_agg_seg_scan<false><<<gi, 256, 0, s>>>(i0, nw, q, sa, segcnt);
+      const unsigned gs = grid_for(ws, 256, kSMs * 8);
+      k_agg_mark<<<gs, 256, 0, s>>>(g0, g1, ws, i0, sa, bm);
+      NIDO_LAUNCH_CHECK();
+      k_agg_seg_count<<<grid_for(nw * 32, 256, kSMs * 8), 256, 0, s>>>(i0, nw, bm, wpre, segcnt);
       NIDO_LAUNCH_CHECK();
       // within the wave: each giant's output offsets need only differences
       // of this scan (segcnt[i0 + nw] is overwritten by the next wave)
       NIDO_TRY(scan_exclusive_i64(segcnt + i0, segcnt + i0, nw, stemp, s));
-      k_agg_seg_scan<true><<<gi, 256, 0, s>>>(i0, nw, q, sa, segcnt);
+      k_agg_emit<<<gs, 256, 0, s>>>(g0, g1, ws, i0, q, sa, bm, wpre, segcnt);
       NIDO_LAUNCH_CHECK();
       k_agg_seg_deg<<<grid_for(g1 - g0, 256, kSMs * 4), 256, 0, s>>>(g1 - g0, dcids + g0, dfirst + g0, segcnt, degp);
       NIDO_LAUNCH_CHECK();

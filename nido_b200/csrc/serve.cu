@@ -132,6 +132,7 @@ extern "C" int64_t nido_graph_footprint(int64_t nv, int64_t ne, int32_t nbatches
   b += 12 * std::max<int64_t>((int64_t)8 << 20, 4 * V);
   b += 20 * std::max<int64_t>((int64_t)4 << 20, 4 * V) + 40 * V + E / 32;
   b += 4 * (E / 32 + 2);  // member index of the coarsening's 32-position blocks
+  b += E;  // first-position bitmaps and word prefixes of the giant segments
   b += (int64_t)32 << 20;
   return b;
 }
