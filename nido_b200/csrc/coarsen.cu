@@ -31,6 +31,9 @@
 namespace nido {
 namespace {
 
+// tiers by member-edge count D: groups of 4/8/16/32 lanes (D <= 4/8/16/32),
+// warp, CTA-S, CTA-L, giant
+constexpr unsigned kAggTiers = 8;
 constexpr int kAggWarpMaxD = 256;   // member edges handled by one warp
 // CTA tiers: threads, shared-memory table slots and list positions (member
 // edges) of one coarse vertex; a table holds at least twice the positions
@@ -136,15 +139,17 @@ __global__ void k_agg_tiers(const int64_t* __restrict__ mo, const int64_t* __res
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   for (int64_t base = blockIdx.x * (int64_t)blockDim.x; base < nvp; base += stride) {
     const int64_t c = base + threadIdx.x;
-    uint32_t t = 4u;
+    uint32_t t = kAggTiers;
     if (c < nvp) {
       const int64_t D = medge[mo[c + 1]] - medge[mo[c]];
-      t = D <= kAggWarpMaxD ? 0u : (D <= kAggSMaxD ? 1u : (D <= kAggLMaxD ? 2u : 3u));
+      t = D <= 4 ? 0u : D <= 8 ? 1u : D <= 16 ? 2u : D <= 32 ? 3u
+        : D <= kAggWarpMaxD ? 4u : D <= kAggSMaxD ? 5u : D <= kAggLMaxD ? 6u : 7u;
       keys[c] = t;
       vals[c] = (uint32_t)c;
     }
     const unsigned peers = __match_any_sync(NIDO_FULL_MASK, t);
-    if (t < 4u && lane == __ffs(peers) - 1) atomicAdd((unsigned long long*)&counts[t], (unsigned long long)__popc(peers));
+    if (t < kAggTiers && lane == __ffs(peers) - 1)
+      atomicAdd((unsigned long long*)&counts[t], (unsigned long long)__popc(peers));
   }
 }
 
@@ -194,15 +199,6 @@ __device__ __forceinline__ int find_or_insert(int* keys, unsigned mask, int X, b
   return -1;
 }
 
-__device__ __forceinline__ int find_slot(const int* keys, unsigned mask, int X) {
-  unsigned h = hash_slot(X, mask);
-  for (unsigned probe = 0; probe <= mask; ++probe) {
-    if (keys[h] == X) return (int)h;
-    h = (h + 1) & mask;
-  }
-  return -1;
-}
-
 __device__ __forceinline__ unsigned cap_for(int64_t D, int64_t nvp) {
   const int64_t U = D < nvp ? D : nvp;
   unsigned c = 64;
@@ -229,6 +225,55 @@ __device__ __forceinline__ void load_pos(const AggArgs& q, int64_t m0, int64_t m
   const int64_t e = q.off[v] + (P - q.medge[i]);
   X = q.newid[q.adj[e]];
   wt = q.w[e];
+}
+
+// D <= G: a group of G lanes per coarse vertex, one list position per lane.
+// Equal new ids are found with __match_any_sync (the group's index is part
+// of the key), their weights folded in lane (= list) order onto the first
+// lane, which is the reference's summation order, and the first lanes write
+// their ids in lane order: no table.
+template <int G>
+__global__ void __launch_bounds__(256) k_agg_group(const int32_t* __restrict__ list, int64_t n, AggArgs q) {
+  constexpr int VPW = 32 / G;
+  const int lane = threadIdx.x & 31, gl = lane & (G - 1), gid = lane / G;
+  const unsigned gmask = G == 32 ? NIDO_FULL_MASK : ((1u << G) - 1u) << (gid * G);
+  const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  for (int64_t b = warp * VPW; b < n; b += nw * VPW) {
+    const int64_t idx = b + gid;
+    int cp = 0;
+    int64_t m0 = 0, m1 = 0, P0 = 0, P1 = 0;
+    if (idx < n) {
+      cp = list[idx];
+      m0 = q.mo[cp];
+      m1 = q.mo[cp + 1];
+      P0 = q.medge[m0];
+      P1 = q.medge[m1];
+    }
+    const int64_t P = P0 + gl;
+    const bool ok = idx < n && P < P1;
+    int X = -1;
+    double wt = 0.;
+    if (ok) load_pos(q, m0, m1, P, X, wt);
+    const unsigned long long key = (unsigned long long)(unsigned)gid << 32 | (unsigned)X;
+    const unsigned peers = __match_any_sync(NIDO_FULL_MASK, key);
+    const bool lead = ok && lane == __ffs(peers) - 1;
+    double e = 0.;
+    unsigned rem = ok ? peers : 0u;
+    const int maxcnt = __reduce_max_sync(NIDO_FULL_MASK, (unsigned)__popc(rem));
+    for (int it = 0; it < maxcnt; ++it) {
+      const int src = rem ? __ffs(rem) - 1 : lane;
+      const double x = __shfl_sync(NIDO_FULL_MASK, wt, src);
+      if (rem) { e += x; rem &= rem - 1; }
+    }
+    const unsigned leaders = __ballot_sync(NIDO_FULL_MASK, lead) & gmask;
+    if (lead) {
+      const int o = __popc(leaders & lanemask_lt());
+      q.tadj[P0 + o] = X;
+      q.tw[P0 + o] = e;
+    }
+    if (gl == 0 && idx < n) q.degp[cp] = __popc(leaders);
+  }
 }
 
 // Warp tier: one warp per coarse vertex, table in shared memory.
@@ -569,7 +614,7 @@ int launch_aggregation(nido_graph_s* g, int* done) {
   int64_t* mo = ar.take<int64_t>(nv + 1);
   int64_t* medge = ar.take<int64_t>(nv + 1);
   int64_t* degp = ar.take<int64_t>(nv + 1);
-  int64_t* counts = ar.take<int64_t>(4);
+  int64_t* counts = ar.take<int64_t>(kAggTiers);
   int64_t* temp = ar.take<int64_t>(std::max(radix_temp_elems(nv), scan_temp_elems(nv + 1)));
   if (!temp) return nido_set_error(NIDO_E_NOMEM, "scratch arena too small (aggregation)");
   const unsigned gv = grid_for(nv, 256, kSMs * 16);
@@ -609,7 +654,7 @@ int launch_aggregation(nido_graph_s* g, int* done) {
     k_member_blocks<<<grid_for(nblk, 256, kSMs * 16), 256, 0, s>>>(medge, nv, g->pm32);
     NIDO_LAUNCH_CHECK();
   }
-  NIDO_CUDA_TRY(cudaMemsetAsync(counts, 0, sizeof(int64_t) * 4, s));
+  NIDO_CUDA_TRY(cudaMemsetAsync(counts, 0, sizeof(int64_t) * kAggTiers, s));
   // coarse-vertex tiers (rk2/rv2 are free after the member sort)
   uint32_t* tk = rk2;
   uint32_t* tv = rv2;
@@ -617,49 +662,57 @@ int launch_aggregation(nido_graph_s* g, int* done) {
   uint32_t* tv2 = reinterpret_cast<uint32_t*>(degp);  // degp is written only after the tier sort
   k_agg_tiers<<<grid_for(nvp, 256, kSMs * 16), 256, 0, s>>>(mo, medge, nvp, tk, tv, counts);
   NIDO_LAUNCH_CHECK();
-  NIDO_TRY(radix_sort_pairs(tk, tv, tk2, tv2, nvp, 2, temp, s));
-  int64_t cnt[4] = {0, 0, 0, 0};
+  NIDO_TRY(radix_sort_pairs(tk, tv, tk2, tv2, nvp, 3, temp, s));
+  int64_t cnt[kAggTiers] = {0, 0, 0, 0, 0, 0, 0, 0};
   NIDO_CUDA_TRY(cudaMemcpyAsync(cnt, counts, sizeof(cnt), cudaMemcpyDeviceToHost, s));
   NIDO_CUDA_TRY(cudaStreamSynchronize(s));
+  int64_t at[kAggTiers + 1] = {0};  // first list entry of every tier
+  for (unsigned t = 0; t < kAggTiers; ++t) at[t + 1] = at[t] + cnt[t];
 
   AggArgs q{g->off, g->adj, g->w, newid, rv, mo, medge, g->adj2, g->w2, degp, nvp,
             reinterpret_cast<unsigned long long*>(g->dcount + 1), g->pm32};
   const int32_t* list = reinterpret_cast<const int32_t*>(tv);
-  // the three tiers write disjoint coarse vertices: the warp and CTA tiers
-  // run on the context's side streams while the giant path (which plans on
-  // the host) runs on its stream; all join before the offsets are scanned
+  // the tiers write disjoint coarse vertices: the lane-group and warp tiers
+  // run on one side stream, the CTA tiers on the other, while the giant path
+  // (which plans on the host) runs on the context's stream; all join before
+  // the offsets are scanned
   nido_ctx_s* ctx = g->ctx;
   NIDO_CUDA_TRY(cudaEventRecord(ctx->fork_ev, s));
   for (int i = 0; i < 2; ++i) NIDO_CUDA_TRY(cudaStreamWaitEvent(ctx->aux[i], ctx->fork_ev, 0));
-  if (cnt[0] > 0) {
+  if (cnt[0] > 0) k_agg_group<4><<<grid_for(cnt[0], 64, kSMs * 16), 256, 0, ctx->aux[0]>>>(list + at[0], cnt[0], q);
+  if (cnt[1] > 0) k_agg_group<8><<<grid_for(cnt[1], 32, kSMs * 16), 256, 0, ctx->aux[0]>>>(list + at[1], cnt[1], q);
+  if (cnt[2] > 0) k_agg_group<16><<<grid_for(cnt[2], 16, kSMs * 16), 256, 0, ctx->aux[0]>>>(list + at[2], cnt[2], q);
+  if (cnt[3] > 0) k_agg_group<32><<<grid_for(cnt[3], 8, kSMs * 16), 256, 0, ctx->aux[0]>>>(list + at[3], cnt[3], q);
+  NIDO_LAUNCH_CHECK();
+  if (cnt[4] > 0) {
     const int capmax = 2 * kAggWarpMaxD;
     const size_t sm = (size_t)8 * capmax * (sizeof(double) + 2 * sizeof(int));
     NIDO_CUDA_TRY(cudaFuncSetAttribute(k_agg_warp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    k_agg_warp<<<grid_for(cnt[0], 8, kSMs * 8), 256, sm, ctx->aux[0]>>>(list, cnt[0], q, capmax);
+    k_agg_warp<<<grid_for(cnt[4], 8, kSMs * 8), 256, sm, ctx->aux[0]>>>(list + at[4], cnt[4], q, capmax);
     NIDO_LAUNCH_CHECK();
   }
-  if (cnt[1] > 0) {
+  if (cnt[5] > 0) {
     constexpr size_t sm = agg_cta_smem<kAggSThreads, kAggSCap, kAggSMaxD>();
     auto k = k_agg_cta<kAggSThreads, kAggSCap, kAggSMaxD>;
     NIDO_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    k<<<grid_for(cnt[1], 1, agg_resident(k, kAggSThreads, sm)), kAggSThreads, sm, ctx->aux[1]>>>(list + cnt[0],
-                                                                                             cnt[1], q);
+    k<<<grid_for(cnt[5], 1, agg_resident(k, kAggSThreads, sm)), kAggSThreads, sm, ctx->aux[1]>>>(list + at[5],
+                                                                                             cnt[5], q);
     NIDO_LAUNCH_CHECK();
   }
-  if (cnt[2] > 0) {
+  if (cnt[6] > 0) {
     constexpr size_t sm = agg_cta_smem<kAggLThreads, kAggLCap, kAggLMaxD>();
     auto k = k_agg_cta<kAggLThreads, kAggLCap, kAggLMaxD>;
     NIDO_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    k<<<grid_for(cnt[2], 1, agg_resident(k, kAggLThreads, sm)), kAggLThreads, sm, ctx->aux[0]>>>(
-        list + cnt[0] + cnt[1], cnt[2], q);
+    k<<<grid_for(cnt[6], 1, agg_resident(k, kAggLThreads, sm)), kAggLThreads, sm, ctx->aux[1]>>>(list + at[6],
+                                                                                             cnt[6], q);
     NIDO_LAUNCH_CHECK();
   }
-  if (cnt[3] > 0) {
+  if (cnt[7] > 0) {
     // plan: per giant coarse vertex a table of >= 2*min(D, nvp) slots and
     // ceil(D / kAggSeg) segment items; giants go in waves whose tables share
     // one region of at most kAggWaveSlots slots (or one larger table)
-    const int64_t n2 = cnt[3];
-    const int32_t* list2 = list + cnt[0] + cnt[1] + cnt[2];
+    const int64_t n2 = cnt[7];
+    const int32_t* list2 = list + at[7];
     int64_t* dsz = ar.take<int64_t>(n2);
     if (!dsz) return nido_set_error(NIDO_E_NOMEM, "scratch arena too small (aggregation plan)");
     k_agg_sizes<<<grid_for(n2, 256, kSMs * 4), 256, 0, s>>>(list2, n2, mo, medge, dsz);
