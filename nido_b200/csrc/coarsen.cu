@@ -580,18 +580,96 @@ __global__ void k_agg_seg_deg(int64_t nlist, const int32_t* __restrict__ cids, c
     degp[cids[i]] = segoff[first[i + 1]] - segoff[first[i]];
 }
 
-// copy each coarse vertex's entries to its final offset
+// Copy each coarse vertex's entries to its final offset.  A warp takes 32
+// consecutive coarse vertices and copies their entries as one run: each
+// lane finds its entry's vertex by a search over the lanes' prefix counts,
+// four entries in flight per lane.  Vertices of more than kCompactBig
+// entries are left out of the runs and listed for k_compact_big.
+constexpr int kCompactBig = 4096;
+
 __global__ void k_compact(int64_t nvp, const int64_t* __restrict__ mo, const int64_t* __restrict__ medge,
                           const int64_t* __restrict__ coff, const int32_t* __restrict__ tadj,
-                          const double* __restrict__ tw, int32_t* __restrict__ adj, double* __restrict__ w) {
+                          const double* __restrict__ tw, int32_t* __restrict__ adj, double* __restrict__ w,
+                          int32_t* __restrict__ big, unsigned long long* __restrict__ nbig) {
   const int lane = threadIdx.x & 31;
   const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-  for (int64_t c = warp; c < nvp; c += nw) {
-    const int64_t src = medge[mo[c]], dst = coff[c], len = coff[c + 1] - coff[c];
-    for (int64_t i = lane; i < len; i += 32) {
-      adj[dst + i] = tadj[src + i];
-      w[dst + i] = tw[src + i];
+  for (int64_t c0 = warp * 32; c0 < nvp; c0 += nw * 32) {
+    const int64_t c = c0 + lane;
+    int64_t src = 0, dst = 0, len = 0;
+    if (c < nvp) {
+      dst = coff[c];
+      len = coff[c + 1] - dst;
+      src = medge[mo[c]];
+      if (len > kCompactBig) {
+        big[atomicAdd(nbig, 1ull)] = (int32_t)c;
+        len = 0;
+      }
+    }
+    int64_t inc = len;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int64_t y = __shfl_up_sync(NIDO_FULL_MASK, inc, o);
+      if (lane >= o) inc += y;
+    }
+    const int64_t pre = inc - len;
+    const int64_t T = __shfl_sync(NIDO_FULL_MASK, inc, 31);
+    for (int64_t b = 0; b < T; b += 4 * 32) {
+      int64_t sp[4], dp[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int64_t i = b + u * 32 + lane;
+        int k = 0;  // the last lane whose run starts at or before i
+#pragma unroll
+        for (int step = 16; step >= 1; step >>= 1) {
+          const int64_t pk = __shfl_sync(NIDO_FULL_MASK, pre, k + step);
+          if (pk <= i) k += step;
+        }
+        const int64_t pk = __shfl_sync(NIDO_FULL_MASK, pre, k);
+        const int64_t sk = __shfl_sync(NIDO_FULL_MASK, src, k);
+        const int64_t dk = __shfl_sync(NIDO_FULL_MASK, dst, k);
+        sp[u] = i < T ? sk + (i - pk) : -1;
+        dp[u] = dk + (i - pk);
+      }
+      int32_t a[4];
+      double x[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+        if (sp[u] >= 0) { a[u] = tadj[sp[u]]; x[u] = tw[sp[u]]; }
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+        if (sp[u] >= 0) { adj[dp[u]] = a[u]; w[dp[u]] = x[u]; }
+    }
+  }
+}
+
+// Entries of the listed large coarse vertices, one CTA per vertex, eight
+// entries in flight per thread.
+__global__ void __launch_bounds__(256) k_compact_big(const int32_t* __restrict__ big,
+                                                     const unsigned long long* __restrict__ nbig,
+                                                     const int64_t* __restrict__ mo,
+                                                     const int64_t* __restrict__ medge,
+                                                     const int64_t* __restrict__ coff,
+                                                     const int32_t* __restrict__ tadj,
+                                                     const double* __restrict__ tw, int32_t* __restrict__ adj,
+                                                     double* __restrict__ w) {
+  const int64_t n = (int64_t)*nbig;
+  for (int64_t t = blockIdx.x; t < n; t += gridDim.x) {
+    const int c = big[t];
+    const int64_t dst = coff[c], len = coff[c + 1] - dst, src = medge[mo[c]];
+    for (int64_t b = 0; b < len; b += 8 * 256) {
+      int32_t a[8];
+      double x[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const int64_t i = b + u * 256 + threadIdx.x;
+        if (i < len) { a[u] = tadj[src + i]; x[u] = tw[src + i]; }
+      }
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const int64_t i = b + u * 256 + threadIdx.x;
+        if (i < len) { adj[dst + i] = a[u]; w[dst + i] = x[u]; }
+      }
     }
   }
 }
@@ -812,8 +890,18 @@ int launch_aggregation(nido_graph_s* g, int* done) {
   // coarse offsets into off2, then the entries into the work CSR (when the
   // current graph is the work CSR, its lists are dead once pass 1 is done)
   NIDO_TRY(scan_exclusive_i64(degp, g->off2, nvp, temp, s));
-  k_compact<<<grid_for(nvp * 32, 256, kSMs * 16), 256, 0, s>>>(nvp, mo, medge, g->off2, g->adj2, g->w2, g->adjA, g->wA);
-  NIDO_LAUNCH_CHECK();
+  {
+    // large coarse vertices are listed in the member-key buffer (free once
+    // the member bounds are known), their count in the tier counters (read)
+    int32_t* big = reinterpret_cast<int32_t*>(rk);
+    unsigned long long* nbig = reinterpret_cast<unsigned long long*>(counts);
+    NIDO_CUDA_TRY(cudaMemsetAsync(nbig, 0, sizeof(unsigned long long), s));
+    k_compact<<<grid_for(nvp, 256, kSMs * 16), 256, 0, s>>>(nvp, mo, medge, g->off2, g->adj2, g->w2, g->adjA,
+                                                             g->wA, big, nbig);
+    NIDO_LAUNCH_CHECK();
+    k_compact_big<<<kSMs * 2, 256, 0, s>>>(big, nbig, mo, medge, g->off2, g->adj2, g->w2, g->adjA, g->wA);
+    NIDO_LAUNCH_CHECK();
+  }
   int64_t nep = 0, nerr = 0;
   NIDO_CUDA_TRY(cudaMemcpyAsync(&nep, g->off2 + nvp, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
   NIDO_CUDA_TRY(cudaMemcpyAsync(&nerr, g->dcount + 1, sizeof(int64_t), cudaMemcpyDeviceToHost, s));

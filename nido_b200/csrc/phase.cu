@@ -121,30 +121,28 @@ __global__ void k_commit(int64_t v0, int64_t v1, const double* __restrict__ k,
 
 // ---- modularity -------------------------------------------------------------------
 // Sum of w[j] over j = j0, j0+step, ... < e with comm[adj[j]] == own, added in
-// that order; four edges' loads are issued before any is added, so four
-// dependent gathers are in flight per lane.
+// that order; four edges' loads (bounds-guarded) are issued before any is
+// added, so four dependent gathers are in flight per lane at every degree.
 __device__ __forceinline__ double own_weight(const int32_t* __restrict__ adj, const double* __restrict__ w,
                                              const int32_t* __restrict__ comm, int32_t own, int64_t j0,
                                              int64_t e, int step) {
   double x = 0.;
-  int64_t j = j0;
-  for (; j + 3 * (int64_t)step < e; j += 4 * (int64_t)step) {
+  for (int64_t j = j0; j < e; j += 4 * (int64_t)step) {
     int u[4];
     double wt[4];
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
-      u[k] = adj[j + k * step];
-      wt[k] = w[j + k * step];
+      const int64_t jk = j + k * (int64_t)step;
+      u[k] = jk < e ? adj[jk] : -1;
+      wt[k] = jk < e ? w[jk] : 0.;
     }
     int c[4];
 #pragma unroll
-    for (int k = 0; k < 4; ++k) c[k] = comm[u[k]];
+    for (int k = 0; k < 4; ++k) c[k] = u[k] >= 0 ? comm[u[k]] : 0;
 #pragma unroll
     for (int k = 0; k < 4; ++k)
-      if (c[k] == own) x += wt[k];
+      if (u[k] >= 0 && c[k] == own) x += wt[k];
   }
-  for (; j < e; j += step)
-    if (comm[adj[j]] == own) x += w[j];
   return x;
 }
 
