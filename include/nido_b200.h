@@ -113,6 +113,16 @@ int nido_ctx_trim(nido_ctx ctx, size_t* released_bytes);
 int nido_graph_upload(nido_ctx ctx, int64_t nv, int64_t ne, const int64_t* off,
                       const int64_t* adj, const double* w, int32_t nbatches,
                       nido_graph* out);
+/* Read a Vite binary straight into device memory: the reference's Graph(file)
+ * (graph.cpp:322-495) followed by the GraphGPU upload, without the host CSR.
+ * Header and offsets are read on the host (offsets not starting at 0 are
+ * rebased; a header edge count that differs from the offsets prints the
+ * reference's warning); the 16-byte edge records stream through pinned
+ * buffers, read by parallel preads while the previous chunk is copied, and
+ * are split into ids and weights on the device.  Same checks and result as
+ * nido_read_vite + nido_graph_upload; NIDO_E_IO for a missing or truncated
+ * file. */
+int nido_graph_upload_vite(nido_ctx ctx, const char* path, int32_t nbatches, nido_graph* out);
 int nido_graph_free(nido_graph g);
 /* sizes of the current (possibly coarsened) graph */
 int nido_graph_size(nido_graph g, int64_t* nv, int64_t* ne);

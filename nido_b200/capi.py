@@ -85,6 +85,7 @@ def lib() -> C.CDLL:
             "nido_ctx_sync": (C.c_int, [vp]),
             "nido_ctx_stream": (C.c_int, [vp, C.POINTER(vp)]),
             "nido_ctx_trim": (C.c_int, [vp, C.POINTER(C.c_size_t)]),
+            "nido_graph_upload_vite": (C.c_int, [vp, C.c_char_p, C.c_int32, C.POINTER(vp)]),
             "nido_graph_upload": (C.c_int, [vp, C.c_int64, C.c_int64, _i64p, _i64p, _f64p, C.c_int32,
                                             C.POINTER(vp)]),
             "nido_graph_free": (C.c_int, [vp]),
@@ -297,6 +298,19 @@ class Graph:
         h = C.c_void_p()
         _check(lib().nido_graph_upload(ctx.h, s.nv, s.ne, s.off, s.adj, s.w, nbatches, C.byref(h)))
         self.h = h
+
+    @classmethod
+    def from_vite(cls, ctx: Context, path: str, nbatches: int = 2) -> "Graph":
+        """Stream a Vite binary file straight to the device
+        (nido_graph_upload_vite)."""
+        self = cls.__new__(cls)
+        self.ctx = ctx
+        self.nbatches = nbatches
+        h = C.c_void_p()
+        _check(lib().nido_graph_upload_vite(ctx.h, os.fsencode(path), nbatches, C.byref(h)))
+        self.h = h
+        self.nv0 = self.size()[0]
+        return self
 
     def close(self):
         if self.h:

@@ -1,9 +1,11 @@
 // engine.cu -- C ABI of the engine: contexts, graph upload, the step-level
 // operators of the reference's GraphGPU (graph_gpu.hpp:168-247) and the
 // whole-run driver LouvainGPU::run (louvain_gpu.cpp:6-139).
+#include <fcntl.h>
 #include <omp.h>
 #include <stdio.h>
 #include <string.h>
+#include <unistd.h>
 
 #include <algorithm>
 #include <chrono>
@@ -68,6 +70,19 @@ void raw_free(nido_ctx_s* ctx, void* p) {
   ctx->free_blocks.emplace(it->second, p);
   ctx->cached_bytes += it->second;
   ctx->live_blocks.erase(it);
+}
+
+cudaError_t pinned_buffer(nido_ctx_s* ctx, size_t bytes, void** p) {
+  if (bytes > ctx->pinned_bytes) {
+    if (ctx->pinned) cudaFreeHost(ctx->pinned);
+    ctx->pinned = nullptr;
+    ctx->pinned_bytes = 0;
+    const cudaError_t e = cudaHostAlloc(&ctx->pinned, bytes, cudaHostAllocDefault);
+    if (e != cudaSuccess) return e;
+    ctx->pinned_bytes = bytes;
+  }
+  *p = ctx->pinned;
+  return cudaSuccess;
 }
 
 void release_cached(nido_ctx_s* ctx) {
@@ -219,6 +234,7 @@ extern "C" int nido_ctx_destroy(nido_ctx ctx) {
   }
   if (ctx->fork_ev) cudaEventDestroy(ctx->fork_ev);
   nido::release_cached(ctx);
+  if (ctx->pinned) cudaFreeHost(ctx->pinned);
   cudaStreamDestroy(ctx->stream);
   delete ctx;
   return NIDO_OK;
@@ -271,16 +287,15 @@ extern "C" int nido_graph_free(nido_graph g) {
   return NIDO_OK;
 }
 
-extern "C" int nido_graph_upload(nido_ctx ctx, int64_t nv, int64_t ne, const int64_t* off,
-                                 const int64_t* adj, const double* w, int32_t nbatches,
-                                 nido_graph* out) {
-  if (!ctx || !out || !off || (ne > 0 && (!adj || !w)))
-    return nido_set_error(NIDO_E_INVALID, "nido_graph_upload: null argument");
+namespace {
+// Every device array of a graph of nv vertices and ne edges; the caller
+// fills g->off, the int64 ids (in the w2 buffer, narrowed by graph_finish)
+// and g->w.
+int graph_create(nido_ctx ctx, int64_t nv, int64_t ne, int32_t nbatches, nido_graph* out) {
   *out = nullptr;
   if (nv < 0 || ne < 0) return nido_set_error(NIDO_E_INVALID, "negative graph size");
   if (nv >= ((int64_t)1 << 31) - 1) return nido_set_error(NIDO_E_TOO_LARGE, "%lld vertices exceed 2^31-1", (long long)nv);
   if (nbatches < 1) return nido_set_error(NIDO_E_INVALID, "nbatches must be >= 1 (got %d)", nbatches);
-  if (off[0] != 0 || off[nv] != ne) return nido_set_error(NIDO_E_INVALID, "offsets must run from 0 to ne");
   NIDO_CUDA_TRY(cudaSetDevice(ctx->device));
   nido_graph g = new (std::nothrow) nido_graph_s();
   if (!g) return nido_set_error(NIDO_E_NOMEM, "host allocation failed");
@@ -307,30 +322,155 @@ extern "C" int nido_graph_upload(nido_ctx ctx, int64_t nv, int64_t ne, const int
   g->off = g->off0;
   g->adj = g->adj0;
   g->w = g->w0;
-  cudaStream_t s = ctx->stream;
-  // int64 ids travel in the (not yet used) w2 buffer and are narrowed on device
-  int64_t* adj64 = reinterpret_cast<int64_t*>(g->w2);
-  NIDO_CUDA_TRY(cudaMemcpyAsync(g->off, off, 8 * (V + 1), cudaMemcpyHostToDevice, s));
-  if (E > 0) {
-    NIDO_CUDA_TRY(cudaMemcpyAsync(adj64, adj, 8 * E, cudaMemcpyHostToDevice, s));
-    NIDO_CUDA_TRY(cudaMemcpyAsync(g->w, w, 8 * E, cudaMemcpyHostToDevice, s));
-  }
+  *out = g;
+  return NIDO_OK;
+}
+
+// The int64 ids travel in the (not yet used) w2 buffer.
+int64_t* staged_ids(nido_graph g) { return reinterpret_cast<int64_t*>(g->w2); }
+
+// After the CSR is on the device: narrow and check the ids and offsets, then
+// k_v, m, the batches and the singleton partition of the first phase.
+int graph_finish(nido_graph g) {
+  cudaStream_t s = g->ctx->stream;
+  const int64_t V = g->nv, E = g->ne;
   unsigned long long* bad = reinterpret_cast<unsigned long long*>(g->dcount);
   NIDO_CUDA_TRY(cudaMemsetAsync(g->dcount, 0, 8 * sizeof(int64_t), s));
-  k_narrow<<<kGrid, 256, 0, s>>>(adj64, E, V, g->adj, g->off, bad);
+  k_narrow<<<kGrid, 256, 0, s>>>(staged_ids(g), E, V, g->adj, g->off, bad);
   NIDO_LAUNCH_CHECK();
   k_iota<<<kGrid, 256, 0, s>>>(g->clus, V);
   NIDO_LAUNCH_CHECK();
   unsigned long long nbad = 0;
   NIDO_CUDA_TRY(cudaMemcpyAsync(&nbad, bad, 8, cudaMemcpyDeviceToHost, s));
   NIDO_CUDA_TRY(cudaStreamSynchronize(s));
-  if (nbad) {
-    nido_graph_free(g);
-    return nido_set_error(NIDO_E_INVALID, "%llu neighbour ids out of range or decreasing offsets", nbad);
+  if (nbad) return nido_set_error(NIDO_E_INVALID, "%llu neighbour ids out of range or decreasing offsets", nbad);
+  NIDO_TRY(prepare_phase(g));
+  return nido::launch_singleton(g);
+}
+
+// Frees a graph whose construction failed (after its stream is idle) and
+// passes the status on.
+int fail_graph(nido_graph g, int st) {
+  cudaStreamSynchronize(g->ctx->stream);
+  nido_graph_free(g);
+  return st;
+}
+
+// Vite edge records {int64 tail; double weight} to ids and weights.
+__global__ void k_split_records(const longlong2* __restrict__ rec, int64_t n, int64_t* __restrict__ adj64,
+                                double* __restrict__ w) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const longlong2 r = rec[i];
+    adj64[i] = r.x;
+    w[i] = __longlong_as_double(r.y);
   }
-  st = prepare_phase(g);
-  if (st == NIDO_OK) st = nido::launch_singleton(g);
-  if (st != NIDO_OK) { nido_graph_free(g); return st; }
+}
+
+// Reads bytes [pos, pos + n) of fd into dst with `threads` concurrent
+// preads; false on a short file or a read error.
+bool pread_all(int fd, char* dst, int64_t n, int64_t pos, int threads) {
+  bool ok = true;
+  const int64_t per = (n + threads - 1) / threads;
+#pragma omp parallel for num_threads(threads) schedule(static) reduction(&& : ok)
+  for (int t = 0; t < threads; ++t) {
+    int64_t lo = (int64_t)t * per, hi = std::min(n, lo + per);
+    while (lo < hi) {
+      const ssize_t r = pread(fd, dst + lo, (size_t)(hi - lo), (off_t)(pos + lo));
+      if (r <= 0) { ok = false; break; }
+      lo += r;
+    }
+  }
+  return ok;
+}
+}  // namespace
+
+extern "C" int nido_graph_upload(nido_ctx ctx, int64_t nv, int64_t ne, const int64_t* off,
+                                 const int64_t* adj, const double* w, int32_t nbatches,
+                                 nido_graph* out) {
+  if (!ctx || !out || !off || (ne > 0 && (!adj || !w)))
+    return nido_set_error(NIDO_E_INVALID, "nido_graph_upload: null argument");
+  *out = nullptr;
+  if (nv >= 0 && ne >= 0 && nv < ((int64_t)1 << 31) - 1 && (off[0] != 0 || off[nv] != ne))
+    return nido_set_error(NIDO_E_INVALID, "offsets must run from 0 to ne");
+  nido_graph g = nullptr;
+  NIDO_TRY(graph_create(ctx, nv, ne, nbatches, &g));
+  cudaStream_t s = ctx->stream;
+  cudaError_t e = cudaMemcpyAsync(g->off, off, 8 * (nv + 1), cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess && ne > 0) e = cudaMemcpyAsync(staged_ids(g), adj, 8 * ne, cudaMemcpyHostToDevice, s);
+  if (e == cudaSuccess && ne > 0) e = cudaMemcpyAsync(g->w, w, 8 * ne, cudaMemcpyHostToDevice, s);
+  if (e != cudaSuccess) return fail_graph(g, nido_set_error(NIDO_E_CUDA, "upload: %s", cudaGetErrorString(e)));
+  const int st = graph_finish(g);
+  if (st != NIDO_OK) return fail_graph(g, st);
+  *out = g;
+  return NIDO_OK;
+}
+
+// Vite binary straight to the device (graph.cpp:322-495 for the format and
+// its checks): the header and offsets are read on the host; the edge records
+// stream through two pinned buffers, each filled by parallel preads while the
+// other is copied, and are split into ids and weights by a kernel.
+extern "C" int nido_graph_upload_vite(nido_ctx ctx, const char* path, int32_t nbatches, nido_graph* out) {
+  if (!ctx || !path || !out) return nido_set_error(NIDO_E_INVALID, "nido_graph_upload_vite: null argument");
+  *out = nullptr;
+  const int fd = open(path, O_RDONLY);
+  if (fd < 0) return nido_set_error(NIDO_E_IO, " Error opening file! (%s)", path);
+  struct FdGuard {
+    int fd;
+    ~FdGuard() { close(fd); }
+  } guard{fd};
+  int64_t hdr[2];
+  if (!pread_all(fd, reinterpret_cast<char*>(hdr), 16, 0, 1) || hdr[0] < 0)
+    return nido_set_error(NIDO_E_IO, "%s: truncated header", path);
+  const int64_t nv = hdr[0];
+  if (nv >= ((int64_t)1 << 31) - 1) return nido_set_error(NIDO_E_TOO_LARGE, "%lld vertices exceed 2^31-1", (long long)nv);
+  const int threads = std::max(1, std::min(16, omp_get_max_threads()));
+  std::vector<int64_t> off((size_t)nv + 1);
+  if (!pread_all(fd, reinterpret_cast<char*>(off.data()), 8 * (nv + 1), 16, threads))
+    return nido_set_error(NIDO_E_IO, "%s: truncated offsets", path);
+  const int64_t ne = off[nv] - off[0];
+  if (ne < 0) return nido_set_error(NIDO_E_IO, "%s: decreasing offsets", path);
+  if (ne != hdr[1]) {
+    printf("!!! The graph has been modified in edges\n");
+    printf("Original edges: %lld\nNew edges: %lld\n", (long long)hdr[1], (long long)ne);
+  }
+  const int64_t base = off[0];
+  for (int64_t& o : off) o -= base;
+  nido_graph g = nullptr;
+  NIDO_TRY(graph_create(ctx, nv, ne, nbatches, &g));
+  cudaStream_t s = ctx->stream;
+  const int64_t rec0 = 16 + 8 * (nv + 1);  // file position of the first record
+  const int64_t chunk = std::min<int64_t>(std::max<int64_t>(ne, 1), (int64_t)1 << 22);
+  int st = NIDO_OK;
+  cudaError_t e = cudaMemcpyAsync(g->off, off.data(), 8 * (nv + 1), cudaMemcpyHostToDevice, s);
+  char* host = nullptr;
+  longlong2* dev = nullptr;
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+  if (e == cudaSuccess) e = nido::pinned_buffer(ctx, (size_t)2 * 16 * chunk, reinterpret_cast<void**>(&host));
+  if (e == cudaSuccess) e = nido::raw_alloc(ctx, reinterpret_cast<void**>(&dev), (size_t)2 * 16 * chunk);
+  for (int b = 0; b < 2 && e == cudaSuccess; ++b) e = cudaEventCreateWithFlags(&ev[b], cudaEventDisableTiming);
+  for (int64_t done = 0, i = 0; e == cudaSuccess && st == NIDO_OK && done < ne; ++i) {
+    const int b = (int)(i & 1);
+    const int64_t n = std::min(chunk, ne - done);
+    if (i >= 2 && (e = cudaEventSynchronize(ev[b])) != cudaSuccess) break;  // buffer b is free again
+    char* hb = host + (size_t)b * 16 * chunk;
+    if (!pread_all(fd, hb, 16 * n, rec0 + 16 * done, threads)) {
+      st = nido_set_error(NIDO_E_IO, "%s: truncated edge records", path);
+      break;
+    }
+    e = cudaMemcpyAsync(dev + (size_t)b * chunk, hb, 16 * n, cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) break;
+    k_split_records<<<kGrid, 256, 0, s>>>(dev + (size_t)b * chunk, n, staged_ids(g) + done, g->w + done);
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaEventRecord(ev[b], s);
+    done += n;
+  }
+  cudaStreamSynchronize(s);
+  for (cudaEvent_t x : ev)
+    if (x) cudaEventDestroy(x);
+  nido::raw_free(ctx, dev);
+  if (st == NIDO_OK && e != cudaSuccess) st = nido_set_error(NIDO_E_CUDA, "upload_vite: %s", cudaGetErrorString(e));
+  if (st == NIDO_OK) st = graph_finish(g);
+  if (st != NIDO_OK) return fail_graph(g, st);
   *out = g;
   return NIDO_OK;
 }
@@ -524,27 +664,54 @@ extern "C" int nido_get_clustering(nido_graph g, int64_t* clustering) {
   return NIDO_OK;
 }
 
+namespace {
+// "%lld\n" of x at p; returns the end
+char* put_line(char* p, int64_t x) {
+  char tmp[20];
+  unsigned long long u = x < 0 ? 0ull - (unsigned long long)x : (unsigned long long)x;
+  int k = 0;
+  do {
+    tmp[k++] = (char)('0' + u % 10);
+    u /= 10;
+  } while (u);
+  if (x < 0) *p++ = '-';
+  while (k) *p++ = tmp[--k];
+  *p++ = '\n';
+  return p;
+}
+}  // namespace
+
+// Clustering::dump_partition (clustering.cpp:23-46): one "%lld\n" line per
+// original vertex, un-permuted through new_orders when given; the lines are
+// formatted by host threads in slices and written in order.
 extern "C" int nido_dump_partition(nido_graph g, const char* path, const int64_t* new_orders) {
   if (!g || !path) return nido_set_error(NIDO_E_INVALID, "null argument");
-  std::vector<int64_t> c(g->nv0);
+  const int64_t n = g->nv0;
+  std::vector<int64_t> c((size_t)n);
   NIDO_TRY(nido_get_clustering(g, c.data()));
   if (new_orders) {
-    std::vector<int64_t> t(g->nv0);
-    for (int64_t i = 0; i < g->nv0; ++i) t[new_orders[i]] = c[i];
+    std::vector<int64_t> t((size_t)n);
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; ++i) t[new_orders[i]] = c[i];
     c.swap(t);
   }
   FILE* f = fopen(path, "wt");
   if (!f) return nido_set_error(NIDO_E_IO, "cannot open %s", path);
-  std::vector<char> buf;
-  buf.reserve(1 << 20);
-  char line[32];
-  for (int64_t i = 0; i < g->nv0; ++i) {
-    const int n = snprintf(line, sizeof(line), "%lld\n", (long long)c[i]);
-    buf.insert(buf.end(), line, line + n);
-    if (buf.size() > (1u << 20)) { fwrite(buf.data(), 1, buf.size(), f); buf.clear(); }
+  const int T = std::max(1, std::min(16, omp_get_max_threads()));
+  const int64_t per = (n + T - 1) / T;
+  std::vector<std::vector<char>> parts((size_t)T);
+#pragma omp parallel for num_threads(T) schedule(static)
+  for (int t = 0; t < T; ++t) {
+    const int64_t lo = std::min(n, (int64_t)t * per), hi = std::min(n, lo + per);
+    std::vector<char>& b = parts[(size_t)t];
+    b.resize((size_t)(hi - lo) * 21);
+    char* p = b.data();
+    for (int64_t i = lo; i < hi; ++i) p = put_line(p, c[(size_t)i]);
+    b.resize((size_t)(p - b.data()));
   }
-  fwrite(buf.data(), 1, buf.size(), f);
-  if (fclose(f) != 0) return nido_set_error(NIDO_E_IO, "short write to %s", path);
+  bool ok = true;
+  for (const std::vector<char>& b : parts) ok = ok && fwrite(b.data(), 1, b.size(), f) == b.size();
+  if (fclose(f) != 0 || !ok) return nido_set_error(NIDO_E_IO, "short write to %s", path);
   return NIDO_OK;
 }
 

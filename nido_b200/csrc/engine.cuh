@@ -79,6 +79,9 @@ struct nido_ctx_s {
   std::multimap<size_t, void*> free_blocks;
   std::unordered_map<void*, size_t> live_blocks;
   size_t cached_bytes = 0;
+  // pinned host staging of nido_graph_upload_vite (grows, kept until destroy)
+  void* pinned = nullptr;
+  size_t pinned_bytes = 0;
 };
 
 struct nido_graph_s {
@@ -222,6 +225,8 @@ int graph_prepare_phase(nido_graph_s* g);               // k, m, tier lists (eng
 cudaError_t raw_alloc(nido_ctx_s* ctx, void** p, size_t bytes);
 void raw_free(nido_ctx_s* ctx, void* p);  // null is a no-op
 void release_cached(nido_ctx_s* ctx);     // cudaFree every cached free block
+// the context's pinned host staging buffer, grown to at least `bytes`
+cudaError_t pinned_buffer(nido_ctx_s* ctx, size_t bytes, void** p);
 // device memory counted against the context's HBM budget (engine.cu)
 int device_alloc(nido_ctx_s* ctx, void** p, size_t bytes);
 void device_free(nido_ctx_s* ctx, void* p, size_t bytes);

@@ -60,19 +60,24 @@ int main(int argc, char** argv) {
     fprintf(stderr, "-b must be at least 1\n");
     return EXIT_FAILURE;
   }
-  Graph graph(inputFileName);
-  printf("#Batches: %d\n#Threshold: %g\nMax #iterations: %lld\n#NGPUs: 1\n", nbatches, tau, maxLoops);
-  printf("--------------------------------------\n");
   nido_ctx ctx = nullptr;
   nido_check(nido_ctx_create(0, 0, &ctx), "nido_ctx_create");
   GraphElem* new_orders = nullptr;
-  if (is_colored) {
+  if (is_colored) {  // the relabel needs the CSR on the host
+    Graph graph(inputFileName);
+    printf("#Batches: %d\n#Threshold: %g\nMax #iterations: %lld\n#NGPUs: 1\n", nbatches, tau, maxLoops);
+    printf("--------------------------------------\n");
     const double t0 = omp_get_wtime();
     new_orders = graph.coloring(ctx);
     printf("Coloring Time: %g s\n", omp_get_wtime() - t0);
-  }
-  {
     GraphGPU graph_gpu(&graph, nbatches, ctx);
+    LouvainGPU louvain(maxLoops, tau, nbatches, tie);
+    louvain.run(&graph_gpu);
+    if (output_communities) graph_gpu.dump_partition(outFileName, new_orders);
+  } else {  // the file streams to the device
+    GraphGPU graph_gpu(inputFileName, nbatches, ctx);
+    printf("#Batches: %d\n#Threshold: %g\nMax #iterations: %lld\n#NGPUs: 1\n", nbatches, tau, maxLoops);
+    printf("--------------------------------------\n");
     LouvainGPU louvain(maxLoops, tau, nbatches, tie);
     louvain.run(&graph_gpu);
     if (output_communities) graph_gpu.dump_partition(outFileName, new_orders);

@@ -30,6 +30,28 @@ inline void nido_check(int st, const char* what) {
   }
 }
 
+// Graph::print_stats (graph.cpp:280-320): degree statistics from the offsets.
+inline void print_graph_stats(const GraphElem* off, GraphElem nv, GraphElem ne) {
+  std::vector<GraphElem> pdeg(nv);
+  for (GraphElem v = 0; v < nv; ++v) pdeg[v] = off[v + 1] - off[v];
+  std::sort(pdeg.begin(), pdeg.end());
+  GraphElem median = 0, mx = 0;
+  double sum = 0., sq = 0.;
+  if (nv > 0) {
+    median = nv % 2 ? pdeg[nv / 2] : (pdeg[nv / 2 - 1] + pdeg[nv / 2]) / 2;
+    mx = pdeg.back();
+    for (GraphElem d : pdeg) { sum += (double)d; sq += (double)d * (double)d; }
+  }
+  const double avg = nv ? sum / nv : 0., avg_sq = nv ? sq / nv : 0.;
+  const double var = std::abs(avg_sq - avg * avg);
+  printf("\n--------------------------------------\nGraph characteristics\n");
+  printf("--------------------------------------\n");
+  printf("Number of vertices: %lld\nNumber of edges: %lld\n", (long long)nv, (long long)ne);
+  printf("Maximum number of edges: %lld\nMedian number of edges: %lld\n", (long long)mx, (long long)median);
+  printf("Expected value of X^2: %g\nVariance: %g\nStandard deviation: %g\n", avg_sq, var, std::sqrt(var));
+  printf("--------------------------------------\n");
+}
+
 class Graph {
  public:
   explicit Graph(const std::string& binfile) {
@@ -61,27 +83,8 @@ class Graph {
   }
   const nido_csr& csr() const { return g_; }
 
-  // graph.cpp:383-423 (degree statistics)
-  void print_stats() const {
-    std::vector<GraphElem> pdeg(g_.nv);
-    for (GraphElem v = 0; v < g_.nv; ++v) pdeg[v] = g_.off[v + 1] - g_.off[v];
-    std::sort(pdeg.begin(), pdeg.end());
-    GraphElem median = 0, mx = 0;
-    double sum = 0., sq = 0.;
-    if (g_.nv > 0) {
-      median = g_.nv % 2 ? pdeg[g_.nv / 2] : (pdeg[g_.nv / 2 - 1] + pdeg[g_.nv / 2]) / 2;
-      mx = pdeg.back();
-      for (GraphElem d : pdeg) { sum += (double)d; sq += (double)d * (double)d; }
-    }
-    const double avg = g_.nv ? sum / g_.nv : 0., avg_sq = g_.nv ? sq / g_.nv : 0.;
-    const double var = std::abs(avg_sq - avg * avg);
-    printf("\n--------------------------------------\nGraph characteristics\n");
-    printf("--------------------------------------\n");
-    printf("Number of vertices: %lld\nNumber of edges: %lld\n", (long long)g_.nv, (long long)g_.ne);
-    printf("Maximum number of edges: %lld\nMedian number of edges: %lld\n", (long long)mx, (long long)median);
-    printf("Expected value of X^2: %g\nVariance: %g\nStandard deviation: %g\n", avg_sq, var, std::sqrt(var));
-    printf("--------------------------------------\n");
-  }
+  // graph.cpp:280-320 (degree statistics)
+  void print_stats() const { print_graph_stats(g_.off, g_.nv, g_.ne); }
 
   // graph.cpp:651-797: colour, relabel the CSR in place so that colour
   // classes are contiguous, return new_orders (new position -> old id);
@@ -115,6 +118,25 @@ class GraphGPU {
   GraphGPU(Graph* graph, int nbatches, nido_ctx ctx) : nv0_(graph->get_num_vertices()) {
     const nido_csr& c = graph->csr();
     nido_check(nido_graph_upload(ctx, c.nv, c.ne, c.off, c.adj, c.w, nbatches, &g_), "GraphGPU");
+  }
+  // Graph(file) + GraphGPU in one step: the Vite file streams to the device
+  // (nido_graph_upload_vite) and only the offsets come back for the
+  // statistics the reference prints while reading.
+  GraphGPU(const std::string& binfile, int nbatches, nido_ctx ctx) {
+    FILE* f = fopen(binfile.c_str(), "rb");
+    if (!f) {
+      printf(" Error opening file! \n");
+      fflush(stdout);
+      abort();
+    }
+    fclose(f);
+    nido_check(nido_graph_upload_vite(ctx, binfile.c_str(), nbatches, &g_), "GraphGPU(binfile)");
+    int64_t nv = 0, ne = 0;
+    nido_check(nido_graph_size(g_, &nv, &ne), "GraphGPU(binfile)");
+    std::vector<int64_t> off((size_t)nv + 1);
+    nido_check(nido_graph_download(g_, off.data(), nullptr, nullptr), "GraphGPU(binfile)");
+    nv0_ = nv;
+    print_graph_stats(off.data(), nv, ne);
   }
   ~GraphGPU() { nido_graph_free(g_); }
   GraphGPU(const GraphGPU&) = delete;

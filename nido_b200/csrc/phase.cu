@@ -95,22 +95,53 @@ __global__ void k_comm_weights(int64_t nv, const int32_t* __restrict__ comm,
 // update_community_weights_kernel + exchange_vector_kernel fused
 // (graph_cuda.cu:1234-1250, 1191-1196): movers subtract k_v from the old
 // community and add it to the new one; then ids swap so newc keeps the old
-// id for restore_community.
+// id for restore_community.  Movers of a warp with the same old (new)
+// community add their k_v first (in lane order) and issue one atomic per
+// community, which takes the contention off communities many vertices join.
+// The atomics' order is not fixed (as in the reference); on integer weights
+// every sum is exact.
+__device__ __forceinline__ void warp_community_add(double* a, int c, double x, bool on) {
+  const int lane = threadIdx.x & 31;
+  const unsigned peers = __match_any_sync(NIDO_FULL_MASK, on ? c : -1);
+  double s = 0.;
+  unsigned rem = on ? peers : 0u;
+  const int maxcnt = __reduce_max_sync(NIDO_FULL_MASK, (unsigned)__popc(rem));
+  for (int it = 0; it < maxcnt; ++it) {
+    const int src = rem ? __ffs(rem) - 1 : lane;
+    const double y = __shfl_sync(NIDO_FULL_MASK, x, src);
+    if (rem) { s += y; rem &= rem - 1; }
+  }
+  if (on && lane == __ffs(peers) - 1) atomicAdd(&a[c], s);
+}
+
 __global__ void k_commit(int64_t v0, int64_t v1, const double* __restrict__ k,
                          int32_t* __restrict__ comm, int32_t* __restrict__ newc,
                          double* __restrict__ a, int64_t* __restrict__ moved) {
   int64_t cnt = 0;
-  for (int64_t v = v0 + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; v < v1;
-       v += (int64_t)gridDim.x * blockDim.x) {
-    const int32_t src = comm[v], dst = newc[v];
-    if (src != dst) {
-      const double kv = k[v];
-      atomicAdd(&a[src], -kv);
-      atomicAdd(&a[dst], kv);
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  // the loop runs warp-uniformly (the warp's first lane decides)
+  for (int64_t base = v0 + blockIdx.x * (int64_t)blockDim.x + (threadIdx.x & ~31); base < v1; base += stride) {
+    const int64_t v = base + (threadIdx.x & 31);
+    int32_t src = 0, dst = 0;
+    double kv = 0.;
+    const bool in = v < v1;
+    if (in) {
+      src = comm[v];
+      dst = newc[v];
+    }
+    const bool mv = in && src != dst;
+    if (mv) {
+      kv = k[v];
       ++cnt;
     }
-    comm[v] = dst;
-    newc[v] = src;
+    if (__any_sync(NIDO_FULL_MASK, mv)) {
+      warp_community_add(a, src, -kv, mv);
+      warp_community_add(a, dst, kv, mv);
+    }
+    if (in) {
+      comm[v] = dst;
+      newc[v] = src;
+    }
   }
   if (moved) {
 #pragma unroll

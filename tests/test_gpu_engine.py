@@ -288,3 +288,45 @@ def test_freed_blocks_reused_and_trimmed(nido_lib):
                 got, st = g.run()
             assert np.array_equal(got, want) and st.final_q == st0.final_q
         assert c.trim() == held  # three uploads, one set of blocks
+
+
+def test_vite_streamed_to_device(nido_lib, ctx, orc, tmp_path):
+    """nido_graph_upload_vite gives the graph that nido_read_vite +
+    nido_graph_upload give: same device CSR (offsets rebased), and on integer
+    weights the same run bit for bit (FP64 weights leave the last bit of Q to
+    the order of the community-weight atomics); a missing or truncated file
+    is an error."""
+    G = nido_lib.gen_sbm(20000, cmin=16, cmax=1024, avg_degree=24.0, wmode=nido_lib.W_LOGNORMAL, seed=9)
+    p = str(tmp_path / "g.bin")
+    nido_lib.write_vite(p, G)
+    with nido_lib.Graph(ctx, nido_lib.read_vite(p), 2) as a, nido_lib.Graph.from_vite(ctx, p, 2) as b:
+        da, db = a.download(), b.download()
+        assert np.array_equal(da.off, db.off) and np.array_equal(da.adj, db.adj)
+        assert np.array_equal(da.w.view(np.uint64), db.w.view(np.uint64))
+        ca, sa = a.run()
+        cb, sb = b.run()
+        assert abs(sa.final_q - sb.final_q) <= 1e-12 and orc.nmi(ca, cb) >= 0.99
+    # offsets starting above 0 are rebased; records span several stream chunks
+    raw = open(p, "rb").read()
+    nv, ne = np.frombuffer(raw[:16], np.int64)
+    off = np.frombuffer(raw[16:16 + 8 * (nv + 1)], np.int64) + 1000
+    p2 = str(tmp_path / "g2.bin")
+    open(p2, "wb").write(raw[:16] + off.tobytes() + raw[16 + 8 * (nv + 1):])
+    with nido_lib.Graph.from_vite(ctx, p2, 2) as c:
+        dc = c.download()
+        assert np.array_equal(dc.off, da.off) and np.array_equal(dc.adj, da.adj)
+    big = nido_lib.gen_rmat(1 << 20, 16 << 20, wmode=nido_lib.W_INT8, seed=4)  # > 4M records: 8 chunks
+    p3 = str(tmp_path / "g3.bin")
+    nido_lib.write_vite(p3, big)
+    with nido_lib.Graph.from_vite(ctx, p3, 2) as d, nido_lib.Graph(ctx, big, 2) as e:
+        dd = d.download()
+        assert np.array_equal(dd.off, big.off) and np.array_equal(dd.adj, big.adj)
+        assert np.array_equal(dd.w, big.w)
+        cd, sd = d.run()
+        ce, se = e.run()
+        assert np.array_equal(cd, ce) and sd.final_q == se.final_q and sd.total_loops == se.total_loops
+    open(p2, "wb").write(raw[: len(raw) - 8])
+    with pytest.raises(nido_lib.NidoError):
+        nido_lib.Graph.from_vite(ctx, p2, 2)
+    with pytest.raises(nido_lib.NidoError):
+        nido_lib.Graph.from_vite(ctx, str(tmp_path / "missing.bin"), 2)
