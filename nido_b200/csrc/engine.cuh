@@ -90,7 +90,9 @@ struct nido_graph_s {
   int64_t nv = 0, ne = 0;    // current phase
   int64_t cap_v = 0, cap_e = 0;
   int nbatches = 1;
-  bool int_weights = false;  // every weight integral and total below 2^53
+  // every weight of the current phase integral and every vertex's sum of |w|
+  // below 2^31 (set with k_v each phase; the move phase then sums in int32)
+  bool int_weights = false;
   double m = 0.0;            // host copy of the mass
 
   int64_t ne0 = 0;           // original edge count

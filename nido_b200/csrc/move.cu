@@ -44,6 +44,11 @@ struct MoveArgs {
   // one graph, whose mass is m)
   const int32_t* __restrict__ gid;
   const double* __restrict__ mg;
+  // every weight integral and every vertex's sum of |w| below 2^31: the
+  // shared-memory tables then add int32 (a native shared-memory atomic; the
+  // FP64 one is several times slower) and every partial sum is exact, so
+  // the e_vc read back are the FP64 sums bit for bit
+  int ints;
 };
 
 // The mass of v's graph (kernels are instantiated per mode, so the
@@ -191,11 +196,19 @@ __global__ void __launch_bounds__(256) k_move_group(const int32_t* __restrict__ 
 // table is reported through *err.
 struct Table {
   int* keys;
-  double* vals;
+  double* vals;  // FP64 values, or with ints the int32 sum in each slot's low word
   int* occ;
   int* nocc;
   unsigned mask;
+  bool ints = false;  // shared-memory tables of integer-weight phases
 };
+
+__device__ __forceinline__ int* int_slot(const Table& t, unsigned h) { return reinterpret_cast<int*>(t.vals + h); }
+
+// e_vc of a slot of a shared-memory table
+__device__ __forceinline__ double table_val(const Table& t, int slot) {
+  return t.ints ? (double)*int_slot(t, (unsigned)slot) : t.vals[slot];
+}
 
 // Adds e to key c's value, inserting c when absent; returns the slot and
 // whether this call inserted it.  Tables in global memory (kGlobal) go
@@ -225,8 +238,13 @@ __device__ __forceinline__ int table_add(const Table& t, int c, double e, bool& 
       hit = isnew || old == c;
     }
     if (hit) {
-      if (kAtomicVals) atomicAdd(&t.vals[h], e);
-      else t.vals[h] += e;
+      if (t.ints) {
+        if (kAtomicVals) atomicAdd(int_slot(t, h), __double2int_rn(e));
+        else *int_slot(t, h) += __double2int_rn(e);
+      } else {
+        if (kAtomicVals) atomicAdd(&t.vals[h], e);
+        else t.vals[h] += e;
+      }
       return (int)h;
     }
     h = (h + 1) & t.mask;
@@ -369,7 +387,7 @@ __device__ __forceinline__ void scan_entries(const MoveArgs& p, double m, const 
       if (ii < n) {
         const int slot = t.occ ? t.occ[ii] : ii;
         cc[k] = cg ? __ldcg(&t.keys[slot]) : t.keys[slot];
-        val[k] = cg ? __ldcg(&t.vals[slot]) : t.vals[slot];
+        val[k] = cg ? __ldcg(&t.vals[slot]) : table_val(t, slot);
       }
     }
 #pragma unroll
@@ -398,7 +416,7 @@ __device__ __forceinline__ void nido_tie_entries(const MoveArgs& p, double m, co
     const int slot = t.occ ? t.occ[i] : i;
     const int cc = cg ? __ldcg(&t.keys[slot]) : t.keys[slot];
     if (cc < 0 || cc == own) continue;
-    const double val = cg ? __ldcg(&t.vals[slot]) : t.vals[slot];
+    const double val = cg ? __ldcg(&t.vals[slot]) : table_val(t, slot);
     if (gain_of(val, ki, p.a[cc], m) != gm) continue;
     unsigned rank = 0;
     for (int q = 0; q < n; ++q) {
@@ -418,7 +436,7 @@ __device__ __forceinline__ void decide(const MoveArgs& p, double m, int v, int o
 }
 
 // ---- 32 < degree <= 256: one warp per vertex, table in shared memory -----------
-template <int kCap, bool kMulti>
+template <int kCap, bool kMulti, bool kInts>
 __global__ void __launch_bounds__(256) k_move_warp(const int32_t* __restrict__ list, int64_t n, MoveArgs p) {
   extern __shared__ double smem[];
   __shared__ int nocc_s[8];
@@ -428,6 +446,7 @@ __global__ void __launch_bounds__(256) k_move_warp(const int32_t* __restrict__ l
   t.keys = reinterpret_cast<int*>(smem + 8 * kCap) + (size_t)wid * 2 * kCap;
   t.occ = t.keys + kCap;
   t.nocc = &nocc_s[wid];
+  t.ints = kInts;
   for (int i = lane; i < kCap; i += 32) { t.keys[i] = -1; t.vals[i] = 0.; }
   if (lane == 0) *t.nocc = 0;
   __syncwarp();
@@ -541,7 +560,7 @@ __device__ __forceinline__ void block_evaluate(const MoveArgs& p, double m, cons
 // kOcc: keep a list of occupied slots (16 bytes a slot) so evaluation and
 // clearing touch only used slots; without it (12 bytes a slot, for the
 // largest table) both walk the vertex's whole table.
-template <int kThreads, int kCap, bool kMulti, bool kOcc = true>
+template <int kThreads, int kCap, bool kMulti, bool kInts, bool kOcc = true>
 __global__ void __launch_bounds__(kThreads) k_move_cta(const int32_t* __restrict__ list, int64_t n, MoveArgs p) {
   extern __shared__ double smem[];
   __shared__ double sg[32];
@@ -553,6 +572,7 @@ __global__ void __launch_bounds__(kThreads) k_move_cta(const int32_t* __restrict
   t.keys = reinterpret_cast<int*>(smem + kCap);
   t.occ = kOcc ? t.keys + kCap : nullptr;
   t.nocc = &nocc_s;
+  t.ints = kInts;
   for (int i = threadIdx.x; i < kCap; i += kThreads) { t.keys[i] = -1; t.vals[i] = 0.; }
   if (threadIdx.x == 0) nocc_s = 0;
   __syncthreads();
@@ -943,7 +963,7 @@ struct Resident {
   int64_t g4 = kSMs, g8 = kSMs, g16 = kSMs, g32 = kSMs, warp = kSMs, ctas = kSMs, ctam = kSMs, ctal = kSMs,
           ctax = kSMs, hubmv = kSMs, hubins = kSMs, hubsl = kSMs;
 };
-Resident g_resident[2];
+Resident g_resident[2][2];  // [many graphs][integer tables]
 
 template <typename K>
 int64_t resident(K kernel, int threads, size_t smem, int sms) {
@@ -955,28 +975,28 @@ int64_t resident(K kernel, int threads, size_t smem, int sms) {
   return (int64_t)std::max(per_sm, 1) * sms;
 }
 
-template <bool kMulti>
+template <bool kMulti, bool kInts>
 int set_smem_mode() {
-  NIDO_TRY(set_smem(k_move_warp<kWarpCap, kMulti>, (size_t)8 * kWarpCap * 16));
-  NIDO_TRY(set_smem(k_move_cta<kCtaSThreads, kCtaSCap, kMulti>, (size_t)kCtaSCap * 16));
-  NIDO_TRY(set_smem(k_move_cta<kCtaMThreads, kCtaMCap, kMulti>, (size_t)kCtaMCap * 16));
-  NIDO_TRY(set_smem(k_move_cta<kCtaLThreads, kCtaLCap, kMulti>, (size_t)kCtaLCap * 16));
-  NIDO_TRY(set_smem(k_move_cta<1024, kCtaXCap, kMulti, false>, (size_t)kCtaXCap * 12));
+  NIDO_TRY(set_smem(k_move_warp<kWarpCap, kMulti, kInts>, (size_t)8 * kWarpCap * 16));
+  NIDO_TRY(set_smem(k_move_cta<kCtaSThreads, kCtaSCap, kMulti, kInts>, (size_t)kCtaSCap * 16));
+  NIDO_TRY(set_smem(k_move_cta<kCtaMThreads, kCtaMCap, kMulti, kInts>, (size_t)kCtaMCap * 16));
+  NIDO_TRY(set_smem(k_move_cta<kCtaLThreads, kCtaLCap, kMulti, kInts>, (size_t)kCtaLCap * 16));
+  NIDO_TRY(set_smem(k_move_cta<1024, kCtaXCap, kMulti, kInts, false>, (size_t)kCtaXCap * 12));
   int dev = 0, sms = kSMs;
   NIDO_CUDA_TRY(cudaGetDevice(&dev));
   NIDO_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
   static std::mutex mu;  // contexts may be created from several threads
   std::lock_guard<std::mutex> lk(mu);
-  Resident& R = g_resident[kMulti ? 1 : 0];
+  Resident& R = g_resident[kMulti ? 1 : 0][kInts ? 1 : 0];
   R.g4 = resident(k_move_group<4, kMulti>, 256, 0, sms);
   R.g8 = resident(k_move_group<8, kMulti>, 256, 0, sms);
   R.g16 = resident(k_move_group<16, kMulti>, 256, 0, sms);
   R.g32 = resident(k_move_group<32, kMulti>, 256, 0, sms);
-  R.warp = resident(k_move_warp<kWarpCap, kMulti>, 256, (size_t)8 * kWarpCap * 16, sms);
-  R.ctas = resident(k_move_cta<kCtaSThreads, kCtaSCap, kMulti>, kCtaSThreads, (size_t)kCtaSCap * 16, sms);
-  R.ctam = resident(k_move_cta<kCtaMThreads, kCtaMCap, kMulti>, kCtaMThreads, (size_t)kCtaMCap * 16, sms);
-  R.ctal = resident(k_move_cta<kCtaLThreads, kCtaLCap, kMulti>, kCtaLThreads, (size_t)kCtaLCap * 16, sms);
-  R.ctax = resident(k_move_cta<1024, kCtaXCap, kMulti, false>, 1024, (size_t)kCtaXCap * 12, sms);
+  R.warp = resident(k_move_warp<kWarpCap, kMulti, kInts>, 256, (size_t)8 * kWarpCap * 16, sms);
+  R.ctas = resident(k_move_cta<kCtaSThreads, kCtaSCap, kMulti, kInts>, kCtaSThreads, (size_t)kCtaSCap * 16, sms);
+  R.ctam = resident(k_move_cta<kCtaMThreads, kCtaMCap, kMulti, kInts>, kCtaMThreads, (size_t)kCtaMCap * 16, sms);
+  R.ctal = resident(k_move_cta<kCtaLThreads, kCtaLCap, kMulti, kInts>, kCtaLThreads, (size_t)kCtaLCap * 16, sms);
+  R.ctax = resident(k_move_cta<1024, kCtaXCap, kMulti, kInts, false>, 1024, (size_t)kCtaXCap * 12, sms);
   R.hubmv = resident(k_move_hub<kMulti>, kHubThreads, 0, sms);
   R.hubins = resident(k_hub_insert, kHubThreads, 0, sms);
   R.hubsl = resident(k_hub_slices<kMulti>, kHubThreads, 0, sms);
@@ -987,10 +1007,10 @@ int set_smem_mode() {
 // tiers cover disjoint vertices and only read comm and a, so they run on
 // three streams: the hub chain and the CTA tiers on the context's side
 // streams, the rest on its stream, joined before the function returns.
-template <bool kMulti>
+template <bool kMulti, bool kInts>
 int launch_tiers(nido_graph_s* g, int batch, int tie, const MoveArgs& p) {
   nido_ctx_s* ctx = g->ctx;
-  const Resident& R = g_resident[kMulti ? 1 : 0];
+  const Resident& R = g_resident[kMulti ? 1 : 0][kInts ? 1 : 0];
   const cudaStream_t main_s = ctx->stream;
   NIDO_CUDA_TRY(cudaEventRecord(ctx->fork_ev, main_s));
   for (int i = 0; i < 2; ++i) NIDO_CUDA_TRY(cudaStreamWaitEvent(ctx->aux[i], ctx->fork_ev, 0));
@@ -1015,20 +1035,20 @@ int launch_tiers(nido_graph_s* g, int batch, int tie, const MoveArgs& p) {
         k_move_group<32, kMulti><<<grid_cap((n + 7) / 8, R.g32), 256, 0, s>>>(list, n, p);
         break;
       case kTierWarp:
-        k_move_warp<kWarpCap, kMulti><<<grid_cap((n + 7) / 8, R.warp), 256, (size_t)8 * kWarpCap * 16, s>>>(
+        k_move_warp<kWarpCap, kMulti, kInts><<<grid_cap((n + 7) / 8, R.warp), 256, (size_t)8 * kWarpCap * 16, s>>>(
             list, n, p);
         break;
       case kTierCtaS:
-        k_move_cta<kCtaSThreads, kCtaSCap, kMulti><<<grid_cap(n, R.ctas), kCtaSThreads, (size_t)kCtaSCap * 16, s>>>(list, n, p);
+        k_move_cta<kCtaSThreads, kCtaSCap, kMulti, kInts><<<grid_cap(n, R.ctas), kCtaSThreads, (size_t)kCtaSCap * 16, s>>>(list, n, p);
         break;
       case kTierCtaM:
-        k_move_cta<kCtaMThreads, kCtaMCap, kMulti><<<grid_cap(n, R.ctam), kCtaMThreads, (size_t)kCtaMCap * 16, s>>>(list, n, p);
+        k_move_cta<kCtaMThreads, kCtaMCap, kMulti, kInts><<<grid_cap(n, R.ctam), kCtaMThreads, (size_t)kCtaMCap * 16, s>>>(list, n, p);
         break;
       case kTierCtaL:
-        k_move_cta<kCtaLThreads, kCtaLCap, kMulti><<<grid_cap(n, R.ctal), kCtaLThreads, (size_t)kCtaLCap * 16, s>>>(list, n, p);
+        k_move_cta<kCtaLThreads, kCtaLCap, kMulti, kInts><<<grid_cap(n, R.ctal), kCtaLThreads, (size_t)kCtaLCap * 16, s>>>(list, n, p);
         break;
       case kTierCtaX:
-        k_move_cta<1024, kCtaXCap, kMulti, false><<<grid_cap(n, R.ctax), 1024, (size_t)kCtaXCap * 12, s>>>(list, n, p);
+        k_move_cta<1024, kCtaXCap, kMulti, kInts, false><<<grid_cap(n, R.ctax), 1024, (size_t)kCtaXCap * 12, s>>>(list, n, p);
         break;
       default: {
         SliceResult* res = reinterpret_cast<SliceResult*>(g->hub_res);
@@ -1067,8 +1087,10 @@ int launch_tiers(nido_graph_s* g, int batch, int tie, const MoveArgs& p) {
 }  // namespace
 
 int move_init_attributes() {
-  NIDO_TRY(set_smem_mode<false>());
-  return set_smem_mode<true>();
+  NIDO_TRY((set_smem_mode<false, false>()));
+  NIDO_TRY((set_smem_mode<false, true>()));
+  NIDO_TRY((set_smem_mode<true, false>()));
+  return set_smem_mode<true, true>();
 }
 
 int launch_move(nido_graph_s* g, int batch, int tie, cudaEvent_t ev_start, cudaEvent_t ev_end) {
@@ -1077,9 +1099,12 @@ int launch_move(nido_graph_s* g, int batch, int tie, cudaEvent_t ev_start, cudaE
   if (!g->bins_valid) NIDO_TRY(build_batches(g));
   cudaStream_t s = g->ctx->stream;
   MoveArgs p{g->off, g->adj, g->w, g->comm, g->k, g->a, g->newc, g->m, tie,
-             reinterpret_cast<unsigned long long*>(g->dcount + 1), g->gid, g->mg};
+             reinterpret_cast<unsigned long long*>(g->dcount + 1), g->gid, g->mg, g->int_weights ? 1 : 0};
   if (ev_start) NIDO_CUDA_TRY(cudaEventRecord(ev_start, s));
-  auto direct = [&]() { return g->gid ? launch_tiers<true>(g, batch, tie, p) : launch_tiers<false>(g, batch, tie, p); };
+  auto direct = [&]() {
+    if (g->gid) return p.ints ? launch_tiers<true, true>(g, batch, tie, p) : launch_tiers<true, false>(g, batch, tie, p);
+    return p.ints ? launch_tiers<false, true>(g, batch, tie, p) : launch_tiers<false, false>(g, batch, tie, p);
+  };
   if (!g->use_graphs) {
     NIDO_TRY(direct());
   } else {

@@ -8,6 +8,8 @@
 // inputs; the per-vertex in-community sums inside Q use a fixed order of this
 // engine, which equals the reference's wherever the sums are exact (integer
 // weights).
+#include <string.h>
+
 #include <algorithm>
 
 #include "common.cuh"
@@ -28,20 +30,38 @@ inline unsigned grid_for(int64_t work, int per_block, int max_blocks = 148 * 16)
 }
 
 // k_v: one warp per vertex, lane l sums edges l, l+32, ... then a shuffle-down
-// tree (sum_vertex_weights_kernel, graph_cuda.cu:302-346).
+// tree (sum_vertex_weights_kernel, graph_cuda.cu:302-346).  Alongside, for
+// the move kernels' choice of integer tables: flags[0] counts weights that
+// are not finite integers and flags[1] keeps the largest sum of |w| of a
+// vertex (as the bits of a non-negative double, which order like the values).
 __global__ void k_vertex_weights(const int64_t* __restrict__ off, const double* __restrict__ w,
-                                 int64_t nv, double* __restrict__ k) {
+                                 int64_t nv, double* __restrict__ k, unsigned long long* __restrict__ flags) {
   const int lane = threadIdx.x & 31;
   const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+  unsigned long long bad = 0;
+  double amax = 0.;
   for (int64_t v = warp; v < nv; v += nw) {
     const int64_t s = off[v], e = off[v + 1];
-    double x = 0.;
-    for (int64_t j = s + lane; j < e; j += 32) x += w[j];
+    double x = 0., ax = 0.;
+    for (int64_t j = s + lane; j < e; j += 32) {
+      const double y = w[j];
+      x += y;
+      ax += fabs(y);
+      if (!(fabs(y) < 9.0e15) || y != trunc(y)) ++bad;
+    }
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(NIDO_FULL_MASK, x, o);
-    if (lane == 0) k[v] = x;
+    for (int o = 16; o > 0; o >>= 1) {
+      x += __shfl_down_sync(NIDO_FULL_MASK, x, o);
+      ax += __shfl_down_sync(NIDO_FULL_MASK, ax, o);
+    }
+    if (lane == 0) {
+      k[v] = x;
+      amax = fmax(amax, ax);
+    }
   }
+  if (bad) atomicAdd(&flags[0], bad);
+  if (lane == 0 && amax > 0.) atomicMax(&flags[1], (unsigned long long)__double_as_longlong(amax));
 }
 
 // m, first stage: compute_mass_reduce_kernel<32><<<4096,32>>>
@@ -379,10 +399,20 @@ __global__ void k_tier_keys(const int64_t* __restrict__ off, int64_t nv, const i
 }  // namespace
 
 int launch_vertex_weights(nido_graph_s* g) {
+  g->int_weights = false;
   if (g->nv == 0) return NIDO_OK;
-  k_vertex_weights<<<grid_for(g->nv * 32, kThreads, 148 * 64), kThreads, 0, g->ctx->stream>>>(
-      g->off, g->w, g->nv, g->k);
+  cudaStream_t s = g->ctx->stream;
+  unsigned long long* flags = reinterpret_cast<unsigned long long*>(g->dcount + 2);
+  NIDO_CUDA_TRY(cudaMemsetAsync(flags, 0, 2 * sizeof(unsigned long long), s));
+  k_vertex_weights<<<grid_for(g->nv * 32, kThreads, 148 * 64), kThreads, 0, s>>>(g->off, g->w, g->nv, g->k, flags);
   NIDO_LAUNCH_CHECK();
+  unsigned long long f[2] = {0, 0};
+  NIDO_CUDA_TRY(cudaMemcpyAsync(f, flags, sizeof(f), cudaMemcpyDeviceToHost, s));
+  NIDO_CUDA_TRY(cudaStreamSynchronize(s));
+  double amax = 0.;
+  memcpy(&amax, &f[1], sizeof(amax));
+  // int32 table sums are exact when no vertex's sum of |w| reaches 2^31
+  g->int_weights = f[0] == 0 && amax < 2147483648.0;
   return NIDO_OK;
 }
 

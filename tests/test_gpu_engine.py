@@ -193,6 +193,21 @@ def test_full_run_vs_oracle(nido_lib, ctx, orc, graphs, gname, tie):
     assert np.array_equal(cl, want)
 
 
+@pytest.mark.parametrize("scale", [1.0, float(1 << 27)])
+def test_integer_weight_paths_vs_oracle(nido_lib, ctx, orc, graphs, scale):
+    """Integer weights run the move tables in int32 while every vertex's sum
+    of |w| stays below 2^31 and in FP64 above (weights scaled by 2^27 push
+    the sums past it); both are exact, so both match the oracle bit for bit."""
+    G0 = graphs["sbm_int"]
+    G = nido_lib.Csr(G0.off, G0.adj, G0.w * scale)
+    want, st_o = orc.louvain(G.off, G.adj, G.w, nbatches=2)
+    with nido_lib.Graph(ctx, G, 2) as g:
+        cl, st = g.run()
+    assert st.phases == st_o.phases and st.total_loops == st_o.total_loops
+    assert np.array_equal(np.array(st.q_phase[: st.phases]), np.array(st_o.q_phase[: st_o.phases]))
+    assert np.array_equal(cl, want)
+
+
 def test_lognormal_run_quality(nido_lib, ctx, orc):
     G = nido_lib.gen_sbm(40000, cmin=16, cmax=2048, avg_degree=20.0, wmode=nido_lib.W_LOGNORMAL, seed=31)
     want, st_o = orc.louvain(G.off, G.adj, G.w, nbatches=2)
