@@ -32,8 +32,10 @@ namespace nido {
 namespace {
 
 // tiers by member-edge count D: groups of 4/8/16/32 lanes (D <= 4/8/16/32),
-// warp, CTA-S, CTA-L, giant
-constexpr unsigned kAggTiers = 8;
+// warp, CTA-S, CTA-L, CTA-L without per-position slots (more than 4096
+// positions but a table that fits: few coarse vertices, 2*min(D, nvp) <= 8192),
+// giant
+constexpr unsigned kAggTiers = 9;
 constexpr int kAggWarpMaxD = 256;   // member edges handled by one warp
 // CTA tiers: threads, shared-memory table slots and list positions (member
 // edges) of one coarse vertex; a table holds at least twice the positions
@@ -142,8 +144,9 @@ __global__ void k_agg_tiers(const int64_t* __restrict__ mo, const int64_t* __res
     uint32_t t = kAggTiers;
     if (c < nvp) {
       const int64_t D = medge[mo[c + 1]] - medge[mo[c]];
+      const int64_t U = D < nvp ? D : nvp;
       t = D <= 4 ? 0u : D <= 8 ? 1u : D <= 16 ? 2u : D <= 32 ? 3u
-        : D <= kAggWarpMaxD ? 4u : D <= kAggSMaxD ? 5u : D <= kAggLMaxD ? 6u : 7u;
+        : D <= kAggWarpMaxD ? 4u : D <= kAggSMaxD ? 5u : D <= kAggLMaxD ? 6u : 2 * U <= kAggLCap ? 7u : 8u;
       keys[c] = t;
       vals[c] = (uint32_t)c;
     }
@@ -194,6 +197,15 @@ __device__ __forceinline__ int find_or_insert(int* keys, unsigned mask, int X, b
       if (old == -1) { *isnew = true; return (int)h; }
       if (old == X) return (int)h;
     }
+    h = (h + 1) & mask;
+  }
+  return -1;
+}
+
+__device__ __forceinline__ int find_slot(const int* keys, unsigned mask, int X) {
+  unsigned h = hash_slot(X, mask);
+  for (unsigned probe = 0; probe <= mask; ++probe) {
+    if (keys[h] == X) return (int)h;
     h = (h + 1) & mask;
   }
   return -1;
@@ -343,6 +355,8 @@ __global__ void __launch_bounds__(256) k_agg_warp(const int32_t* __restrict__ li
 // and records the slot of every position in shared memory; pass 2 walks the
 // positions in order from those slots (no second walk through members,
 // offsets and the new-id gather) and emits each id at its first position.
+// kMaxD == 0: any number of positions (the table still holds every id);
+// pass 2 gathers each position's id again and looks its slot up.
 template <int kThreads, int kCap, int kMaxD>
 __global__ void __launch_bounds__(kThreads) k_agg_cta(const int32_t* __restrict__ list, int64_t n, AggArgs q) {
   extern __shared__ double smem[];
@@ -389,8 +403,10 @@ __global__ void __launch_bounds__(kThreads) k_agg_cta(const int32_t* __restrict_
           atomicAdd(q.err, 1ull);
         }
       }
-      h = __shfl_sync(NIDO_FULL_MASK, h, leader);
-      if (ok) hpos[P - P0] = h;
+      if (kMaxD > 0) {
+        h = __shfl_sync(NIDO_FULL_MASK, h, leader);
+        if (ok) hpos[P - P0] = h;
+      }
     }
     // emit in list order: per kThreads positions one barrier, the warps'
     // counts double-buffered, every thread carrying the running total
@@ -398,7 +414,17 @@ __global__ void __launch_bounds__(kThreads) k_agg_cta(const int32_t* __restrict_
     int running = 0, par = 0;
     for (int64_t base = 0; base < P1 - P0; base += kThreads, par ^= 1) {
       const int i = (int)base + threadIdx.x;
-      const int h = i < P1 - P0 ? hpos[i] : -1;
+      int h = -1;
+      if (i < P1 - P0) {
+        if (kMaxD > 0) {
+          h = hpos[i];
+        } else {
+          int X;
+          double wt;
+          load_pos(q, m0, m1, P0 + i, X, wt);
+          h = find_slot(keys, mask, X);
+        }
+      }
       const bool first = h >= 0 && fpos[h] == i;
       const unsigned bal = __ballot_sync(NIDO_FULL_MASK, first);
       if (lane == 0) wsum[par][wid] = __popc(bal);
@@ -740,8 +766,8 @@ int launch_aggregation(nido_graph_s* g, int* done) {
   uint32_t* tv2 = reinterpret_cast<uint32_t*>(degp);  // degp is written only after the tier sort
   k_agg_tiers<<<grid_for(nvp, 256, kSMs * 16), 256, 0, s>>>(mo, medge, nvp, tk, tv, counts);
   NIDO_LAUNCH_CHECK();
-  NIDO_TRY(radix_sort_pairs(tk, tv, tk2, tv2, nvp, 3, temp, s));
-  int64_t cnt[kAggTiers] = {0, 0, 0, 0, 0, 0, 0, 0};
+  NIDO_TRY(radix_sort_pairs(tk, tv, tk2, tv2, nvp, 4, temp, s));
+  int64_t cnt[kAggTiers] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
   NIDO_CUDA_TRY(cudaMemcpyAsync(cnt, counts, sizeof(cnt), cudaMemcpyDeviceToHost, s));
   NIDO_CUDA_TRY(cudaStreamSynchronize(s));
   int64_t at[kAggTiers + 1] = {0};  // first list entry of every tier
@@ -786,11 +812,19 @@ int launch_aggregation(nido_graph_s* g, int* done) {
     NIDO_LAUNCH_CHECK();
   }
   if (cnt[7] > 0) {
+    constexpr size_t sm = agg_cta_smem<kAggLThreads, kAggLCap, 0>();
+    auto k = k_agg_cta<kAggLThreads, kAggLCap, 0>;
+    NIDO_CUDA_TRY(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    k<<<grid_for(cnt[7], 1, agg_resident(k, kAggLThreads, sm)), kAggLThreads, sm, ctx->aux[1]>>>(list + at[7],
+                                                                                             cnt[7], q);
+    NIDO_LAUNCH_CHECK();
+  }
+  if (cnt[8] > 0) {
     // plan: per giant coarse vertex a table of >= 2*min(D, nvp) slots and
     // ceil(D / kAggSeg) segment items; giants go in waves whose tables share
     // one region of at most kAggWaveSlots slots (or one larger table)
-    const int64_t n2 = cnt[7];
-    const int32_t* list2 = list + at[7];
+    const int64_t n2 = cnt[8];
+    const int32_t* list2 = list + at[8];
     int64_t* dsz = ar.take<int64_t>(n2);
     if (!dsz) return nido_set_error(NIDO_E_NOMEM, "scratch arena too small (aggregation plan)");
     k_agg_sizes<<<grid_for(n2, 256, kSMs * 4), 256, 0, s>>>(list2, n2, mo, medge, dsz);

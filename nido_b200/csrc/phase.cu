@@ -31,9 +31,11 @@ inline unsigned grid_for(int64_t work, int per_block, int max_blocks = 148 * 16)
 
 // k_v: one warp per vertex, lane l sums edges l, l+32, ... then a shuffle-down
 // tree (sum_vertex_weights_kernel, graph_cuda.cu:302-346).  Alongside, for
-// the move kernels' choice of integer tables: flags[0] counts weights that
-// are not finite integers and flags[1] keeps the largest sum of |w| of a
-// vertex (as the bits of a non-negative double, which order like the values).
+// the move kernels' choice of integer tables: flags[0] becomes nonzero when a
+// weight is not a finite integer and flags[1] keeps the largest sum of |w| of
+// a vertex (as the bits of a non-negative double, which order like the
+// values).  One lane per warp writes each, and only while the value would
+// change, so the flags cost no queue of same-address atomics.
 __global__ void k_vertex_weights(const int64_t* __restrict__ off, const double* __restrict__ w,
                                  int64_t nv, double* __restrict__ k, unsigned long long* __restrict__ flags) {
   const int lane = threadIdx.x & 31;
@@ -60,8 +62,13 @@ __global__ void k_vertex_weights(const int64_t* __restrict__ off, const double* 
       amax = fmax(amax, ax);
     }
   }
-  if (bad) atomicAdd(&flags[0], bad);
-  if (lane == 0 && amax > 0.) atomicMax(&flags[1], (unsigned long long)__double_as_longlong(amax));
+  const bool anybad = __any_sync(NIDO_FULL_MASK, bad != 0);
+  if (lane == 0) {
+    volatile unsigned long long* vf = flags;
+    if (anybad && vf[0] == 0) atomicExch(&flags[0], 1ull);
+    const unsigned long long ab = (unsigned long long)__double_as_longlong(amax);
+    if (amax > 0. && vf[1] < ab) atomicMax(&flags[1], ab);
+  }
 }
 
 // m, first stage: compute_mass_reduce_kernel<32><<<4096,32>>>
@@ -398,21 +405,15 @@ __global__ void k_tier_keys(const int64_t* __restrict__ off, int64_t nv, const i
 
 }  // namespace
 
+// k_v of the current phase; its weight flags (dcount[2..3]) are read back by
+// build_batches, which every phase runs after it
 int launch_vertex_weights(nido_graph_s* g) {
-  g->int_weights = false;
   if (g->nv == 0) return NIDO_OK;
   cudaStream_t s = g->ctx->stream;
   unsigned long long* flags = reinterpret_cast<unsigned long long*>(g->dcount + 2);
   NIDO_CUDA_TRY(cudaMemsetAsync(flags, 0, 2 * sizeof(unsigned long long), s));
   k_vertex_weights<<<grid_for(g->nv * 32, kThreads, 148 * 64), kThreads, 0, s>>>(g->off, g->w, g->nv, g->k, flags);
   NIDO_LAUNCH_CHECK();
-  unsigned long long f[2] = {0, 0};
-  NIDO_CUDA_TRY(cudaMemcpyAsync(f, flags, sizeof(f), cudaMemcpyDeviceToHost, s));
-  NIDO_CUDA_TRY(cudaStreamSynchronize(s));
-  double amax = 0.;
-  memcpy(&amax, &f[1], sizeof(amax));
-  // int32 table sums are exact when no vertex's sum of |w| reaches 2^31
-  g->int_weights = f[0] == 0 && amax < 2147483648.0;
   return NIDO_OK;
 }
 
@@ -613,7 +614,15 @@ int build_batches(nido_graph_s* g) {
     NIDO_CUDA_TRY(cudaMemcpyAsync(g->cuts.data(), dcuts, sizeof(int64_t) * (nb + 1), cudaMemcpyDeviceToHost, s));
   NIDO_CUDA_TRY(cudaMemcpyAsync(g->tier_off.data(), counts, sizeof(int64_t) * (nkeys + 1), cudaMemcpyDeviceToHost, s));
   NIDO_CUDA_TRY(cudaMemcpyAsync(&md, maxdeg, sizeof(md), cudaMemcpyDeviceToHost, s));
+  unsigned long long wf[2] = {1, 0};  // weight flags of the last k_v
+  if (nv > 0) NIDO_CUDA_TRY(cudaMemcpyAsync(wf, g->dcount + 2, sizeof(wf), cudaMemcpyDeviceToHost, s));
   NIDO_CUDA_TRY(cudaStreamSynchronize(s));
+  {
+    double amax = 0.;
+    memcpy(&amax, &wf[1], sizeof(amax));
+    // int32 table sums are exact when no vertex's sum of |w| reaches 2^31
+    g->int_weights = wf[0] == 0 && amax < 2147483648.0;
+  }
   g->max_degree = (int64_t)md;
   g->bins_valid = true;
   ++g->plan_epoch;
