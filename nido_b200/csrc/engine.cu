@@ -659,7 +659,30 @@ extern "C" int nido_get_clustering(nido_graph g, int64_t* clustering) {
   if (!tmp) return nido_set_error(NIDO_E_NOMEM, "scratch arena too small");
   k_widen<<<kGrid, 256, 0, s>>>(g->clus, g->nv0, tmp);
   NIDO_LAUNCH_CHECK();
-  NIDO_CUDA_TRY(cudaMemcpyAsync(clustering, tmp, 8 * g->nv0, cudaMemcpyDeviceToHost, s));
+  // A pageable destination (a fresh host array, say) is copied to at a
+  // fraction of the link's speed and faults its pages in one at a time; such
+  // copies go through the context's pinned buffer and are spread over the
+  // host threads.
+  const size_t bytes = 8 * (size_t)g->nv0;
+  cudaPointerAttributes pa{};
+  bool pinned = cudaPointerGetAttributes(&pa, clustering) == cudaSuccess && pa.type == cudaMemoryTypeHost;
+  if (!pinned) cudaGetLastError();
+  void* stage = nullptr;
+  if (!pinned && bytes >= ((size_t)1 << 20) && nido::pinned_buffer(g->ctx, bytes, &stage) == cudaSuccess) {
+    NIDO_CUDA_TRY(cudaMemcpyAsync(stage, tmp, bytes, cudaMemcpyDeviceToHost, s));
+    NIDO_CUDA_TRY(cudaStreamSynchronize(s));
+    const int T = std::max(1, std::min(16, omp_get_max_threads()));
+    const int64_t n = g->nv0, per = (n + T - 1) / T;
+    const int64_t* src = static_cast<const int64_t*>(stage);
+#pragma omp parallel for num_threads(T) schedule(static)
+    for (int t = 0; t < T; ++t) {
+      const int64_t lo = std::min(n, (int64_t)t * per), hi = std::min(n, lo + per);
+      if (hi > lo) memcpy(clustering + lo, src + lo, sizeof(int64_t) * (size_t)(hi - lo));
+    }
+    return NIDO_OK;
+  }
+  cudaGetLastError();
+  NIDO_CUDA_TRY(cudaMemcpyAsync(clustering, tmp, bytes, cudaMemcpyDeviceToHost, s));
   NIDO_CUDA_TRY(cudaStreamSynchronize(s));
   return NIDO_OK;
 }
