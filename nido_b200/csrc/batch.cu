@@ -587,9 +587,16 @@ extern "C" int nido_batch_run(nido_batch B, const nido_params* p, int64_t* out_c
   nido_run_stats st;
   memset(&st, 0, sizeof(st));
   const uint64_t launches0 = nido_launch_count();
-  cudaEvent_t t0, t1;
-  NIDO_CUDA_TRY(cudaEventCreate(&t0));
-  NIDO_CUDA_TRY(cudaEventCreate(&t1));
+  struct RunEvents {  // destroyed on every return, early ones included
+    cudaEvent_t t0 = nullptr, t1 = nullptr;
+    ~RunEvents() {
+      if (t0) cudaEventDestroy(t0);
+      if (t1) cudaEventDestroy(t1);
+    }
+  } re;
+  NIDO_CUDA_TRY(cudaEventCreate(&re.t0));
+  NIDO_CUDA_TRY(cudaEventCreate(&re.t1));
+  cudaEvent_t t0 = re.t0, t1 = re.t1;
   std::vector<cudaEvent_t>& ev = g->ctx->move_ev;
   while (ev.size() < 2) {
     cudaEvent_t e;
@@ -773,8 +780,6 @@ extern "C" int nido_batch_run(nido_batch B, const nido_params* p, int64_t* out_c
   NIDO_CUDA_TRY(cudaEventSynchronize(t1));
   float tot = 0.f;
   NIDO_CUDA_TRY(cudaEventElapsedTime(&tot, t0, t1));
-  cudaEventDestroy(t0);
-  cudaEventDestroy(t1);
   int64_t nerr = 0;
   NIDO_CUDA_TRY(cudaMemcpyAsync(&nerr, g->dcount + 1, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
   NIDO_CUDA_TRY(cudaStreamSynchronize(s));

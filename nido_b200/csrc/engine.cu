@@ -888,9 +888,16 @@ extern "C" int nido_run(nido_graph g, const nido_params* p, int64_t* out_comm, n
   nido_run_stats st;
   memset(&st, 0, sizeof(st));
   cudaStream_t s = g->ctx->stream;
-  cudaEvent_t t0, t1;
-  NIDO_CUDA_TRY(cudaEventCreate(&t0));
-  NIDO_CUDA_TRY(cudaEventCreate(&t1));
+  struct RunEvents {  // destroyed on every return, early ones included
+    cudaEvent_t t0 = nullptr, t1 = nullptr;
+    ~RunEvents() {
+      if (t0) cudaEventDestroy(t0);
+      if (t1) cudaEventDestroy(t1);
+    }
+  } re;
+  NIDO_CUDA_TRY(cudaEventCreate(&re.t0));
+  NIDO_CUDA_TRY(cudaEventCreate(&re.t1));
+  cudaEvent_t t0 = re.t0, t1 = re.t1;
   auto now_ms = [] {
     return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
   };
@@ -994,8 +1001,6 @@ extern "C" int nido_run(nido_graph g, const nido_params* p, int64_t* out_comm, n
   NIDO_CUDA_TRY(cudaEventSynchronize(t1));
   float tot = 0.f;
   NIDO_CUDA_TRY(cudaEventElapsedTime(&tot, t0, t1));
-  cudaEventDestroy(t0);
-  cudaEventDestroy(t1);
   st.total_ms = tot;
   st.phases = phases;
   NIDO_TRY(qt.finish());
