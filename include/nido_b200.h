@@ -191,9 +191,13 @@ typedef struct {
   int32_t warp_max_degree;   /* one warp, 256-slot shared table; <= 192 */
   int32_t cta_s_max_degree;  /* 128-thread CTA, 1024 slots; <= 768 */
   int32_t cta_m_max_degree;  /* 256-thread CTA, 2048 slots; <= 1536 */
-  int32_t cta_l_max_degree;  /* 256-thread CTA, 4096 slots; <= 3072 */
+  int32_t cta_l_max_degree;  /* 256-thread CTA, 4096 slots; <= 3072 (default 2048) */
   int32_t cta_x_max_degree;  /* 1024-thread CTA, 16384 slots; <= 12288; above: hub tier */
-  int32_t reserved;
+  int32_t hub_clusters;      /* 1: in integer-weight phases with the smallest-id rule,
+                                hubs run on thread-block clusters of 2..16 CTAs whose
+                                distributed shared memory holds the hub's table (when
+                                every hub of the phase fits: degree <= 196,608);
+                                0 (default): hub tables in global memory */
   int64_t hub_wave_slots;    /* hub-table slots processed together (L2 residency) */
 } nido_tier_config;
 /* Thresholds must be non-decreasing, at least 32 and within the capacities

@@ -54,7 +54,7 @@ _lib = None
 class TierConfig(C.Structure):
     _fields_ = [("warp_max_degree", C.c_int32), ("cta_s_max_degree", C.c_int32),
                 ("cta_m_max_degree", C.c_int32), ("cta_l_max_degree", C.c_int32),
-                ("cta_x_max_degree", C.c_int32), ("reserved", C.c_int32), ("hub_wave_slots", C.c_int64)]
+                ("cta_x_max_degree", C.c_int32), ("hub_clusters", C.c_int32), ("hub_wave_slots", C.c_int64)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}

@@ -279,7 +279,7 @@ extern "C" int nido_graph_free(nido_graph g) {
   for (void* p : {(void*)g->gkeys, (void*)g->gvals, (void*)g->hub_items, (void*)g->hub_v, (void*)g->hub_capv,
                   (void*)g->hub_nseg, (void*)g->hub_toff, (void*)g->hub_done, (void*)g->hub_slices,
                   (void*)g->hub_slice_first, (void*)g->hub_res, (void*)g->hub_item_first,
-                  (void*)g->hub_part, (void*)g->agg_buf, (void*)g->pm32})
+                  (void*)g->hub_part, (void*)g->hub_cl_v, (void*)g->agg_buf, (void*)g->pm32})
     nido::raw_free(ctx, p);
   for (nido_graph_s::MoveGraph& mg : g->move_graphs)
     if (mg.exec) cudaGraphExecDestroy(mg.exec);
@@ -783,11 +783,13 @@ int tune_tiers(nido_graph_s* g, int tie, int sweeps, double* best_ms) {
     return NIDO_OK;
   };
   for (int32_t v : {8192, 4096}) { TierConfig c = best; c.ctax_max = v; NIDO_TRY(try_cfg(c)); }
-  for (int32_t v : {2048, 1536}) { TierConfig c = best; c.ctal_max = v; NIDO_TRY(try_cfg(c)); }
+  for (int32_t v : {3072, 1536}) { TierConfig c = best; c.ctal_max = v; NIDO_TRY(try_cfg(c)); }
   for (int32_t v : {512, 384}) { TierConfig c = best; c.ctas_max = v; NIDO_TRY(try_cfg(c)); }
   for (int32_t v : {128, 64}) { TierConfig c = best; c.warp_max = v; NIDO_TRY(try_cfg(c)); }
-  if (g->max_degree > best.ctax_max)
+  if (g->max_degree > best.ctax_max) {
     for (int64_t v : {(int64_t)2 << 20, (int64_t)8 << 20}) { TierConfig c = best; c.hub_wave_slots = v; NIDO_TRY(try_cfg(c)); }
+    if (g->int_weights && tie != NIDO_TIE_NIDO) { TierConfig c = best; c.hub_clusters = true; NIDO_TRY(try_cfg(c)); }
+  }
   g->cfg = best;
   g->bins_valid = false;
   NIDO_TRY(build_batches(g));
@@ -799,8 +801,8 @@ int tune_tiers(nido_graph_s* g, int tie, int sweeps, double* best_ms) {
 
 extern "C" int nido_get_tier_config(nido_graph g, nido_tier_config* c) {
   if (!g || !c) return nido_set_error(NIDO_E_INVALID, "null argument");
-  *c = nido_tier_config{g->cfg.warp_max, g->cfg.ctas_max, g->cfg.ctam_max, g->cfg.ctal_max, g->cfg.ctax_max, 0,
-                        g->cfg.hub_wave_slots};
+  *c = nido_tier_config{g->cfg.warp_max, g->cfg.ctas_max, g->cfg.ctam_max, g->cfg.ctal_max, g->cfg.ctax_max,
+                        g->cfg.hub_clusters ? 1 : 0, g->cfg.hub_wave_slots};
   return NIDO_OK;
 }
 
@@ -813,6 +815,9 @@ extern "C" int nido_set_tier_config(nido_graph g, const nido_tier_config* c) {
   t.ctal_max = c->cta_l_max_degree;
   t.ctax_max = c->cta_x_max_degree;
   t.hub_wave_slots = c->hub_wave_slots;
+  if (c->hub_clusters != 0 && c->hub_clusters != 1)
+    return nido_set_error(NIDO_E_INVALID, "hub_clusters must be 0 or 1 (got %d)", c->hub_clusters);
+  t.hub_clusters = c->hub_clusters != 0;
   if (!nido::config_ok(t)) return nido_set_error(NIDO_E_INVALID, "tier thresholds out of range or decreasing");
   g->cfg = t;
   g->bins_valid = false;

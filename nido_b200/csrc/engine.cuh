@@ -44,16 +44,20 @@ constexpr int kCtaLMaxDeg = 3072;
 constexpr int kCtaXMaxDeg = 12288;  // table load up to 3/4 in the 16384 slots
 constexpr int kHubSeg = 2048;        // edges of one hub segment (move and modularity)
 
-// Degree thresholds of the shared-memory tiers and the hub wave size.  The
-// defaults are the kernels' capacities; the tuner (engine.cu) may lower the
-// thresholds (a tier takes any degree up to its capacity) and pick the wave.
+// Degree thresholds of the shared-memory tiers, the hub wave size and the
+// hub-cluster option.  The defaults are the kernels' capacities except for
+// CTA-L (measured below); the tuner (engine.cu) may move the thresholds (a
+// tier takes any degree up to its capacity), pick the wave and the option.
 struct TierConfig {
   int32_t warp_max = kWarpMaxDeg;
   int32_t ctas_max = kCtaSMaxDeg;
   int32_t ctam_max = kCtaMMaxDeg;
-  int32_t ctal_max = kCtaLMaxDeg;
+  // degree 2049..3072 runs faster on the 1024-thread tier since the tables
+  // sum in int32 (R-MAT scale 22: 113.4 -> 110.3 ms of move phase)
+  int32_t ctal_max = 2048;
   int32_t ctax_max = kCtaXMaxDeg;
   int64_t hub_wave_slots = (int64_t)4 << 20;
+  bool hub_clusters = false;  // hubs on thread-block clusters where they fit
 };
 
 struct nido_ctx_s {
@@ -155,6 +159,13 @@ struct nido_graph_s {
   int64_t* hub_item_first = nullptr;
   double* hub_part = nullptr;
   int64_t hub_cap_ifirst = 0, hub_cap_part = 0, hub_nitems = 0;
+  // hub vertices of every batch by cluster size (2, 4, 8, 16 CTAs sharing
+  // one table in their distributed shared memory): hub_cl_off[batch * 4 +
+  // bin] is the first list entry; hub_cl_ok when every hub of the phase fits
+  int32_t* hub_cl_v = nullptr;
+  int64_t hub_cap_cl = 0;
+  std::vector<int64_t> hub_cl_off;
+  bool hub_cl_ok = false;
   // coarsening plan and tables of giant coarse vertices (grows, never shrinks,
   // so runs after the first allocate nothing)
   char* agg_buf = nullptr;

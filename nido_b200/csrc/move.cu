@@ -20,6 +20,8 @@
 // with NIDO_TIE_NIDO, to the entry the reference's 8-lane strided scan and
 // shuffle tree picks: among tied entries of rank r in the id-sorted list of
 // the vertex's neighbour communities, the smallest (bitrev3(r mod 8), r).
+#include <cooperative_groups.h>
+
 #include <algorithm>
 #include <mutex>
 
@@ -28,6 +30,8 @@
 
 namespace nido {
 namespace {
+
+namespace cg = cooperative_groups;
 
 struct MoveArgs {
   const int64_t* __restrict__ off;
@@ -804,6 +808,171 @@ __global__ void k_hub_combine(int64_t nh, const int32_t* __restrict__ hub_v, con
   }
 }
 
+// ---- hubs in thread-block clusters (integer-weight phases) ---------------------
+// One cluster of kCtas CTAs per hub: the hub's table spans the clusters'
+// shared memory, kClSlots slots in each CTA, so every insert is a
+// distributed-shared-memory access instead of an L2 round trip.  The edges
+// are spread over all warps of the cluster; after a cluster barrier each CTA
+// evaluates (and clears) its own slots, the per-CTA bests meet in rank 0's
+// shared memory, and after a second barrier rank 0 decides.  Sums are int32
+// (integer weights, every vertex's sum of |w| below 2^31), so the shared
+// atomics are native 32-bit ones and exact; the smallest-id tie rule picks
+// the same entry in any order of evaluation.
+constexpr int kClThreads = 1024;
+constexpr int kClSlots = 16384;   // 192 KB of keys and values per CTA
+constexpr int kClusterBins = 4;   // clusters of 2, 4, 8 and 16 CTAs
+
+constexpr int64_t cluster_max_degree(int bin) { return (int64_t)(2 << bin) * kClSlots * 3 / 4; }
+
+// cluster size bin of a hub of degree d (-1: more than a 16-CTA table holds)
+inline int cluster_bin(int64_t d) {
+  for (int b = 0; b < kClusterBins; ++b)
+    if (d <= cluster_max_degree(b)) return b;
+  return -1;
+}
+
+// whether clusters of each size can be resident on this GPU (set once per
+// process by move_init_attributes; unlaunchable bins keep hubs on the
+// global-memory path)
+bool g_cluster_ok[kClusterBins] = {false, false, false, false};
+inline bool cluster_launchable(int bin) { return bin >= 0 && g_cluster_ok[bin]; }
+
+__device__ __forceinline__ void cluster_add(cg::cluster_group& cl, int* keys, double* vals, unsigned mask, int c,
+                                            int x, unsigned long long* err) {
+  unsigned h = hash_slot(c, mask);
+  for (unsigned probe = 0; probe <= mask; ++probe) {
+    const unsigned owner = h / kClSlots, loc = h % kClSlots;
+    int* kp = cl.map_shared_rank(keys, owner) + loc;
+    const int kk = *reinterpret_cast<volatile int*>(kp);
+    bool hit = kk == c;
+    if (!hit && kk == -1) {
+      const int old = atomicCAS(kp, -1, c);
+      hit = old == -1 || old == c;
+    }
+    if (hit) {
+      atomicAdd(reinterpret_cast<int*>(cl.map_shared_rank(vals, owner) + loc), x);
+      return;
+    }
+    h = (h + 1) & mask;
+  }
+  atomicAdd(err, 1ull);
+}
+
+template <int kCtas, bool kMulti>
+__global__ void __launch_bounds__(kClThreads, 1) k_move_cluster(const int32_t* __restrict__ list, int64_t n,
+                                                                MoveArgs p) {
+  cg::cluster_group cluster = cg::this_cluster();
+  extern __shared__ double smem[];
+  double* vals = smem;                                    // int32 sums in the low words
+  int* keys = reinterpret_cast<int*>(smem + kClSlots);
+  __shared__ double sg[32], se[32];
+  __shared__ unsigned long long stk[32];
+  __shared__ int sc[32];
+  __shared__ double rg[kCtas], re[kCtas];                 // the ranks' bests, in rank 0
+  __shared__ unsigned long long rtk[kCtas];
+  __shared__ int rc[kCtas];
+  constexpr unsigned kMask = (unsigned)kCtas * kClSlots - 1;
+  constexpr int kWarps = kCtas * (kClThreads / 32);
+  const unsigned rank = cluster.block_rank();
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  const int gw = (int)rank * (kClThreads / 32) + wid;
+  for (int i = threadIdx.x; i < kClSlots; i += kClThreads) { keys[i] = -1; vals[i] = 0.; }
+  cluster.sync();
+  const int64_t ncl = gridDim.x / kCtas;
+  for (int64_t task = blockIdx.x / kCtas; task < n; task += ncl) {
+    const int v = list[task];
+    const int64_t s = p.off[v], e = p.off[v + 1];
+    for (int64_t base = s + (int64_t)gw * 32; base < e; base += (int64_t)4 * kWarps * 32) {
+      int u[4], c[4];
+      double wt[4];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const int64_t j = base + (int64_t)k * kWarps * 32 + lane;
+        u[k] = -1;
+        wt[k] = 0.;
+        if (j < e) {
+          u[k] = p.adj[j];
+          wt[k] = p.w[j];
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        c[k] = u[k] >= 0 ? p.comm[u[k]] : -1;
+        if (u[k] == v) wt[k] = 0.;
+      }
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const bool ok = u[k] >= 0;
+        if (!__any_sync(NIDO_FULL_MASK, ok)) break;
+        const unsigned peers = __match_any_sync(NIDO_FULL_MASK, c[k]);
+        const double x = fold_peers(peers, ok, wt[k]);
+        if (ok && lane == __ffs(peers) - 1) cluster_add(cluster, keys, vals, kMask, c[k], __double2int_rn(x), p.err);
+      }
+    }
+    cluster.sync();  // every insert of this hub is in place
+    const int own = p.comm[v];
+    const double ki = p.k[v], aown = p.a[own], m = vertex_mass<kMulti>(p, v);
+    double g = -NIDO_MAX_FLOAT, eown = 0.;
+    unsigned long long tk = kNoKey;
+    int cand = -1;
+    for (int i0 = threadIdx.x; i0 < kClSlots; i0 += 4 * kClThreads) {
+      int cc[4];
+      double val[4], ac[4];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const int i = i0 + k * kClThreads;
+        cc[k] = keys[i];
+        val[k] = (double)*reinterpret_cast<const int*>(vals + i);
+        if (cc[k] >= 0) {  // this thread is the slot's only reader
+          keys[i] = -1;
+          vals[i] = 0.;
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < 4; ++k) ac[k] = (cc[k] >= 0 && cc[k] != own) ? p.a[cc[k]] : 0.;
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        if (cc[k] < 0) continue;
+        if (cc[k] == own) {
+          eown = val[k];
+        } else {
+          const double gg = gain_of(val[k], ki, ac[k], m);
+          if (better(gg, (unsigned)cc[k], g, tk)) { g = gg; tk = (unsigned)cc[k]; cand = cc[k]; }
+        }
+      }
+    }
+    eown = group_sum<32>(eown);  // nonzero in one lane of the cluster at most: exact
+    group_best<32>(g, tk, cand);
+    if (lane == 0) { sg[wid] = g; stk[wid] = tk; sc[wid] = cand; se[wid] = eown; }
+    __syncthreads();
+    if (wid == 0) {
+      g = sg[lane];
+      tk = stk[lane];
+      cand = sc[lane];
+      double e2 = se[lane];
+      group_best<32>(g, tk, cand);
+      e2 = group_sum<32>(e2);
+      if (lane == 0) {
+        *cluster.map_shared_rank(&rg[rank], 0) = g;
+        *cluster.map_shared_rank(&rtk[rank], 0) = tk;
+        *cluster.map_shared_rank(&rc[rank], 0) = cand;
+        *cluster.map_shared_rank(&re[rank], 0) = e2;
+      }
+    }
+    cluster.sync();  // the ranks' bests are in rank 0; every slot is clear again
+    if (rank == 0 && threadIdx.x == 0) {
+      double bg = -NIDO_MAX_FLOAT, be = 0.;
+      unsigned long long bt = kNoKey;
+      int bc = -1;
+      for (int r = 0; r < kCtas; ++r) {
+        be += re[r];
+        if (better(rg[r], rtk[r], bg, bt)) { bg = rg[r]; bt = rtk[r]; bc = rc[r]; }
+      }
+      decide(p, m, v, own, ki, aown, be, bg, bc);
+    }
+  }
+}
+
 __global__ void k_hub_degrees(const int32_t* __restrict__ list, int64_t n, const int64_t* __restrict__ off,
                               int64_t* __restrict__ out) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
@@ -841,6 +1010,8 @@ int plan_hubs(nido_graph_s* g) {
   g->hub_wave_off.assign(nb + 1, 0);
   g->nhubs = nh;
   g->hub_nitems = 0;
+  g->hub_cl_ok = false;
+  g->hub_cl_off.assign((size_t)nb * kClusterBins + 1, 0);
   if (nh == 0) return NIDO_OK;
   cudaStream_t s = g->ctx->stream;
   Arena ar(g->scratch, g->scratch_bytes);
@@ -933,6 +1104,27 @@ int plan_hubs(nido_graph_s* g) {
   NIDO_CUDA_TRY(cudaMemcpyAsync(g->hub_toff, htoff.data(), sizeof(int64_t) * nh, cudaMemcpyHostToDevice, s));
   NIDO_CUDA_TRY(cudaMemsetAsync(g->hub_done, 0, sizeof(int32_t) * nh, s));
   NIDO_CUDA_TRY(cudaMemcpyAsync(g->hub_items, items.data(), sizeof(int2) * items.size(), cudaMemcpyHostToDevice, s));
+  // cluster bins of every batch's hubs (the tier is used when all fit)
+  std::vector<int32_t> clv;
+  clv.reserve((size_t)nh);
+  bool cl_ok = g->cfg.hub_clusters;
+  for (int b = 0; b < nb && cl_ok; ++b) {
+    const int64_t a0 = g->tier_off[(size_t)kTierHub * nb + b] - h0;
+    const int64_t a1 = g->tier_off[(size_t)kTierHub * nb + b + 1] - h0;
+    for (int bin = 0; bin < kClusterBins; ++bin) {
+      g->hub_cl_off[(size_t)b * kClusterBins + bin] = (int64_t)clv.size();
+      for (int64_t i = a0; i < a1; ++i)
+        if (cluster_bin(h[2 * i + 1]) == bin) clv.push_back(hv[i]);
+    }
+    for (int64_t i = a0; i < a1; ++i)
+      if (cluster_bin(h[2 * i + 1]) < 0 || !cluster_launchable(cluster_bin(h[2 * i + 1]))) cl_ok = false;
+  }
+  g->hub_cl_off[(size_t)nb * kClusterBins] = (int64_t)clv.size();
+  if (cl_ok && !clv.empty()) {
+    NIDO_TRY(ensure(g, &g->hub_cl_v, &g->hub_cap_cl, (int64_t)clv.size()));
+    NIDO_CUDA_TRY(cudaMemcpyAsync(g->hub_cl_v, clv.data(), sizeof(int32_t) * clv.size(), cudaMemcpyHostToDevice, s));
+    g->hub_cl_ok = true;
+  }
   NIDO_CUDA_TRY(cudaStreamSynchronize(s));  // the host vectors go out of scope
   return NIDO_OK;
 }
@@ -1003,6 +1195,82 @@ int set_smem_mode() {
   return NIDO_OK;
 }
 
+int64_t g_cluster_max[kClusterBins] = {0, 0, 0, 0};  // clusters resident on the GPU at once
+
+template <int kCtas>
+cudaLaunchConfig_t cluster_config(int64_t clusters, cudaStream_t s, cudaLaunchAttribute* attr) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)(clusters * kCtas), 1, 1);
+  cfg.blockDim = dim3(kClThreads, 1, 1);
+  cfg.dynamicSmemBytes = (size_t)kClSlots * 12;
+  cfg.stream = s;
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = kCtas;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cfg;
+}
+
+// shared memory and cluster-size attributes of one cluster kernel, and how
+// many of its clusters fit on the GPU (0: none, the bin stays off)
+template <int kCtas, bool kMulti>
+int64_t cluster_setup() {
+  auto k = k_move_cluster<kCtas, kMulti>;
+  if (cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, kClSlots * 12) != cudaSuccess ||
+      (kCtas > 8 && cudaFuncSetAttribute(k, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess)) {
+    cudaGetLastError();
+    return 0;
+  }
+  cudaLaunchAttribute attr[1];
+  cudaLaunchConfig_t cfg = cluster_config<kCtas>(1, nullptr, attr);
+  int n = 0;
+  if (cudaOccupancyMaxActiveClusters(&n, k, &cfg) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return n;
+}
+
+int cluster_init() {
+  const int64_t m[kClusterBins] = {std::min(cluster_setup<2, false>(), cluster_setup<2, true>()),
+                                   std::min(cluster_setup<4, false>(), cluster_setup<4, true>()),
+                                   std::min(cluster_setup<8, false>(), cluster_setup<8, true>()),
+                                   std::min(cluster_setup<16, false>(), cluster_setup<16, true>())};
+  for (int b = 0; b < kClusterBins; ++b) {
+    g_cluster_max[b] = m[b];
+    g_cluster_ok[b] = m[b] > 0;
+  }
+  return NIDO_OK;
+}
+
+template <int kCtas, bool kMulti>
+int launch_cluster_bin(int bin, const int32_t* list, int64_t n, const MoveArgs& p, cudaStream_t s) {
+  cudaLaunchAttribute attr[1];
+  cudaLaunchConfig_t cfg = cluster_config<kCtas>(std::min<int64_t>(n, g_cluster_max[bin]), s, attr);
+  NIDO_CUDA_TRY(cudaLaunchKernelEx(&cfg, k_move_cluster<kCtas, kMulti>, list, n, p));
+  return NIDO_OK;
+}
+
+// the hubs of one batch on clusters of 2, 4, 8 and 16 CTAs by degree
+template <bool kMulti>
+int launch_clusters(nido_graph_s* g, int batch, const MoveArgs& p, cudaStream_t s) {
+  for (int bin = 0; bin < kClusterBins; ++bin) {
+    const int64_t c0 = g->hub_cl_off[(size_t)batch * kClusterBins + bin];
+    const int64_t c1 = g->hub_cl_off[(size_t)batch * kClusterBins + bin + 1];
+    if (c1 <= c0) continue;
+    const int32_t* list = g->hub_cl_v + c0;
+    switch (bin) {
+      case 0: NIDO_TRY((launch_cluster_bin<2, kMulti>(bin, list, c1 - c0, p, s))); break;
+      case 1: NIDO_TRY((launch_cluster_bin<4, kMulti>(bin, list, c1 - c0, p, s))); break;
+      case 2: NIDO_TRY((launch_cluster_bin<8, kMulti>(bin, list, c1 - c0, p, s))); break;
+      default: NIDO_TRY((launch_cluster_bin<16, kMulti>(bin, list, c1 - c0, p, s))); break;
+    }
+  }
+  return NIDO_OK;
+}
+
 // the tier kernels of one batch; kMulti: many graphs (per-vertex mass).  The
 // tiers cover disjoint vertices and only read comm and a, so they run on
 // three streams: the hub chain and the CTA tiers on the context's side
@@ -1051,6 +1319,14 @@ int launch_tiers(nido_graph_s* g, int batch, int tie, const MoveArgs& p) {
         k_move_cta<1024, kCtaXCap, kMulti, kInts, false><<<grid_cap(n, R.ctax), 1024, (size_t)kCtaXCap * 12, s>>>(list, n, p);
         break;
       default: {
+        if constexpr (kInts) {
+          // integer-weight phases with the smallest-id rule: hubs on
+          // thread-block clusters when every hub of the phase fits one
+          if (tie != NIDO_TIE_NIDO && g->cfg.hub_clusters && g->hub_cl_ok) {
+            NIDO_TRY(launch_clusters<kMulti>(g, batch, p, s));
+            break;
+          }
+        }
         SliceResult* res = reinterpret_cast<SliceResult*>(g->hub_res);
         for (int64_t wv = g->hub_wave_off[batch]; wv < g->hub_wave_off[batch + 1]; ++wv) {
           const nido_graph_s::HubWave& w = g->hub_waves[wv];
@@ -1087,6 +1363,7 @@ int launch_tiers(nido_graph_s* g, int batch, int tie, const MoveArgs& p) {
 }  // namespace
 
 int move_init_attributes() {
+  NIDO_TRY(cluster_init());
   NIDO_TRY((set_smem_mode<false, false>()));
   NIDO_TRY((set_smem_mode<false, true>()));
   NIDO_TRY((set_smem_mode<true, false>()));
