@@ -784,6 +784,7 @@ int tune_tiers(nido_graph_s* g, int tie, int sweeps, double* best_ms) {
   };
   for (int32_t v : {8192, 4096}) { TierConfig c = best; c.ctax_max = v; NIDO_TRY(try_cfg(c)); }
   for (int32_t v : {3072, 1536}) { TierConfig c = best; c.ctal_max = v; NIDO_TRY(try_cfg(c)); }
+  for (int32_t v : {1024, 768}) { TierConfig c = best; c.ctam_max = v; NIDO_TRY(try_cfg(c)); }
   for (int32_t v : {512, 384}) { TierConfig c = best; c.ctas_max = v; NIDO_TRY(try_cfg(c)); }
   for (int32_t v : {128, 64}) { TierConfig c = best; c.warp_max = v; NIDO_TRY(try_cfg(c)); }
   if (g->max_degree > best.ctax_max) {
