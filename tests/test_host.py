@@ -180,3 +180,42 @@ def test_many_graphs_packed_small(nido_lib):
     assert (u.w >= 1).all() and (u.w == np.round(u.w)).all()  # integer weights (duplicates summed)
     g5 = W.unpack(vbase, u, 5)
     assert g5.nv == V[5] and g5.off[0] == 0 and (g5.adj < V[5]).all()
+
+
+_CTYPES = {"int64_t": "c_long", "int32_t": "c_int", "double": "c_double", "uint64_t": "c_ulong"}
+
+
+def header_structs():
+    """Field (name, C type, array length) lists of the header's typedef structs."""
+    text = re.sub(r"/\*.*?\*/", "", open(HEADER).read(), flags=re.S)
+    out = {}
+    for body, name in re.findall(r"typedef struct \{(.*?)\}\s*(nido_\w+);", text, flags=re.S):
+        fields = []
+        for decl in body.split(";"):
+            m = re.match(r"\s*(const\s+)?(\w+)\s*(\*?)\s*(\w+)\s*(\[(\d+)\])?\s*$", decl)
+            if m:
+                ctype = "pointer" if m.group(3) else m.group(2)
+                fields.append((m.group(4), ctype, int(m.group(6)) if m.group(6) else 0))
+        out[name] = fields
+    return out
+
+
+@pytest.mark.parametrize("cname,pyname", [("nido_csr", "_Csr"), ("nido_params", "_Params"),
+                                          ("nido_run_stats", "RunStats"), ("nido_tier_config", "TierConfig"),
+                                          ("nido_request_info", "RequestInfo")])
+def test_ctypes_structs_match_header(nido_lib, cname, pyname):
+    """The Python mirrors of the C ABI's structs have the header's fields in
+    the header's order with the same widths, so no field is read at the
+    wrong offset."""
+    want = header_structs()[cname]
+    cls = getattr(nido_lib, pyname)
+    got = cls._fields_
+    assert [f[0] for f in got] == [f[0] for f in want], cname
+    for (name, ctype), (_, htype, n) in zip(got, want):
+        if htype == "pointer":
+            assert C.sizeof(ctype) == 8, name
+            continue
+        base = ctype._type_ if n else ctype
+        if n:
+            assert ctype._length_ == n, name
+        assert C.sizeof(base) == C.sizeof(getattr(C, _CTYPES[htype])), name
