@@ -61,6 +61,12 @@ typedef struct {
   int32_t verbose;   /* print the reference's per-loop lines to stdout */
   int32_t tune;      /* 1: autotune the degree tiers on the first phase of the
                         first run of this graph (nido_tune), then keep them */
+  double tau_phase;  /* LouvainGPU's tol_phase (louvain_gpu.hpp:20-21): a phase
+                        is coarsened when it gained more than this; used only
+                        when tau_phase_set, otherwise tau (the reference's
+                        three-argument LouvainGPU) */
+  int32_t tau_phase_set;
+  int32_t reserved;  /* must be 0 */
 } nido_params;
 
 /* Per-run statistics (the reference prints these, louvain_gpu.cpp:43-131). */
@@ -146,7 +152,8 @@ int nido_host_unregister(void* ptr);
 
 /* ---- step-level operators: GraphGPU's public methods (graph_gpu.hpp:172-241) */
 int nido_singleton_partition(nido_graph g);                  /* graph_gpu.cpp:519-536 */
-int nido_set_community_ids(nido_graph g, const int64_t* comm);/* graph_gpu.cpp:433-455 */
+int nido_set_community_ids(nido_graph g, const int64_t* comm);/* graph_gpu.cpp:433-448 */
+int nido_compute_community_weights(nido_graph g);            /* graph_gpu.cpp:450-455 */
 int nido_compute_modularity(nido_graph g, double* q);        /* graph_gpu.cpp:862-905 */
 int nido_louvain_update(nido_graph g, int32_t batch, int32_t tie_mode); /* graph_gpu.cpp:602-624 */
 int nido_update_community_weights(nido_graph g, int32_t batch);/* graph_gpu.cpp:779-791 */
@@ -169,7 +176,9 @@ int nido_dump_partition(nido_graph g, const char* path, const int64_t* new_order
  * device memory is all handed to a fixed pool).  No counterpart in the
  * reference, whose modularity cudaMallocs a partials buffer on every call.
  * Layout as in the reference: d_off[nv+1] and d_adj (int64), d_w (FP64),
- * d_comm[nv] (int64 community ids in [0, nv)), d_a[nv] community degrees
+ * all non-null when nv > 0 (a graph without edges may pass any non-null
+ * d_adj and d_w; they are not read), d_comm[nv] (int64 community ids in
+ * [0, nv)), d_a[nv] community degrees
  * a_c indexed by community id, m the mass; Q is written to d_q (device) on
  * `stream` (a cudaStream_t, NULL for the legacy default stream), without a
  * host synchronisation.  The reduction follows the reference's order, so Q
@@ -272,7 +281,9 @@ int nido_server_submit(nido_server s, const nido_csr* g, const nido_params* p, i
 int nido_server_poll(nido_server s, int64_t ticket, int32_t* state);
 /* Blocks until the request finishes (timeout_s < 0: no limit); NIDO_E_TIMEOUT
  * leaves the ticket valid.  Returns the request's own status and releases
- * the ticket. */
+ * the ticket.  One waiter per ticket: a wait on a ticket that another thread
+ * is already waiting on returns NIDO_E_INVALID at once.  Submissions and
+ * waits on other tickets may proceed from any thread meanwhile. */
 int nido_server_wait(nido_server s, int64_t ticket, double timeout_s, nido_request_info* info);
 /* budget, bytes reserved by running requests, running and queued counts */
 int nido_server_budget(nido_server s, int64_t* budget, int64_t* reserved, int32_t* running,
@@ -280,18 +291,18 @@ int nido_server_budget(nido_server s, int64_t* budget, int64_t* reserved, int32_
 /* Finishes every queued request, then stops the workers. */
 int nido_server_destroy(nido_server s);
 
-/* ---- colouring for -c (Graph::coloring, graph.cpp:651-797) ---------------------- */
+/* ---- colouring for -c (Graph::coloring, graph.cpp:548-694) ---------------------- */
 /* Jones-Plassmann-Luby colouring on the device; colors has nv entries;
  * returns the number of colours in *ncolors. Proper (no two neighbours share a
  * colour) and deterministic for a given seed. */
 int nido_color(nido_ctx ctx, const nido_csr* in, uint64_t seed, int64_t* colors,
                int64_t* ncolors);
-/* relabel by (colour, id) as graph.cpp:714-796: out gets the permuted CSR (its
+/* relabel by (colour, id) as graph.cpp:611-693: out gets the permuted CSR (its
  * arrays caller-allocated with the input sizes), new_orders[p] = old id */
 int nido_color_relabel(nido_ctx ctx, const nido_csr* in, const int64_t* colors,
                        nido_csr* out, int64_t* new_orders);
 
-/* ---- Vite binary files (graph.cpp:425-598) -------------------------------------- */
+/* ---- Vite binary files (graph.cpp:322-495) -------------------------------------- */
 int nido_read_vite(const char* path, nido_csr* out); /* arrays malloc'ed */
 int nido_write_vite(const char* path, const nido_csr* g);
 void nido_csr_free(nido_csr* g);

@@ -1,0 +1,7 @@
+// graph_gpu.hpp -- the reference's header name for its host classes, for programs
+// written against sg0/nido: everything is in nido_host.hpp (Graph,
+// Clustering, GraphGPU, LouvainGPU and the types of types.hpp).
+#ifndef NIDO_COMPAT_GRAPH_GPU_HPP_
+#define NIDO_COMPAT_GRAPH_GPU_HPP_
+#include "../nido_host.hpp"
+#endif

@@ -36,7 +36,8 @@ class _Csr(C.Structure):
 
 class _Params(C.Structure):
     _fields_ = [("nbatches", C.c_int32), ("tie_mode", C.c_int32), ("tau", C.c_double),
-                ("max_iter", C.c_int64), ("verbose", C.c_int32), ("tune", C.c_int32)]
+                ("max_iter", C.c_int64), ("verbose", C.c_int32), ("tune", C.c_int32),
+                ("tau_phase", C.c_double), ("tau_phase_set", C.c_int32), ("reserved", C.c_int32)]
 
 
 class RunStats(C.Structure):
@@ -98,6 +99,7 @@ def lib() -> C.CDLL:
             "nido_host_unregister": (C.c_int, [vp]),
             "nido_singleton_partition": (C.c_int, [vp]),
             "nido_set_community_ids": (C.c_int, [vp, _i64p]),
+            "nido_compute_community_weights": (C.c_int, [vp]),
             "nido_compute_modularity": (C.c_int, [vp, _f64p]),
             "nido_louvain_update": (C.c_int, [vp, C.c_int32, C.c_int32]),
             "nido_update_community_weights": (C.c_int, [vp, C.c_int32]),
@@ -358,6 +360,9 @@ class Graph:
         comm = np.ascontiguousarray(comm, dtype=np.int64)
         _check(lib().nido_set_community_ids(self.h, _p64(comm)))
 
+    def compute_community_weights(self):
+        _check(lib().nido_compute_community_weights(self.h))
+
     def compute_modularity(self) -> float:
         q = C.c_double()
         _check(lib().nido_compute_modularity(self.h, C.byref(q)))
@@ -523,10 +528,15 @@ class Server:
     def wait(self, ticket: int, timeout: float = -1.0):
         info = RequestInfo()
         rc = lib().nido_server_wait(self.h, ticket, timeout, C.byref(info))
-        if rc == -6:  # NIDO_E_TIMEOUT: still pending
-            _check(rc)
-        _, out = self._keep.pop(ticket)
+        if rc != 0:
+            st = C.c_int32()
+            if lib().nido_server_poll(self.h, ticket, C.byref(st)) == 0:
+                # still live (timed out, or another thread waits on it): the
+                # engine may still use its buffers
+                _check(rc)
+        kept = self._keep.pop(ticket, None)
         _check(rc)
+        out = kept[1]
         return out, info
 
     def budget(self):

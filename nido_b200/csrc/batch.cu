@@ -607,6 +607,7 @@ extern "C" int nido_batch_run(nido_batch B, const nido_params* p, int64_t* out_c
   NIDO_TRY(batch_reset(B));
   const int ng = B->ng, nb = g->nbatches;
   const double tau = p->tau;
+  const double tau_phase = p->tau_phase_set ? p->tau_phase : p->tau;
   std::vector<int64_t> base(B->vbase), edges(ng);
   std::vector<int32_t> fin(ng, 0), flags(ng);
   // graphs whose final clustering is written to outc (empty graphs have none)
@@ -731,7 +732,7 @@ extern "C" int nido_batch_run(nido_batch B, const nido_params* p, int64_t* out_c
     }
     // phase end: aggregate the graphs that gained more than tau
     NIDO_CUDA_TRY(cudaMemsetAsync(B->counters, 0, sizeof(int64_t) * 4, s));
-    k_phase_end<<<grid_for(np, 128), 128, 0, s>>>(B->plist, np, B->Q, B->Qold, tau, B->gagg, B->gfin, B->phases,
+    k_phase_end<<<grid_for(np, 128), 128, 0, s>>>(B->plist, np, B->Q, B->Qold, tau_phase, B->gagg, B->gfin, B->phases,
                                                   reinterpret_cast<unsigned long long*>(B->counters));
     NIDO_LAUNCH_CHECK();
     NIDO_CUDA_TRY(cudaMemcpyAsync(cnt, B->counters, sizeof(cnt), cudaMemcpyDeviceToHost, s));

@@ -1,8 +1,8 @@
-// color.cu -- colouring for -c (Graph::coloring, graph.cpp:651-797).
+// color.cu -- colouring for -c (Graph::coloring, graph.cpp:548-694).
 //
 // The reference colours with one racy parallel greedy pass over random
-// priorities (graph.cpp:675-709) and then relabels the CSR so colour classes
-// are contiguous, ordered by (colour, vertex id) (graph.cpp:714-796).  Here
+// priorities (graph.cpp:572-606) and then relabels the CSR so colour classes
+// are contiguous, ordered by (colour, vertex id) (graph.cpp:611-693).  Here
 // the colouring is Jones-Plassmann-Luby on the device: in every round each
 // uncoloured vertex whose (hashed priority, id) beats all uncoloured
 // neighbours takes the smallest colour unused by its neighbours.  The result

@@ -36,7 +36,9 @@ size_t block_size(size_t bytes) {
 }  // namespace
 
 cudaError_t raw_alloc(nido_ctx_s* ctx, void** p, size_t bytes) {
-  if (ctx->async_alloc) return cudaMallocAsync(p, bytes, ctx->stream);
+  if (ctx->async_alloc)
+    return ctx->pool ? cudaMallocFromPoolAsync(p, bytes, ctx->pool, ctx->stream)
+                     : cudaMallocAsync(p, bytes, ctx->stream);
   const size_t b = block_size(bytes);
   auto it = ctx->free_blocks.lower_bound(b);
   if (it != ctx->free_blocks.end() && it->first <= 2 * b) {
@@ -585,6 +587,12 @@ extern "C" int nido_set_community_ids(nido_graph g, const int64_t* comm) {
   return NIDO_OK;
 }
 
+extern "C" int nido_compute_community_weights(nido_graph g) {
+  if (!g) return nido_set_error(NIDO_E_INVALID, "null graph");
+  NIDO_CUDA_TRY(cudaSetDevice(g->ctx->device));
+  return nido::launch_set_comm(g);
+}
+
 extern "C" int nido_compute_modularity(nido_graph g, double* q) {
   if (!g || !q) return nido_set_error(NIDO_E_INVALID, "null argument");
   return nido::launch_modularity(g, q);
@@ -929,6 +937,7 @@ extern "C" int nido_run(nido_graph g, const nido_params* p, int64_t* out_comm, n
   NIDO_TRY(reset_graph(g));
   lap(0);
   const double tau = p->tau;
+  const double tau_phase = p->tau_phase_set ? p->tau_phase : p->tau;
   bool done = false;
   int64_t phases = 0;
   while (!done && phases < 200) {
@@ -987,7 +996,7 @@ extern "C" int nido_run(nido_graph g, const nido_params* p, int64_t* out_comm, n
       if (loops >= p->max_iter) printf("Exceed maximum loop number\n");
       printf("Final Q: %g\n", Q);
     }
-    if (Q - Q_old > tau) {
+    if (Q - Q_old > tau_phase) {
       int d = 0;
       lap(1);
       NIDO_TRY(at.begin(s));

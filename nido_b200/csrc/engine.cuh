@@ -73,10 +73,13 @@ struct nido_ctx_s {
   cudaStream_t aux[2] = {nullptr, nullptr};
   cudaEvent_t fork_ev = nullptr;
   cudaEvent_t join_ev[2] = {nullptr, nullptr};
-  // stream-ordered allocation (cudaMallocAsync / cudaFreeAsync on the
+  // stream-ordered allocation (cudaMallocFromPoolAsync / cudaFreeAsync on the
   // context's stream): allocating or freeing then does not wait for the work
-  // of other contexts on the same GPU
+  // of other contexts on the same GPU.  The pool is the owner's (the serving
+  // loop creates one for its workers), so the device's default pool and its
+  // settings are left alone.
   bool async_alloc = false;
+  cudaMemPool_t pool = nullptr;
   // otherwise blocks come from cudaMalloc and are kept for reuse when freed
   // (raw_alloc / raw_free): free blocks by size, the size of every block in
   // use, and the bytes held in free blocks

@@ -1,12 +1,12 @@
 // host_io.cpp -- Vite binary graph files and library-wide error state.
 //
-// File layout (graph.cpp:444-498): int64 NV, int64 NE, int64 offsets[NV+1],
+// File layout (graph.cpp:341-395): int64 NV, int64 NE, int64 offsets[NV+1],
 // then {int64 tail; double weight} records (types.hpp:49-55).  As in the
-// reference's first-touch read path (graph.cpp:500-538, always compiled in by
+// reference's first-touch read path (graph.cpp:397-435, always compiled in by
 // its Makefile) the records are read right after the offsets, for
 // offsets[NV]-offsets[0] records; a header NE that disagrees is reported with
-// the reference's message (graph.cpp:479-485) and the offsets win; offsets
-// are rebased to start at 0 (graph.cpp:573-575).
+// the reference's message (graph.cpp:376-382) and the offsets win; offsets
+// are rebased to start at 0 (graph.cpp:470-472).
 #include <stdarg.h>
 #include <stdio.h>
 #include <stdlib.h>

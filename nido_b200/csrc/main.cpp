@@ -71,14 +71,16 @@ int main(int argc, char** argv) {
     new_orders = graph.coloring(ctx);
     printf("Coloring Time: %g s\n", omp_get_wtime() - t0);
     GraphGPU graph_gpu(&graph, nbatches, ctx);
-    LouvainGPU louvain(maxLoops, tau, nbatches, tie);
+    graph_gpu.set_tie_rule(tie);
+    LouvainGPU louvain(maxLoops, tau, nbatches);
     louvain.run(&graph_gpu);
     if (output_communities) graph_gpu.dump_partition(outFileName, new_orders);
   } else {  // the file streams to the device
     GraphGPU graph_gpu(inputFileName, nbatches, ctx);
+    graph_gpu.set_tie_rule(tie);
     printf("#Batches: %d\n#Threshold: %g\nMax #iterations: %lld\n#NGPUs: 1\n", nbatches, tau, maxLoops);
     printf("--------------------------------------\n");
-    LouvainGPU louvain(maxLoops, tau, nbatches, tie);
+    LouvainGPU louvain(maxLoops, tau, nbatches);
     louvain.run(&graph_gpu);
     if (output_communities) graph_gpu.dump_partition(outFileName, new_orders);
   }

@@ -104,7 +104,9 @@ int scratch_for_current_device(double** out) {
 extern "C" int nido_modularity_noalloc(void* stream, int64_t nv, const int64_t* d_off, const int64_t* d_adj,
                                        const double* d_w, const int64_t* d_comm, const double* d_a, double m,
                                        double* d_q) {
-  if (nv < 0 || !d_q || (nv > 0 && (!d_off || !d_comm || !d_a)))
+  // every array the kernels may read must be given once there are vertices;
+  // a caller whose graph has no edges passes any non-null d_adj and d_w
+  if (nv < 0 || !d_q || (nv > 0 && (!d_off || !d_adj || !d_w || !d_comm || !d_a)))
     return nido_set_error(NIDO_E_INVALID, "nido_modularity_noalloc: bad arguments");
   if (nv > kNoallocMaxVertices)
     return nido_set_error(NIDO_E_TOO_LARGE, "nido_modularity_noalloc: %lld vertices exceed the limit of %lld",

@@ -42,6 +42,7 @@ struct Request {
   int64_t* out = nullptr;
   int64_t bytes = 0;
   int state = 0;  // 0 queued, 1 running, 2 finished
+  bool claimed = false;  // a nido_server_wait is blocked on it
   nido_request_info info{};
   std::string err;
   double t_submit = 0, t_start = 0;
@@ -62,6 +63,10 @@ struct nido_server_s {
   int64_t next_id = 1;
   int running = 0;
   bool stop = false;
+  // the workers' stream-ordered allocations come from this pool, whose
+  // release threshold keeps freed blocks for the next request; the device's
+  // default pool (and every other allocator in the process) is untouched
+  cudaMemPool_t pool = nullptr;
 };
 
 namespace {
@@ -144,15 +149,28 @@ extern "C" int nido_server_create(int device, size_t hbm_budget_bytes, int32_t n
   NIDO_CUDA_TRY(cudaSetDevice(device));
   size_t freeb = 0, totalb = 0;
   NIDO_CUDA_TRY(cudaMemGetInfo(&freeb, &totalb));
-  // freed blocks stay in the device's pool for the next request instead of
-  // going back to the driver at every synchronization (process-local setting)
-  cudaMemPool_t pool;
-  NIDO_CUDA_TRY(cudaDeviceGetDefaultMemPool(&pool, device));
+  // freed blocks stay in the server's own pool for the next request instead
+  // of going back to the driver at every synchronization
+  cudaMemPoolProps props = {};
+  props.allocType = cudaMemAllocationTypePinned;
+  props.handleTypes = cudaMemHandleTypeNone;
+  props.location.type = cudaMemLocationTypeDevice;
+  props.location.id = device;
+  cudaMemPool_t pool = nullptr;
+  NIDO_CUDA_TRY(cudaMemPoolCreate(&pool, &props));
   uint64_t keep = UINT64_MAX;
-  NIDO_CUDA_TRY(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
+  const cudaError_t pe = cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+  if (pe != cudaSuccess) {
+    cudaMemPoolDestroy(pool);
+    return nido_set_error(NIDO_E_CUDA, "cudaMemPoolSetAttribute failed: %s", cudaGetErrorString(pe));
+  }
   nido_server S = new (std::nothrow) nido_server_s();
-  if (!S) return nido_set_error(NIDO_E_NOMEM, "host allocation failed");
+  if (!S) {
+    cudaMemPoolDestroy(pool);
+    return nido_set_error(NIDO_E_NOMEM, "host allocation failed");
+  }
   S->device = device;
+  S->pool = pool;
   const int64_t cap = (int64_t)freeb - ((int64_t)1 << 30);  // keep 1 GiB for the runtime
   S->budget = hbm_budget_bytes ? std::min<int64_t>((int64_t)hbm_budget_bytes, cap) : cap;
   for (int i = 0; i < nworkers; ++i) {
@@ -160,10 +178,12 @@ extern "C" int nido_server_create(int device, size_t hbm_budget_bytes, int32_t n
     const int st = nido_ctx_create(device, 0, &c);
     if (st != NIDO_OK) {
       for (nido_ctx x : S->ctxs) nido_ctx_destroy(x);
+      cudaMemPoolDestroy(S->pool);
       delete S;
       return st;
     }
     c->async_alloc = true;
+    c->pool = S->pool;
     S->ctxs.push_back(c);
   }
   for (int i = 0; i < nworkers; ++i) S->workers.emplace_back(worker_loop, S, i);
@@ -230,13 +250,21 @@ extern "C" int nido_server_wait(nido_server S, int64_t ticket, double timeout_s,
   auto it = S->live.find(ticket);
   if (it == S->live.end()) return nido_set_error(NIDO_E_INVALID, "unknown ticket %lld", (long long)ticket);
   Request* r = it->second;
+  // one waiter per ticket: the waiter that returns frees the request, so a
+  // second one would be left reading freed memory
+  if (r->claimed)
+    return nido_set_error(NIDO_E_INVALID, "ticket %lld is already being waited on", (long long)ticket);
+  r->claimed = true;
   const auto pred = [&] { return r->state == 2; };
   if (timeout_s < 0) {
     S->cv_done.wait(lk, pred);
   } else if (!S->cv_done.wait_for(lk, std::chrono::duration<double>(timeout_s), pred)) {
+    r->claimed = false;
     return nido_set_error(NIDO_E_TIMEOUT, "request %lld still running", (long long)ticket);
   }
-  S->live.erase(it);
+  // submissions made while this thread waited may have rehashed the map:
+  // erase by key, not through the iterator taken before the wait
+  S->live.erase(ticket);
   lk.unlock();
   if (info) *info = r->info;
   const int rc = r->info.status;
@@ -255,6 +283,10 @@ extern "C" int nido_server_destroy(nido_server S) {
   for (std::thread& t : S->workers) t.join();
   for (auto& kv : S->live) delete kv.second;
   for (nido_ctx c : S->ctxs) nido_ctx_destroy(c);
+  if (S->pool) {
+    cudaSetDevice(S->device);
+    cudaMemPoolDestroy(S->pool);
+  }
   delete S;
   return NIDO_OK;
 }

@@ -25,10 +25,10 @@ static const double kMaxFloat = 1.0E+308;  // cuda_wrapper.hpp:94 (MAX_FLOAT)
 extern "C" void orc_free(void* p) { free(p); }
 
 // ---------------------------------------------------------------------------
-// Vite binary reader.  graph.cpp:425-598.  With GRAPH_FT_LOAD defined (the
+// Vite binary reader.  graph.cpp:322-495.  With GRAPH_FT_LOAD defined (the
 // reference Makefile always defines it) the edge records are read starting
 // right after the offsets, for indices[nv]-indices[0] records (graph.cpp:
-// 500-538); offsets are then rebased to start at 0 (graph.cpp:573-575).
+// 397-435); offsets are then rebased to start at 0 (graph.cpp:470-472).
 extern "C" int orc_read_vite(const char* path, int64_t* nv_out, int64_t* ne_out,
                              int64_t** off_out, int64_t** adj_out, double** w_out) {
   FILE* f = fopen(path, "rb");
@@ -375,7 +375,7 @@ extern "C" int64_t orc_coarsen(int64_t nv, const int64_t* off, const int64_t* ad
 }
 
 // ---------------------------------------------------------------------------
-// Colour relabel (graph.cpp:714-796).
+// Colour relabel (graph.cpp:611-693).
 extern "C" void orc_color_relabel(int64_t nv, const int64_t* off, const int64_t* adj,
                                   const double* w, const int64_t* colors, int64_t* new_orders,
                                   int64_t* noff, int64_t* nadj, double* nw) {
@@ -397,7 +397,7 @@ extern "C" void orc_color_relabel(int64_t nv, const int64_t* off, const int64_t*
   }
 }
 
-// nido's colouring loop on one thread (graph.cpp:651-709).
+// nido's colouring loop on one thread (graph.cpp:548-606).
 extern "C" void orc_color_nido_seq(int64_t nv, const int64_t* off, const int64_t* adj,
                                    int64_t* colors) {
   std::vector<int64_t> prio(nv);

@@ -30,7 +30,7 @@ extern "C" {
 #define ORC_TIE_SMALLEST_ID 0 /* smallest community id among equal gains */
 #define ORC_TIE_NIDO 1        /* nido's 8-lane strided scan + shuffle tree (graph_cuda.cu:1493-1526) */
 
-/* Vite binary reader (graph.cpp:425-598 with GRAPH_FT_LOAD defined). Arrays are
+/* Vite binary reader (graph.cpp:322-495 with GRAPH_FT_LOAD defined). Arrays are
  * malloc'ed; release with orc_free.  Returns 0, or -1 when the file cannot be
  * opened or is truncated. */
 int orc_read_vite(const char* path, int64_t* nv, int64_t* ne, int64_t** off,
@@ -83,13 +83,13 @@ int64_t orc_coarsen(int64_t nv, const int64_t* off, const int64_t* adj, const do
                     const int64_t* comm, int64_t* newid, int64_t** coff, int64_t** cadj,
                     double** cw, int64_t* cne);
 
-/* Colour-class relabel of the CSR (graph.cpp:714-796): new vertex p is old
+/* Colour-class relabel of the CSR (graph.cpp:611-693): new vertex p is old
  * vertex new_orders[p], vertices ordered by (colour, old id).  Output arrays
  * are caller-allocated with the input sizes. */
 void orc_color_relabel(int64_t nv, const int64_t* off, const int64_t* adj, const double* w,
                        const int64_t* colors, int64_t* new_orders, int64_t* noff,
                        int64_t* nadj, double* nw);
-/* nido's greedy colouring run on one thread (graph.cpp:651-709): priorities
+/* nido's greedy colouring run on one thread (graph.cpp:548-606): priorities
  * from std::mt19937_64(1) and uniform_int_distribution(0, 4*nv). */
 void orc_color_nido_seq(int64_t nv, const int64_t* off, const int64_t* adj, int64_t* colors);
 

@@ -12,10 +12,20 @@ library's seeded generators, so the script regenerates exactly the same
 graphs everywhere.
 
     python tests/golden/make_ref_fixtures.py --out tests/golden
+    python tests/golden/make_ref_fixtures.py --configs c1,c2 --out tests/golden
+
+--configs records whole reference runs on the benchmark configurations at
+their full size (c1: planted partition, 65,536 vertices, U[0.5,1.5] weights,
+-b 1; c2: R-MAT scale 22, unit weights, -b 2) into <out>/configs/<name>.json:
+every phase's final Q and every loop's Q (17 digits), loop counts, the
+number of communities and the sha256 of the partition file; c1 also keeps
+the whole partition (<name>_partition.npz).
 """
 from __future__ import annotations
 
 import argparse
+import hashlib
+import json
 import os
 import re
 import subprocess
@@ -83,11 +93,57 @@ def read_scalars(d):
     return vals
 
 
+# benchmark configurations recorded at full size: (workload, -b)
+CONFIGS = {"c1": ("planted", 1), "c2": ("rmat22", 2)}
+
+
+def parse_run(out: str):
+    """Per-phase final Q, per-phase loop Q lists and loop counts from the
+    reference's stdout (louvain_gpu.cpp:30-131 with 17-digit printing)."""
+    phases = []
+    for block in out.split("PHASE #")[1:]:
+        loops = re.findall(r"^(\d+) \t(\S+) \t(\S+)$", block, flags=re.M)
+        fq = re.search(r"Final Q: (\S+)", block)
+        phases.append({"loop_q": [q for i, q, _ in loops if int(i) > 0],
+                       "start_q": next((q for i, q, _ in loops if int(i) == 0), None),
+                       "final_q": fq.group(1) if fq else None})
+    return phases
+
+
+def record_configs(out_dir: str, names: list[str]):
+    from nido_b200 import workloads
+    os.makedirs(os.path.join(out_dir, "configs"), exist_ok=True)
+    tmp = tempfile.mkdtemp()
+    for name in names:
+        wl, nb = CONFIGS[name]
+        g = workloads.single_graph(wl)
+        path = os.path.join(tmp, name + ".bin")
+        capi.write_vite(path, g)
+        part = os.path.join(tmp, name + "_part.txt")
+        out = run([HARNESS, "run", path, str(nb), "1e-06", "500", part])
+        raw = open(part, "rb").read()
+        labels = np.array(raw.split(), dtype=np.int64)
+        rec = {"config": name, "workload": wl, "nv": g.nv, "ne": g.ne, "nbatches": nb, "tau": 1e-6,
+               "max_iter": 500, "phases": parse_run(out), "ncommunities": int(labels.max()) + 1 if len(labels) else 0,
+               "partition_sha256": hashlib.sha256(raw).hexdigest(),
+               "recorded_with": "oracle/_ref/ref_harness run (the unmodified reference's GraphGPU + LouvainGPU)"}
+        with open(os.path.join(out_dir, "configs", name + ".json"), "w") as f:
+            json.dump(rec, f, indent=1)
+        if name == "c1":
+            np.savez_compressed(os.path.join(out_dir, "configs", name + "_partition.npz"), partition=labels)
+        os.remove(path)
+        print(name, g.nv, g.ne, "phases", len(rec["phases"]), "final Q", rec["phases"][-1]["final_q"], flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=os.path.join(ROOT, "tests", "golden"))
+    ap.add_argument("--configs", default="", help="comma-separated: record whole runs of these configurations")
     args = ap.parse_args()
     os.makedirs(args.out, exist_ok=True)
+    if args.configs:
+        record_configs(args.out, [c for c in args.configs.split(",") if c])
+        return
     tmp = tempfile.mkdtemp()
     for name, g in cases().items():
         path = os.path.join(tmp, name + ".bin")

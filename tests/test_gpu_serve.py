@@ -107,3 +107,32 @@ def test_wait_timeout_keeps_ticket(nido_lib):
         a, ia = srv.wait(t1)
         b, ib = srv.wait(t2)
         assert np.array_equal(a, b) and ib.queue_ms >= ia.run_ms * 0.5
+
+
+def test_submit_while_another_thread_waits(nido_lib, ctx):
+    """A thread blocked in wait() while the main thread submits many more
+    requests (which grows the server's ticket table) gets its own result,
+    and a second wait on the same ticket is refused instead of racing the
+    first waiter for the request."""
+    big = nido_lib.gen_rmat(1 << 20, 16 << 20, wmode=nido_lib.W_INT8, seed=9)
+    small = [nido_lib.gen_planted(8, 16, 6.0, 0.8, nido_lib.W_INT8, 300 + i) for i in range(64)]
+    with nido_lib.Graph(ctx, big, 2) as g:
+        want_big, _ = g.run()
+    with nido_lib.Server(0, 0, workers=1) as srv:
+        t0 = srv.submit(big)  # the big request below queues behind this one
+        tb = srv.submit(big)
+        box = {}
+        th = threading.Thread(target=lambda: box.update(res=srv.wait(tb)))
+        th.start()
+        time.sleep(0.05)  # the waiter is blocked on the queued request by now
+        with pytest.raises(nido_lib.NidoError) as e:
+            srv.wait(tb, timeout=5.0)
+        assert e.value.code == -1  # NIDO_E_INVALID: one waiter per ticket
+        ts = [srv.submit(G) for G in small]
+        outs = [srv.wait(t) for t in ts]
+        th.join()
+        srv.wait(t0)
+    out, info = box["res"]
+    assert info.status == 0 and np.array_equal(out, want_big)
+    for G, (o, i) in zip(small, outs):
+        assert i.status == 0 and len(o) == G.nv

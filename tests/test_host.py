@@ -39,6 +39,25 @@ def test_no_device_is_an_error_not_a_fallback(nido_lib):
     assert e.value.code == -7  # NIDO_E_NODEVICE
 
 
+def test_noalloc_argument_checks_without_a_device(nido_lib):
+    """nido_modularity_noalloc checks its arguments before any CUDA call, so
+    the refusals are tested here, where no GPU exists and no pointer can be
+    dereferenced: a negative size, each missing array once there are
+    vertices, and more vertices than the fixed scratch array covers."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present: argument refusals are tested only where no kernel can run")
+    lib = nido_lib.lib()
+    fake = [C.c_void_p(0x1000 * (i + 1)) for i in range(6)]  # never dereferenced: no device here
+    assert lib.nido_modularity_noalloc(None, -1, *fake[:5], 1.0, fake[5]) == -1
+    for missing in range(6):
+        args = list(fake)
+        args[missing] = None
+        assert lib.nido_modularity_noalloc(None, 4, *args[:5], 1.0, args[5]) == -1, missing
+    st = lib.nido_modularity_noalloc(None, (1 << 31) + 5, *fake[:5], 1.0, fake[5])
+    assert st == -5 and b"exceed" in lib.nido_last_error()
+
+
 def test_vite_round_trip_and_errors(nido_lib, tmp_path):
     d = load_golden("selfloop_int")
     g = nido_lib.Csr(d["off"], d["adj"], d["w"])

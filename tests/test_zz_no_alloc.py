@@ -28,7 +28,7 @@ def _reference_q(capi, ctx, G, comm):
 
 
 @pytest.mark.parametrize("wmode,exact", [(3, True), (2, False)])
-def test_noalloc_matches_allocating_entry_point(nido_lib, ctx, wmode, exact):
+def test_noalloc_matches_allocating_entry_point(nido_lib, ctx, orc, wmode, exact):
     import torch
 
     capi = nido_lib
@@ -54,16 +54,33 @@ def test_noalloc_matches_allocating_entry_point(nido_lib, ctx, wmode, exact):
         assert st == 0, capi.lib().nido_last_error()
         torch.cuda.synchronize()
         q = float(d_q.item())
+        # and directly against the CPU oracle's modularity of the same inputs
+        q_orc = orc.modularity(G.off, G.adj, G.w, comm, a, m)
         if exact:
             assert np.float64(q).view(np.uint64) == np.float64(q_ref).view(np.uint64), (call, q, q_ref)
+            assert np.float64(q).view(np.uint64) == np.float64(q_orc).view(np.uint64), (call, q, q_orc)
         else:
             assert abs(q - q_ref) <= 1e-12 * abs(q_ref), (call, q, q_ref)
+            assert abs(q - q_orc) <= 1e-12 * abs(q_orc), (call, q, q_orc)
 
 
-def test_noalloc_rejects_bad_sizes(nido_lib, ctx):
+def test_noalloc_graph_without_edges(nido_lib, ctx):
+    """Four isolated vertices: Q = 0.  The argument checks (null arrays, too
+    many vertices) are tested without a GPU in test_host.py, so no call here
+    hands the kernels a pointer they may not read."""
+    import torch
+
     lib = nido_lib.lib()
-    assert lib.nido_modularity_noalloc(None, -1, None, None, None, None, None, 1.0, None) != 0
-    big = (1 << 31) + 5
-    one = C.c_void_p(16)  # never dereferenced: the size check comes first
-    st = lib.nido_modularity_noalloc(None, big, one, one, one, one, one, 1.0, one)
-    assert st == -5 and b"exceed" in lib.nido_last_error()
+    dev = torch.device("cuda", 0)
+    nv = 4
+    off = torch.zeros(nv + 1, dtype=torch.int64, device=dev)
+    adj = torch.zeros(1, dtype=torch.int64, device=dev)
+    w = torch.zeros(1, dtype=torch.float64, device=dev)
+    comm = torch.arange(nv, dtype=torch.int64, device=dev)
+    a = torch.zeros(nv, dtype=torch.float64, device=dev)
+    q = torch.full((1,), 7.0, dtype=torch.float64, device=dev)
+    p = lambda t: C.c_void_p(t.data_ptr())  # noqa: E731
+    torch.cuda.synchronize()
+    assert lib.nido_modularity_noalloc(None, nv, p(off), p(adj), p(w), p(comm), p(a), 1.0, p(q)) == 0
+    torch.cuda.synchronize()
+    assert float(q.item()) == 0.0
