@@ -1,22 +1,26 @@
 #!/usr/bin/env python
 """Benchmark: whole Louvain runs on one B200 per rank, nido's options.
 
-Default workload (one GPU): "Plain Louvain drop-in on one R-MAT graph":
-R-MAT scale 22 (4,194,304 vertices), edge factor 16, (a,b,c,d) =
-(0.57,0.19,0.19,0.05), symmetrised, self-loops and duplicates removed, weights
-1.0, seed 2, nido defaults -b 2 -t 1e-6 -i 500.  A step is one whole Louvain
-run (all phases, coarsening included) from the graph resident in HBM.
+Default workload (one GPU): the many-graph batch the metric is quoted on
+("graphs/s, p99 latency batched vs plain"): 4,096 independent graphs, vertex
+counts log-uniform in [100, 1e6] scaled to a total of 1.5e9 directed edges,
+half SBM and half R-MAT, average degree U[8, 64], integer weights U{1..8} as
+FP64, seed 4, nido defaults -b 2 -t 1e-6 -i 500.  A step is one batched run of
+every graph to completion (all phases, coarsening included) from the packed
+CSR resident in HBM.  The same line carries the plain comparison (the same
+engine one graph at a time on a systematic sample of the graphs) and the
+serving replay's p50/p99 latency (Poisson arrivals of the serving workload).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                  [--workload rmat22|planted|sbm]
+                  [--workload many|serve|rmat22|planted|sbm]
 
 Prints one JSON line.  `value` is graphs/s over all ranks from CUDA events on
 the engine's stream; `e2e` is the same metric through the public C ABI with
 host buffers (pinned H2D upload of the CSR, run, D2H of the partition inside
 the timed region).  `roofline` covers the move phase (all degree-tier kernels
 of a sweep): algorithmic bytes 16*E + 32*V per sweep (int32 ids, FP64
-weights) over the CUDA-event time of the move kernels.  For N > 1 the ranks
-are independent replicas (no collective on the data path).
+weights) over the device time of the move kernels.  For N > 1 the ranks are
+independent replicas (no collective on the data path).
 """
 from __future__ import annotations
 
@@ -69,6 +73,23 @@ WORKLOADS = {
                       "2.5, 16..65,536, 70% intra) / R-MAT (0.57,0.19,0.19,0.05), average degree U[8,64], "
                       "integer weights U{1..8} as FP64, seed 4", nbatches=2, tau=1e-6),
 }
+
+
+def config_of(args, wl, world):
+    """The workload's description: the same keys and values on both arms."""
+    c = {"workload": args.workload, "graph": wl["desc"], "nbatches": wl["nbatches"], "tau": wl["tau"],
+         "max_iter": 500, "parallelism": f"replicas x{world}",
+         "l2": ("CSR of 24 MB fits in L2; runs are not flushed" if args.workload == "planted"
+                else "inputs larger than L2 (126 MB): no flush needed")}
+    if args.workload == "many":
+        c["ngraphs"] = args.many_graphs
+        c["edge_cap"] = args.many_edges
+        if args.many_graphs != 4096 or args.many_edges != 1.5e9:
+            c["graph"] += f" [reduced: {args.many_graphs} graphs, {args.many_edges:.3g} edge cap]"
+    if args.workload == "serve":
+        c.update(requests=args.serve_requests, rate_per_s=args.serve_rate, vmax=args.serve_vmax,
+                 workers=args.serve_workers, hbm_budget_gb=args.serve_budget_gb)
+    return c
 
 
 def make_graph(capi, name):
@@ -269,9 +290,8 @@ def run_ours(args, world, rank, local):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic", "impl": "ours",
-        "config": {"workload": args.workload, "graph": wl["desc"], "nv": G.nv, "ne": G.ne,
-                   "nbatches": wl["nbatches"], "tau": wl["tau"], "ids": "int32 on device",
-                   "parallelism": f"replicas x{world}", "l2": "inputs larger than L2 (CSR 12 B/edge)"},
+        "config": config_of(args, wl, world),
+        "graph_size": {"nv": G.nv, "ne": G.ne}, "device_layout": "int32 ids, int64 offsets, FP64 weights",
         "edges_scanned_per_s": world * edges_per_run * args.steps / sec,
         "move_sweeps_per_run": sweeps / args.steps, "final_q": final_q,
         "breakdown_ms_per_run": breakdown,
@@ -380,22 +400,22 @@ def run_many(args, world, rank, local):
                "sample": f"CPU oracle (port of the reference's algorithm), whole runs of {done} of the "
                          f"sampled graphs ({t_cpu:.1f} s)"}
     ctx.close()
+    serving = None
+    if not args.no_serve and world == 1:
+        # the metric's latency half: the serving workload's Poisson replay
+        serving = serve_replay(args, local)
     if rank != 0:
         return None
     pk, pk_kind = peaks()
     achieved = move_bytes / (move_ms * 1e-3) / 1e9 if move_ms > 0 else 0.0
     sec = ms_max * 1e-3
-    desc = wl["desc"]
-    if args.many_graphs != 4096 or args.many_edges != 1.5e9:
-        desc += f" [reduced: {args.many_graphs} graphs, {args.many_edges:.3g} edge cap]"
     return {
         "metric": "graphs/s", "value": world * ng * args.steps / sec, "unit": "graphs/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max / args.steps,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic", "impl": "ours",
-        "config": {"workload": "many", "graph": desc, "ngraphs": ng, "nv": U.nv, "ne": U.ne,
-                   "nbatches": wl["nbatches"], "tau": wl["tau"], "parallelism": f"replicas x{world}",
-                   "l2": "inputs larger than L2", "generation_s": round(gen_s, 1)},
+        "config": config_of(args, wl, world),
+        "set": {"ngraphs": ng, "nv": U.nv, "ne": U.ne, "generation_s": round(gen_s, 1)},
         "plain": {"graphs_per_s": world * plain_gps, "sampled_graphs": len(sample),
                   "batched_over_plain": (ng * args.steps / sec) / plain_gps,
                   "max_abs_dq_vs_plain": dq, "partition_mismatches": mismatch},
@@ -413,10 +433,14 @@ def run_many(args, world, rank, local):
         "cpu_baseline": cpu,
         "clocks": clocks,
         "gpu_launches": launches,
+        "kernel_launches_per_step": launches / args.steps,
+        "latency_ms": serving["latency_ms"] if serving else None,
+        "serving": ({k: serving[k] for k in ("graphs_per_s", "requests", "latency_ms", "overlap", "workload")}
+                    if serving else None),
     }
 
 
-def run_serve(args, world, rank, local):
+def serve_replay(args, local):
     """A stream of requests with Poisson arrivals through the request loop
     (nido_server_*): graphs/s from first arrival to last result, and the
     latency (arrival to result in host memory) of every request."""
@@ -429,12 +453,9 @@ def run_serve(args, world, rank, local):
     gen_s = time.perf_counter() - t0
     budget = int(args.serve_budget_gb * 1e9)
     srv = capi.Server(local, budget, workers=args.serve_workers)
-    warm = [W.make_request(2000 + 500 * i, i % 2, 77 + i) for i in range(args.warmup)]
+    warm = [W.make_request(2000 + 500 * i, i % 2, 77 + i) for i in range(3)]
     for t in [srv.submit(g, wl["nbatches"], wl["tau"]) for g in warm]:
         srv.wait(t)
-    barrier(world)
-    sampler = ClockSampler(local)
-    sampler.start()
     l0 = capi.lib().nido_launch_count()
     tickets = [None] * len(graphs)
     start = time.perf_counter()
@@ -452,40 +473,54 @@ def run_serve(args, world, rank, local):
     infos = [srv.wait(t)[1] for t in tickets]
     wall = time.perf_counter() - start
     launches = int(capi.lib().nido_launch_count() - l0)
-    clocks = sampler.stop()
     srv.close()
     lat = np.array([i.latency_ms for i in infos])
-    wall_max = reduce_max(wall, world)
-    if rank != 0:
-        return None
-    ne = int(sum(g.ne for g in graphs))
     dev_ms = float(sum(i.device_ms for i in infos))
     return {
-        "metric": "graphs/s", "value": world * len(graphs) / wall_max, "unit": "graphs/s", "n_gpus": world,
-        "steps": 1, "warmup": args.warmup, "ms_per_step": wall_max * 1e3, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "ours",
-        "config": {"workload": "serve", "graph": wl["desc"], "requests": len(graphs),
-                   "rate_per_s": args.serve_rate, "vmax": args.serve_vmax, "workers": args.serve_workers,
-                   "hbm_budget_bytes": budget, "total_edges": ne, "generation_s": round(gen_s, 1),
-                   "parallelism": f"replicas x{world}", "l2": "inputs larger than L2"},
+        "graphs_per_s": len(graphs) / wall, "wall_s": wall, "requests": len(graphs),
         "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
                        "max": float(lat.max()), "mean_queue": float(np.mean([i.queue_ms for i in infos]))},
-        "overlap": {"sum_device_ms": dev_ms, "wall_ms": wall * 1e3,
-                    "concurrency": dev_ms / (wall * 1e3)},
-        "e2e": {"value": world * len(graphs) / wall_max, "unit": "graphs/s",
-                "h2d_bytes_per_step": int(sum(g.off.nbytes + g.adj.nbytes + g.w.nbytes for g in graphs)),
-                "d2h_bytes_per_step": int(sum(8 * g.nv for g in graphs))},
+        "overlap": {"sum_device_ms": dev_ms, "wall_ms": wall * 1e3, "concurrency": dev_ms / (wall * 1e3)},
+        "workload": {"graph": wl["desc"], "rate_per_s": args.serve_rate, "vmax": args.serve_vmax,
+                     "workers": args.serve_workers, "hbm_budget_bytes": budget,
+                     "total_edges": int(sum(g.ne for g in graphs)), "generation_s": round(gen_s, 1)},
+        "h2d_bytes": int(sum(g.off.nbytes + g.adj.nbytes + g.w.nbytes for g in graphs)),
+        "d2h_bytes": int(sum(8 * g.nv for g in graphs)),
+        "launches": launches,
+    }
+
+
+def run_serve(args, world, rank, local):
+    """The serving workload on its own: one step is the whole replay."""
+    sampler = ClockSampler(local)
+    barrier(world)
+    sampler.start()
+    r = serve_replay(args, local)
+    clocks = sampler.stop()
+    wall_max = reduce_max(r["wall_s"], world)
+    if rank != 0:
+        return None
+    return {
+        "metric": "graphs/s", "value": world * r["requests"] / wall_max, "unit": "graphs/s", "n_gpus": world,
+        "steps": 1, "warmup": 3, "ms_per_step": wall_max * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "ours",
+        "config": config_of(args, WORKLOADS["serve"], world),
+        "requests": r["requests"], "serving": r["workload"],
+        "latency_ms": r["latency_ms"], "overlap": r["overlap"],
+        "e2e": {"value": world * r["requests"] / wall_max, "unit": "graphs/s",
+                "h2d_bytes_per_step": r["h2d_bytes"], "d2h_bytes_per_step": r["d2h_bytes"]},
         "roofline": None,
         "cpu_baseline": None,
         "clocks": clocks,
-        "gpu_launches": launches,
+        "gpu_launches": r["launches"],
     }
 
 
 def run_reference_set(args, world, wl):
     """Reference arm of the graph-set workloads: whole CPU-oracle runs, all
     host threads, one graph after another (the reference runs one graph per
-    process), each step about 20 s of graphs drawn in order from the set."""
+    process).  Every step runs whole graphs drawn in order from the set until
+    about --ref-step-s seconds have passed; the step's time is what it took."""
     from nido_b200 import workloads as W
     from oracle import oracle as orc
     threads = os.cpu_count() or 1
@@ -498,10 +533,10 @@ def run_reference_set(args, world, wl):
         _, Vs, ks = W.serving_requests(args.serve_requests, args.serve_rate, 5, 1e3, args.serve_vmax)
         items = [(int(v), int(k), i) for i, (v, k) in enumerate(zip(Vs, ks))]
         make = lambda it: W.make_request(it[0], it[1], 5_000_003 + it[2])
-    pos, times = 0, []
+    pos, steps = 0, []
     for step in range(args.warmup + args.steps):
         done, el = 0, 0.0
-        while el < 20.0:
+        while el < args.ref_step_s:
             G = make(items[pos % len(items)])
             pos += 1
             c0 = time.perf_counter()
@@ -509,15 +544,18 @@ def run_reference_set(args, world, wl):
             el += time.perf_counter() - c0
             done += 1
         if step >= args.warmup:
-            times.append((done, el))
-    value = sum(t[0] for t in times) / sum(t[1] for t in times)
-    sample = (f"CPU oracle (port of the reference's algorithm), {threads} threads, whole runs of graphs drawn "
-              f"in order from the {args.workload} set, about 20 s per step")
+            steps.append((done, el))
+    total_s = sum(t[1] for t in steps)
+    value = sum(t[0] for t in steps) / total_s
+    sample = (f"CPU oracle (port of the reference's algorithm), {threads} threads: each step whole runs of "
+              f"graphs drawn in order from the {args.workload} set's systematic sample, about "
+              f"{args.ref_step_s:g} s ({sum(t[0] for t in steps)} graphs in {total_s:.1f} s over {len(steps)} steps)")
     return {
         "metric": "graphs/s", "value": value, "unit": "graphs/s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": 1e3 / value, "higher_is_better": True,
+        "warmup": args.warmup, "ms_per_step": 1e3 * total_s / len(steps), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
-        "config": {"workload": args.workload, "graph": wl["desc"], "nbatches": wl["nbatches"], "tau": wl["tau"]},
+        "config": config_of(args, wl, world),
+        "graphs_per_step": [t[0] for t in steps],
         "cpu_baseline": {"value": value, "unit": "graphs/s", "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": "graphs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -525,8 +563,8 @@ def run_reference_set(args, world, wl):
 
 def run_reference(args, world, rank):
     """The reference's path on the host cores: the CPU oracle (a port of nido's
-    algorithm; nido itself has no CPU implementation), all threads, each step
-    a bounded sample scaled to a whole run."""
+    algorithm; nido itself has no CPU implementation), all threads.  Every
+    step is one whole Louvain run of the workload's graph, timed as it runs."""
     if rank != 0:
         return None
     from nido_b200 import capi
@@ -536,37 +574,27 @@ def run_reference(args, world, rank):
         return run_reference_set(args, world, wl)
     G = make_graph(capi, args.workload)
     threads = os.cpu_count() or 1
-    # warm-up 1: one whole run fixes the edges a run visits (the oracle's
-    # trajectory is the engine's, bit for bit on integer weights)
-    t0 = time.perf_counter()
-    _, full = orc.louvain(G.off, G.adj, G.w, nbatches=wl["nbatches"], tau=wl["tau"])
-    full_s = time.perf_counter() - t0
-    edges_per_run = sum(full.ne_phase[p] * (1 + 2 * full.loops_phase[p]) for p in range(full.phases))
-    samples = []
-    small = False
-    for i in range(args.warmup - 1 + args.steps):
-        el, scanned, st, small = cpu_baseline_sample(G, wl, threads)
-        if i >= args.warmup - 1:
-            samples.append((el, scanned))
-    el = sum(s[0] for s in samples)
-    scanned = sum(s[1] for s in samples)
-    if small:
-        value = len(samples) / el
-        sample = f"CPU oracle (port of the reference's algorithm), {threads} threads, one whole run per step"
-    else:
-        value = scanned / el / edges_per_run
-        sample = (f"CPU oracle (port of the reference's algorithm), {threads} threads; each step the first "
-                  f"Louvain phase capped at 3 iterations without coarsening, scaled by the {edges_per_run:.4g} "
-                  f"edges a whole run visits; one whole run took {full_s:.1f} s")
+    times, final_q = [], None
+    for i in range(args.warmup + args.steps):
+        t0 = time.perf_counter()
+        _, st = orc.louvain(G.off, G.adj, G.w, nbatches=wl["nbatches"], tau=wl["tau"])
+        el = time.perf_counter() - t0
+        final_q = st.final_q
+        if i >= args.warmup:
+            times.append(el)
+    total_s = sum(times)
+    value = len(times) / total_s
+    sample = (f"CPU oracle (port of the reference's algorithm), {threads} threads, one whole run per step "
+              f"({total_s:.1f} s for {len(times)} runs)")
     return {
         "metric": "graphs/s", "value": value, "unit": "graphs/s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": 1e3 / value, "higher_is_better": True,
+        "warmup": args.warmup, "ms_per_step": 1e3 * total_s / len(times), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
-        "config": {"workload": args.workload, "graph": wl["desc"], "nv": G.nv, "ne": G.ne,
-                   "nbatches": wl["nbatches"], "tau": wl["tau"]},
+        "config": config_of(args, wl, world),
+        "graph_size": {"nv": G.nv, "ne": G.ne},
         "cpu_baseline": {"value": value, "unit": "graphs/s", "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": "graphs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "full_run_s": full_s, "full_run_q": full.final_q,
+        "final_q": final_q,
     }
 
 
@@ -576,16 +604,19 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="rmat22")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="many")
+    ap.add_argument("--no-serve", action="store_true", help="many: skip the serving replay's latency figures")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--many-graphs", type=int, default=4096)
     ap.add_argument("--many-edges", type=float, default=1.5e9)
     ap.add_argument("--plain-sample", type=int, default=256, help="graphs run one at a time for the comparison")
-    ap.add_argument("--serve-requests", type=int, default=32)
+    ap.add_argument("--serve-requests", type=int, default=24)
     ap.add_argument("--serve-rate", type=float, default=4.0, help="Poisson arrival rate, requests per second")
     ap.add_argument("--serve-vmax", type=float, default=1e7)
     ap.add_argument("--serve-workers", type=int, default=4)
     ap.add_argument("--serve-budget-gb", type=float, default=150.0)
+    ap.add_argument("--ref-step-s", type=float, default=8.0,
+                    help="reference arm of the graph sets: seconds of whole CPU runs per step")
     args = ap.parse_args()
     if args.warmup < 3:
         raise SystemExit("--warmup must be at least 3")
