@@ -66,7 +66,10 @@ typedef struct {
                         when tau_phase_set, otherwise tau (the reference's
                         three-argument LouvainGPU) */
   int32_t tau_phase_set;
-  int32_t reserved;  /* must be 0 */
+  int32_t host_loop; /* 0 (default): each phase's iteration loop runs on the
+                        device as one CUDA graph with a conditional while node,
+                        read back once per phase; 1: the host drives it, one Q
+                        readback per iteration, as the reference does */
 } nido_params;
 
 /* Per-run statistics (the reference prints these, louvain_gpu.cpp:43-131). */

@@ -2,7 +2,7 @@
 line of run statistics per run.
 
   python -m nido_b200 (--file graph.bin | --workload rmat22|rmat20|planted|sbm)
-                      [--runs 1] [-b 2] [-t 1e-6] [-i 500] [--tie nido] [--tune]
+                      [--runs 1] [-b 2] [-t 1e-6] [-i 500] [--tie nido] [--tune] [--host-loop]
 """
 import argparse
 import json
@@ -22,12 +22,13 @@ def main():
     ap.add_argument("--tie", choices=["smallest", "nido"], default="smallest")
     ap.add_argument("--tune", action="store_true")
     ap.add_argument("--device", type=int, default=0)
+    ap.add_argument("--host-loop", action="store_true", help="drive the iteration loop from the host")
     a = ap.parse_args()
     G = capi.read_vite(a.file) if a.file else workloads.single_graph(a.workload)
     tie = capi.NIDO_TIE_NIDO if a.tie == "nido" else capi.NIDO_TIE_SMALLEST_ID
     with capi.Context(a.device) as ctx, capi.Graph(ctx, G, a.b) as g:
         for r in range(a.runs):
-            _, st = g.run(tau=a.t, max_iter=a.i, tie=tie, tune=a.tune)
+            _, st = g.run(tau=a.t, max_iter=a.i, tie=tie, tune=a.tune, host_loop=a.host_loop)
             print(json.dumps({"run": r, "nv": G.nv, "ne": G.ne, "phases": st.phases, "loops": st.total_loops,
                               "final_q": st.final_q, "total_ms": st.total_ms, "move_ms": st.move_ms,
                               "q_ms": st.q_ms, "agg_ms": st.agg_ms,

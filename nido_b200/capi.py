@@ -37,7 +37,7 @@ class _Csr(C.Structure):
 class _Params(C.Structure):
     _fields_ = [("nbatches", C.c_int32), ("tie_mode", C.c_int32), ("tau", C.c_double),
                 ("max_iter", C.c_int64), ("verbose", C.c_int32), ("tune", C.c_int32),
-                ("tau_phase", C.c_double), ("tau_phase_set", C.c_int32), ("reserved", C.c_int32)]
+                ("tau_phase", C.c_double), ("tau_phase_set", C.c_int32), ("host_loop", C.c_int32)]
 
 
 class RunStats(C.Structure):
@@ -422,9 +422,12 @@ class Graph:
         return b.value
 
     def run(self, tau: float = 1e-6, max_iter: int = 500, tie: int = NIDO_TIE_SMALLEST_ID,
-            verbose: bool = False, tune: bool = False):
-        """LouvainGPU::run; returns (clustering of the input vertices, RunStats)."""
-        p = _Params(self.nbatches, tie, tau, max_iter, int(verbose), int(tune))
+            verbose: bool = False, tune: bool = False, host_loop: bool = False, tau_phase: float | None = None):
+        """LouvainGPU::run; returns (clustering of the input vertices, RunStats).
+        host_loop: drive each phase's iterations from the host (one readback per
+        iteration) instead of the device-resident loop."""
+        p = _Params(self.nbatches, tie, tau, max_iter, int(verbose), int(tune),
+                    0.0 if tau_phase is None else tau_phase, int(tau_phase is not None), int(host_loop))
         out = np.empty(self.nv0, np.int64)
         st = RunStats()
         _check(lib().nido_run(self.h, C.byref(p), _p64(out), C.byref(st)))
@@ -482,10 +485,10 @@ class Batch:
         self.close()
 
     def run(self, tau: float = 1e-6, max_iter: int = 500, tie: int = NIDO_TIE_SMALLEST_ID,
-            tune: bool = False):
+            tune: bool = False, host_loop: bool = False):
         """Returns (per-graph clusterings, final Q per graph, phases per graph,
         loops per graph, RunStats)."""
-        p = _Params(self.nbatches, tie, tau, max_iter, 0, int(tune))
+        p = _Params(self.nbatches, tie, tau, max_iter, 0, int(tune), 0.0, 0, int(host_loop))
         out = np.empty(self.nv, np.int64)
         q = np.empty(self.ngraphs, np.float64)
         ph = np.empty(self.ngraphs, np.int64)

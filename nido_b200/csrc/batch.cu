@@ -66,6 +66,7 @@ struct nido_batch_s {
   double* modv = nullptr;
   double* selfv = nullptr;
   int64_t* counters = nullptr; // [0] iterating graphs [1] restoring [2] iterating vertices [3] aggregating
+  int64_t* bctl = nullptr;     // control block of the device-resident sweep loop (BatchCtl)
   int32_t* gid = nullptr;
   int64_t* outc = nullptr;     // final clustering of every original vertex (ids within its graph)
   int32_t* elist = nullptr;    // graphs whose clustering is written out now
@@ -294,7 +295,9 @@ struct PermRanges {
 __global__ void k_commit_listed(PermRanges r, int nr, const int32_t* __restrict__ perm,
                                 const int32_t* __restrict__ gid, const int32_t* __restrict__ flag,
                                 const double* __restrict__ k, int32_t* __restrict__ comm,
-                                int32_t* __restrict__ newc, double* __restrict__ a) {
+                                int32_t* __restrict__ newc, double* __restrict__ a,
+                                const int64_t* __restrict__ gate) {
+  if (gate && *gate == 0) return;  // the device-resident loop's restore, when no graph needs it
   const int64_t total = r.pre[nr];
   for (int64_t x = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; x < total; x += (int64_t)gridDim.x * blockDim.x) {
     int t = 0;
@@ -311,6 +314,50 @@ __global__ void k_commit_listed(PermRanges r, int nr, const int32_t* __restrict_
     newc[v] = src;
   }
 }
+
+// Control block of the device-resident sweep loop: stamps and device times
+// of the move kernels and of the modularity, sweeps run, and the counters of
+// the last sweep.
+struct BatchCtl {
+  unsigned long long t_move, move_ns, t_q, q_ns;
+  long long sweeps;
+  long long cnt[4];
+};
+
+// After k_control: go on while some graph iterates and the graphs still
+// iterating hold at least 3/4 of the listed vertices (below that the host
+// rebuilds the tier lists without the stopped graphs).
+__global__ void k_batch_cond(const unsigned long long* __restrict__ counters, BatchCtl* c, int64_t listed_v,
+                             cudaGraphConditionalHandle h) {
+  c->sweeps += 1;
+  for (int i = 0; i < 4; ++i) c->cnt[i] = (long long)counters[i];
+  const bool any = counters[0] > 0;
+  const bool keep = 4 * (long long)counters[2] >= 3 * listed_v;
+  cudaGraphSetConditional(h, any && keep ? 1u : 0u);
+}
+
+__global__ void k_batch_ctl_reset(BatchCtl* c) {
+  c->move_ns = 0;
+  c->q_ns = 0;
+  c->sweeps = 0;
+}
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+__global__ void k_bstamp(unsigned long long* t) { *t = global_ns(); }
+__global__ void k_blap(const unsigned long long* t0, unsigned long long* acc) { *acc += global_ns() - *t0; }
+
+struct LoopGraph {  // destroyed on every return
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  ~LoopGraph() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+  }
+};
 
 // end of a phase (louvain_gpu.cpp:100-118): aggregate if Q - Q_old > tau,
 // else the graph is finished
@@ -490,7 +537,7 @@ extern "C" int nido_batch_free(nido_batch B) {
                     (void*)B->gfin, (void*)B->loops_phase, (void*)B->loops_total, (void*)B->phases, (void*)B->Q,
                     (void*)B->Qold, (void*)B->qnew, (void*)B->mg, (void*)B->plist, (void*)B->llist,
                     (void*)B->moff, (void*)B->qoff, (void*)B->part, (void*)B->modv, (void*)B->selfv,
-                    (void*)B->counters, (void*)B->gid, (void*)B->outc,
+                    (void*)B->counters, (void*)B->bctl, (void*)B->gid, (void*)B->outc,
                     (void*)B->elist})
       raw_free(ctx, p);
     ctx->used -= std::min(ctx->used, B->bytes);
@@ -537,7 +584,7 @@ extern "C" int nido_batch_upload(nido_ctx ctx, int32_t ngraphs, const int64_t* v
   take(&B->Q, G); take(&B->Qold, G); take(&B->qnew, G); take(&B->mg, G);
   take(&B->plist, G); take(&B->llist, G); take(&B->moff, G + 1); take(&B->qoff, G + 1);
   take(&B->part, B->cap_part); take(&B->modv, B->cap_modv); take(&B->selfv, V);
-  take(&B->counters, 4); take(&B->gid, V);
+  take(&B->counters, 4); take(&B->bctl, 16); take(&B->gid, V);
   take(&B->outc, V); take(&B->elist, G);
   if (st != NIDO_OK) {
     // device_alloc counted only what it allocated; nido_batch_free subtracts B->bytes
@@ -673,23 +720,131 @@ extern "C" int nido_batch_run(nido_batch B, const nido_params* p, int64_t* out_c
     NIDO_TRY(batch_modularity(B, ql, B->Q));
     NIDO_CUDA_TRY(cudaMemcpyAsync(B->Qold, B->Q, sizeof(double) * ng, cudaMemcpyDeviceToDevice, s));
     int64_t n_iter = p->max_iter > 0 ? np : 0;
+    // the commit of every batch's listed vertices of the iterating graphs
+    auto commit_batch = [&](int b) -> int {
+      PermRanges r{};
+      int64_t tot = 0;
+      for (int t = 0; t < kNumTiers; ++t) {
+        r.start[t] = g->tier_off[(size_t)t * nb + b];
+        r.pre[t] = tot;
+        tot += g->tier_off[(size_t)t * nb + b + 1] - r.start[t];
+      }
+      r.pre[kNumTiers] = tot;
+      if (tot > 0) {
+        k_commit_listed<<<grid_for(tot, kThreads), kThreads, 0, s>>>(r, kNumTiers, g->perm, B->gid, B->giter, g->k,
+                                                                      g->comm, g->newc, g->a, nullptr);
+        NIDO_LAUNCH_CHECK();
+      }
+      return NIDO_OK;
+    };
+    // the undo of the graphs whose last sweep lowered Q (gate: only when the
+    // device counter of such graphs is non-zero)
+    auto restore_listed = [&](const int64_t* gate) -> int {
+      PermRanges r{};
+      r.start[0] = 0;
+      r.pre[0] = 0;
+      r.pre[1] = g->tier_off[(size_t)kNumTiers * nb];  // every listed vertex
+      if (r.pre[1] > 0) {
+        k_commit_listed<<<grid_for(r.pre[1], kThreads), kThreads, 0, s>>>(r, 1, g->perm, B->gid, B->grest, g->k,
+                                                                           g->comm, g->newc, g->a, gate);
+        NIDO_LAUNCH_CHECK();
+      }
+      NIDO_CUDA_TRY(cudaMemsetAsync(B->grest, 0, sizeof(int32_t) * ng, s));
+      return NIDO_OK;
+    };
+    // Sweeps on the device: one CUDA graph whose conditional while node runs
+    // move + commit of every batch, the per-graph modularity and the per-graph
+    // loop control, until no graph iterates or the iterating graphs hold less
+    // than 3/4 of the listed vertices.  One readback at the end.
+    auto device_sweeps = [&](bool* unsupported) -> int {
+      *unsupported = false;
+      BatchCtl* ctl = reinterpret_cast<BatchCtl*>(B->bctl);
+      k_batch_ctl_reset<<<1, 1, 0, s>>>(ctl);
+      NIDO_LAUNCH_CHECK();
+      LoopGraph lg;
+      NIDO_CUDA_TRY(cudaGraphCreate(&lg.graph, 0));
+      cudaGraphConditionalHandle h;
+      if (cudaGraphConditionalHandleCreate(&h, lg.graph, 1, cudaGraphCondAssignDefault) != cudaSuccess) {
+        cudaGetLastError();
+        *unsupported = true;
+        return NIDO_OK;
+      }
+      cudaGraphNodeParams cp = {cudaGraphNodeTypeConditional};
+      cp.conditional.handle = h;
+      cp.conditional.type = cudaGraphCondTypeWhile;
+      cp.conditional.size = 1;
+      cudaGraphNode_t node;
+      if (cudaGraphAddNode(&node, lg.graph, nullptr, 0, &cp) != cudaSuccess) {
+        cudaGetLastError();
+        *unsupported = true;
+        return NIDO_OK;
+      }
+      const uint64_t l0 = nido_launch_count();
+      NIDO_CUDA_TRY(cudaStreamBeginCaptureToGraph(s, cp.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                                  cudaStreamCaptureModeThreadLocal));
+      auto body = [&]() -> int {
+        for (int b = 0; b < nb; ++b) {
+          k_bstamp<<<1, 1, 0, s>>>(&ctl->t_move);
+          NIDO_LAUNCH_CHECK();
+          NIDO_TRY(launch_move_tiers(g, b, p->tie_mode));
+          k_blap<<<1, 1, 0, s>>>(&ctl->t_move, &ctl->move_ns);
+          NIDO_LAUNCH_CHECK();
+          NIDO_TRY(commit_batch(b));
+        }
+        k_bstamp<<<1, 1, 0, s>>>(&ctl->t_q);
+        NIDO_LAUNCH_CHECK();
+        NIDO_TRY(batch_modularity(B, ql, B->qnew));
+        k_blap<<<1, 1, 0, s>>>(&ctl->t_q, &ctl->q_ns);
+        NIDO_LAUNCH_CHECK();
+        NIDO_CUDA_TRY(cudaMemsetAsync(B->counters, 0, sizeof(int64_t) * 4, s));
+        k_control<<<grid_for((int64_t)ql.ids.size(), 128), 128, 0, s>>>(
+            B->llist, (int)ql.ids.size(), B->qnew, B->Q, B->loops_phase, B->loops_total, B->giter, B->grest, tau,
+            p->max_iter, g->gbase, reinterpret_cast<unsigned long long*>(B->counters));
+        NIDO_LAUNCH_CHECK();
+        k_batch_cond<<<1, 1, 0, s>>>(reinterpret_cast<unsigned long long*>(B->counters), ctl, listed_v, h);
+        NIDO_LAUNCH_CHECK();
+        return restore_listed(B->counters + 1);
+      };
+      const int bst = body();
+      cudaGraph_t captured = nullptr;
+      const cudaError_t ce = cudaStreamEndCapture(s, &captured);
+      if (bst != NIDO_OK) return bst;
+      if (ce != cudaSuccess) return nido_set_error(NIDO_E_CUDA, "sweep-loop capture failed: %s", cudaGetErrorString(ce));
+      const uint64_t body_kernels = nido_launch_count() - l0;
+      const cudaError_t ie = cudaGraphInstantiate(&lg.exec, lg.graph, 0);
+      if (ie != cudaSuccess) {
+        lg.exec = nullptr;
+        return nido_set_error(NIDO_E_CUDA, "sweep-loop graph instantiation failed: %s", cudaGetErrorString(ie));
+      }
+      NIDO_CUDA_TRY(cudaGraphLaunch(lg.exec, s));
+      BatchCtl hc;
+      NIDO_CUDA_TRY(cudaMemcpyAsync(&hc, ctl, sizeof(hc), cudaMemcpyDeviceToHost, s));
+      NIDO_CUDA_TRY(cudaStreamSynchronize(s));
+      if (hc.sweeps > 1) nido_count_launches(body_kernels * (uint64_t)(hc.sweeps - 1));
+      st.move_launches += (int64_t)nb * hc.sweeps;
+      st.edges_scanned += (double)listed_e * (double)hc.sweeps;
+      st.move_bytes += (16.0 * (double)listed_e + 32.0 * (double)listed_v) * (double)hc.sweeps;
+      st.total_loops += hc.sweeps;
+      st.move_ms += hc.move_ns * 1e-6;
+      st.q_ms += hc.q_ns * 1e-6;
+      for (int i = 0; i < 4; ++i) cnt[i] = (unsigned long long)hc.cnt[i];
+      return NIDO_OK;
+    };
     while (n_iter > 0) {
+      bool ran_on_device = false;
+      if (!p->host_loop && g->ctx->device_loop) {
+        bool unsupported = false;
+        NIDO_TRY(device_sweeps(&unsupported));
+        if (unsupported) g->ctx->device_loop = false;
+        ran_on_device = !unsupported;
+      }
+      if (ran_on_device) {
+        n_iter = (int64_t)cnt[0];
+      } else {
       NIDO_CUDA_TRY(cudaEventRecord(ev[0], s));
       for (int b = 0; b < nb; ++b) {
         NIDO_TRY(launch_move(g, b, p->tie_mode, nullptr, nullptr));
-        PermRanges r{};
-        int64_t tot = 0;
-        for (int t = 0; t < kNumTiers; ++t) {
-          r.start[t] = g->tier_off[(size_t)t * nb + b];
-          r.pre[t] = tot;
-          tot += g->tier_off[(size_t)t * nb + b + 1] - r.start[t];
-        }
-        r.pre[kNumTiers] = tot;
-        if (tot > 0) {
-          k_commit_listed<<<grid_for(tot, kThreads), kThreads, 0, s>>>(r, kNumTiers, g->perm, B->gid, B->giter, g->k,
-                                                                        g->comm, g->newc, g->a);
-          NIDO_LAUNCH_CHECK();
-        }
+        NIDO_TRY(commit_batch(b));
       }
       NIDO_CUDA_TRY(cudaEventRecord(ev[1], s));
       st.move_launches += nb;
@@ -707,17 +862,9 @@ extern "C" int nido_batch_run(nido_batch B, const nido_params* p, int64_t* out_c
       float ms = 0.f;
       NIDO_CUDA_TRY(cudaEventElapsedTime(&ms, ev[0], ev[1]));
       st.move_ms += ms;
-      if (cnt[1]) {
-        PermRanges r{};
-        r.start[0] = 0;
-        r.pre[0] = 0;
-        r.pre[1] = g->tier_off[(size_t)kNumTiers * nb];  // every listed vertex
-        k_commit_listed<<<grid_for(r.pre[1], kThreads), kThreads, 0, s>>>(r, 1, g->perm, B->gid, B->grest, g->k,
-                                                                           g->comm, g->newc, g->a);
-        NIDO_LAUNCH_CHECK();
-        NIDO_CUDA_TRY(cudaMemsetAsync(B->grest, 0, sizeof(int32_t) * ng, s));
-      }
+      if (cnt[1]) NIDO_TRY(restore_listed(nullptr));
       n_iter = (int64_t)cnt[0];
+      }
       // drop stopped graphs from the tier lists once a quarter of the listed
       // vertices belong to them
       if (n_iter > 0 && 4 * (int64_t)cnt[2] < 3 * listed_v) {

@@ -281,7 +281,8 @@ extern "C" int nido_graph_free(nido_graph g) {
   for (void* p : {(void*)g->gkeys, (void*)g->gvals, (void*)g->hub_items, (void*)g->hub_v, (void*)g->hub_capv,
                   (void*)g->hub_nseg, (void*)g->hub_toff, (void*)g->hub_done, (void*)g->hub_slices,
                   (void*)g->hub_slice_first, (void*)g->hub_res, (void*)g->hub_item_first,
-                  (void*)g->hub_part, (void*)g->hub_cl_v, (void*)g->agg_buf, (void*)g->pm32})
+                  (void*)g->hub_part, (void*)g->hub_cl_v, (void*)g->agg_buf, (void*)g->pm32,
+                  (void*)g->loop_buf})
     nido::raw_free(ctx, p);
   for (nido_graph_s::MoveGraph& mg : g->move_graphs)
     if (mg.exec) cudaGraphExecDestroy(mg.exec);
@@ -948,13 +949,40 @@ extern "C" int nido_run(nido_graph g, const nido_params* p, int64_t* out_comm, n
       lap(6);
     }
     NIDO_TRY(nido::launch_singleton(g));
-    double Q;
+    double Q = 0., Q_old = 0.;
+    int64_t loops = 0;
+    bool host_loop = p->host_loop != 0 || !g->ctx->device_loop || (p->verbose && p->max_iter > nido::kLoopLogCap);
+    if (!host_loop) {
+      // the phase's iteration loop as one device-resident CUDA graph
+      nido::PhaseLoop r;
+      bool unsupported = false;
+      NIDO_TRY(nido::device_phase_loop(g, p->tie_mode, tau, p->max_iter, p->verbose != 0, &r, &unsupported));
+      if (unsupported) {
+        g->ctx->device_loop = false;  // this driver has no conditional graph nodes
+        host_loop = true;
+      } else {
+        Q_old = r.q_old;
+        Q = r.q;
+        loops = r.loops;
+        st.move_ms += r.move_ms;
+        st.q_ms += r.q_ms;
+        st.move_launches += g->nbatches * loops;
+        st.edges_scanned += (double)g->ne * (double)loops;
+        st.move_bytes += (16.0 * (double)g->ne + 32.0 * (double)g->nv) * (double)loops;
+        if (p->verbose) {
+          printf("LOOP# \tQ \t\tdQ\n----------------------------------------\n0 \t%g \t0\n", Q_old);
+          for (size_t i = 0; 2 * i + 1 < r.log.size(); ++i)
+            printf("%lld \t%g \t%g\n", (long long)(i + 1), r.log[2 * i], r.log[2 * i + 1]);
+        }
+        lap(1);
+      }
+    }
+    if (host_loop) {
     NIDO_TRY(modularity(&Q));
     lap(2);
-    const double Q_old = Q;
+    Q_old = Q;
     if (p->verbose) printf("LOOP# \tQ \t\tdQ\n----------------------------------------\n0 \t%g \t0\n", Q);
     double dQ = NIDO_MAX_FLOAT;
-    int64_t loops = 0;
     while (tau < dQ && loops < p->max_iter) {
       std::vector<cudaEvent_t>& ev = g->ctx->move_ev;
       while (ev.size() < 2 * (size_t)g->nbatches) {
@@ -983,6 +1011,7 @@ extern "C" int nido_run(nido_graph g, const nido_params* p, int64_t* out_comm, n
       if (dQ < 0) NIDO_TRY(nido::launch_commit(g, 0, g->nv));
       else Q = Qtmp;
       if (p->verbose) printf("%lld \t%g \t%g\n", (long long)loops, Qtmp, dQ);
+    }
     }
     if (phases < 200) {
       st.q_phase[phases] = Q;
@@ -1020,7 +1049,7 @@ extern "C" int nido_run(nido_graph g, const nido_params* p, int64_t* out_comm, n
   st.phases = phases;
   NIDO_TRY(qt.finish());
   NIDO_TRY(at.finish());
-  st.q_ms = qt.ms;
+  st.q_ms += qt.ms;
   st.agg_ms = at.ms;
   int64_t nerr = 0;
   NIDO_CUDA_TRY(cudaMemcpyAsync(&nerr, g->dcount + 1, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
@@ -1031,5 +1060,6 @@ extern "C" int nido_run(nido_graph g, const nido_params* p, int64_t* out_comm, n
   lap(5);
   st.kernel_launches = (int64_t)(nido_launch_count() - launches0);
   if (stats) *stats = st;
+  if (p->verbose) fflush(stdout);
   return NIDO_OK;
 }

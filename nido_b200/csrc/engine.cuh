@@ -80,6 +80,9 @@ struct nido_ctx_s {
   // settings are left alone.
   bool async_alloc = false;
   cudaMemPool_t pool = nullptr;
+  // phase loops run on the device (loop.cu) until the driver turns out to
+  // lack conditional graph nodes
+  bool device_loop = true;
   // otherwise blocks come from cudaMalloc and are kept for reuse when freed
   // (raw_alloc / raw_free): free blocks by size, the size of every block in
   // use, and the bytes held in free blocks
@@ -207,6 +210,9 @@ struct nido_graph_s {
   std::vector<MoveGraph> move_graphs;
   int64_t plan_epoch = 0;
   bool use_graphs = true;
+  // device-resident iteration loop (loop.cu): its control block and per-loop log
+  char* loop_buf = nullptr;
+  size_t loop_bytes = 0;
   double host_pinned_dummy = 0;
 };
 
@@ -235,6 +241,8 @@ int launch_singleton(nido_graph_s* g);
 int launch_set_comm(nido_graph_s* g);                   // a from comm
 int launch_commit(nido_graph_s* g, int64_t v0, int64_t v1);
 int launch_modularity(nido_graph_s* g, double* q);      // host value
+int launch_modularity_dev(nido_graph_s* g);             // into g->dm[1], no host sync
+int launch_commit_gated(nido_graph_s* g, int64_t v0, int64_t v1, const int32_t* gate);
 int launch_q_self(nido_graph_s* g, double* selfv);      // per-vertex in-community weight
 int graph_prepare_phase(nido_graph_s* g);               // k, m, tier lists (engine.cu)
 // device memory of a context: stream-ordered when ctx->async_alloc (engine.cu)
@@ -250,11 +258,22 @@ int build_batches(nido_graph_s* g);                     // cuts (host) + tier li
 // move phase (move.cu)
 // ev_start / ev_end (may be null) are recorded around the tier kernels
 int launch_move(nido_graph_s* g, int batch, int tie, cudaEvent_t ev_start, cudaEvent_t ev_end);
+int launch_move_tiers(nido_graph_s* g, int batch, int tie);  // enqueue only (capturable)
 int plan_hubs(nido_graph_s* g);          // per phase, after the tier lists
 int move_init_attributes();              // once per device
 // times `sweeps` move sweeps (no commit) for candidate tier configurations
 // and keeps the fastest in g->cfg (engine.cu); clobbers newc
 int tune_tiers(nido_graph_s* g, int tie, int sweeps, double* best_ms);
+// the iteration loop of one phase on the device (loop.cu)
+constexpr int64_t kLoopLogCap = 65536;  // per-loop (Qtmp, dQ) entries kept for printing
+struct PhaseLoop {
+  double q_old = 0., q = 0.;
+  int64_t loops = 0;
+  double move_ms = 0., q_ms = 0.;
+  std::vector<double> log;  // Qtmp, dQ of every iteration (with want_log)
+};
+int device_phase_loop(nido_graph_s* g, int tie, double tau, int64_t max_iter, bool want_log, PhaseLoop* r,
+                      bool* unsupported);
 // coarsening (coarsen.cu)
 int launch_aggregation(nido_graph_s* g, int* done);
 

@@ -1370,18 +1370,35 @@ int move_init_attributes() {
   return set_smem_mode<true, true>();
 }
 
+namespace {
+MoveArgs move_args(nido_graph_s* g, int tie) {
+  return MoveArgs{g->off, g->adj, g->w, g->comm, g->k, g->a, g->newc, g->m, tie,
+                  reinterpret_cast<unsigned long long*>(g->dcount + 1), g->gid, g->mg, g->int_weights ? 1 : 0};
+}
+
+int tiers_direct(nido_graph_s* g, int batch, int tie, const MoveArgs& p) {
+  if (g->gid) return p.ints ? launch_tiers<true, true>(g, batch, tie, p) : launch_tiers<true, false>(g, batch, tie, p);
+  return p.ints ? launch_tiers<false, true>(g, batch, tie, p) : launch_tiers<false, false>(g, batch, tie, p);
+}
+}  // namespace
+
+// The tier kernels of one batch, enqueued directly (no events, no per-batch
+// graph): what the device-resident loop captures.  The plan (tier lists, hub
+// plan) must be valid.
+int launch_move_tiers(nido_graph_s* g, int batch, int tie) {
+  if (batch < 0 || batch >= g->nbatches)
+    return nido_set_error(NIDO_E_INVALID, "louvain_update: batch %d out of range [0,%d)", batch, g->nbatches);
+  return tiers_direct(g, batch, tie, move_args(g, tie));
+}
+
 int launch_move(nido_graph_s* g, int batch, int tie, cudaEvent_t ev_start, cudaEvent_t ev_end) {
   if (batch < 0 || batch >= g->nbatches)
     return nido_set_error(NIDO_E_INVALID, "louvain_update: batch %d out of range [0,%d)", batch, g->nbatches);
   if (!g->bins_valid) NIDO_TRY(build_batches(g));
   cudaStream_t s = g->ctx->stream;
-  MoveArgs p{g->off, g->adj, g->w, g->comm, g->k, g->a, g->newc, g->m, tie,
-             reinterpret_cast<unsigned long long*>(g->dcount + 1), g->gid, g->mg, g->int_weights ? 1 : 0};
+  const MoveArgs p = move_args(g, tie);
   if (ev_start) NIDO_CUDA_TRY(cudaEventRecord(ev_start, s));
-  auto direct = [&]() {
-    if (g->gid) return p.ints ? launch_tiers<true, true>(g, batch, tie, p) : launch_tiers<true, false>(g, batch, tie, p);
-    return p.ints ? launch_tiers<false, true>(g, batch, tie, p) : launch_tiers<false, false>(g, batch, tie, p);
-  };
+  auto direct = [&]() { return tiers_direct(g, batch, tie, p); };
   if (!g->use_graphs) {
     NIDO_TRY(direct());
   } else {

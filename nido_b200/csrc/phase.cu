@@ -143,7 +143,9 @@ __device__ __forceinline__ void warp_community_add(double* a, int c, double x, b
 
 __global__ void k_commit(int64_t v0, int64_t v1, const double* __restrict__ k,
                          int32_t* __restrict__ comm, int32_t* __restrict__ newc,
-                         double* __restrict__ a, int64_t* __restrict__ moved) {
+                         double* __restrict__ a, int64_t* __restrict__ moved,
+                         const int32_t* __restrict__ gate) {
+  if (gate && *gate == 0) return;  // the device-resident loop's restore, when not needed
   int64_t cnt = 0;
   const int64_t stride = (int64_t)gridDim.x * blockDim.x;
   // the loop runs warp-uniformly (the warp's first lane decides)
@@ -449,7 +451,16 @@ int launch_set_comm(nido_graph_s* g) {
 int launch_commit(nido_graph_s* g, int64_t v0, int64_t v1) {
   if (v1 <= v0) return NIDO_OK;
   k_commit<<<grid_for(v1 - v0, kThreads), kThreads, 0, g->ctx->stream>>>(v0, v1, g->k, g->comm,
-                                                                         g->newc, g->a, nullptr);
+                                                                         g->newc, g->a, nullptr, nullptr);
+  NIDO_LAUNCH_CHECK();
+  return NIDO_OK;
+}
+
+// the commit of [v0, v1) only when *gate is non-zero (read on the device)
+int launch_commit_gated(nido_graph_s* g, int64_t v0, int64_t v1, const int32_t* gate) {
+  if (v1 <= v0) return NIDO_OK;
+  k_commit<<<grid_for(v1 - v0, kThreads), kThreads, 0, g->ctx->stream>>>(v0, v1, g->k, g->comm,
+                                                                         g->newc, g->a, nullptr, gate);
   NIDO_LAUNCH_CHECK();
   return NIDO_OK;
 }
@@ -549,8 +560,23 @@ int launch_q_self(nido_graph_s* g, double* selfv) {
 
 int launch_modularity(nido_graph_s* g, double* q) {
   cudaStream_t s = g->ctx->stream;
+  if (g->nv == 0) { *q = 0.; return NIDO_OK; }
+  NIDO_TRY(launch_modularity_dev(g));
+  NIDO_CUDA_TRY(cudaMemcpyAsync(q, g->dm + 1, sizeof(double), cudaMemcpyDeviceToHost, s));
+  NIDO_CUDA_TRY(cudaStreamSynchronize(s));
+  return NIDO_OK;
+}
+
+// Q of the current partition into g->dm[1], enqueued only (no host
+// synchronisation), so it can be captured into the device-resident loop.
+// The tier lists must be valid (build_batches) before a capture.
+int launch_modularity_dev(nido_graph_s* g) {
+  cudaStream_t s = g->ctx->stream;
   const int64_t nv = g->nv;
-  if (nv == 0) { *q = 0.; return NIDO_OK; }
+  if (nv == 0) {
+    NIDO_CUDA_TRY(cudaMemsetAsync(g->dm + 1, 0, sizeof(double), s));
+    return NIDO_OK;
+  }
   if (!g->bins_valid) NIDO_TRY(build_batches(g));
   Arena ar(g->scratch, g->scratch_bytes);
   double* selfv = ar.take<double>(nv);
@@ -567,8 +593,6 @@ int launch_modularity(nido_graph_s* g, double* q) {
   NIDO_LAUNCH_CHECK();
   k_reduce_1024<<<1, 1024, 0, s>>>(modv, ngroups, 1.0, g->dm + 1);
   NIDO_LAUNCH_CHECK();
-  NIDO_CUDA_TRY(cudaMemcpyAsync(q, g->dm + 1, sizeof(double), cudaMemcpyDeviceToHost, s));
-  NIDO_CUDA_TRY(cudaStreamSynchronize(s));
   return NIDO_OK;
 }
 
