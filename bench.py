@@ -265,6 +265,24 @@ def run_ours(args, world, rank, local):
     for a in (G.off, G.adj, G.w):
         capi.host_unregister(a)
 
+    color = None
+    if args.color_batches:
+        # conflict-free colour-class batches against the edge-balanced -b cuts
+        with capi.Graph(ctx, G, wl["nbatches"]) as g3:
+            for _ in range(args.warmup):
+                g3.run(tau=wl["tau"], color_batches=True)
+            ctx.sync()
+            c0, c1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            c0.record(stream)
+            cst = [g3.run(tau=wl["tau"], color_batches=True)[1] for _ in range(args.steps)]
+            c1.record(stream)
+            ctx.sync()
+            cms = c0.elapsed_time(c1)
+        color = {"graphs_per_s": args.steps / (cms * 1e-3), "final_q": cst[-1].final_q,
+                 "phases": cst[-1].phases, "loops": cst[-1].total_loops,
+                 "edge_balanced": {"graphs_per_s": args.steps / sec_of(ms), "final_q": final_q,
+                                   "nbatches": wl["nbatches"]}}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
@@ -307,7 +325,12 @@ def run_ours(args, world, rank, local):
         "cpu_baseline": cpu,
         "clocks": clocks,
         "gpu_launches": launches,
+        "color_batches": color,
     }
+
+
+def sec_of(ms):
+    return ms * 1e-3
 
 
 def run_many(args, world, rank, local):
@@ -606,6 +629,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="many")
     ap.add_argument("--no-serve", action="store_true", help="many: skip the serving replay's latency figures")
+    ap.add_argument("--color-batches", action="store_true",
+                    help="one-graph workloads: also time colour-class batches against the -b cuts")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--many-graphs", type=int, default=4096)
     ap.add_argument("--many-edges", type=float, default=1.5e9)

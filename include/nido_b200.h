@@ -70,6 +70,12 @@ typedef struct {
                         device as one CUDA graph with a conditional while node,
                         read back once per phase; 1: the host drives it, one Q
                         readback per iteration, as the reference does */
+  int32_t color_batches; /* 1: conflict-free batches instead of the -b cuts:
+                        every phase colours its graph (Jones-Plassmann-Luby,
+                        seed 1) and sweeps the colour classes in colour order,
+                        one class per batch, so no two neighbours move in the
+                        same batch (one-graph runs only) */
+  int32_t reserved;  /* must be 0 */
 } nido_params;
 
 /* Per-run statistics (the reference prints these, louvain_gpu.cpp:43-131). */
@@ -138,7 +144,8 @@ int nido_graph_size(nido_graph g, int64_t* nv, int64_t* ne);
 /* download the current CSR (caller sizes from nido_graph_size) */
 int nido_graph_download(nido_graph g, int64_t* off, int64_t* adj, double* w);
 /* batch cut points of the current graph, nbatches+1 entries
- * (GraphGPU::vertex_per_batch_, graph_gpu.cpp:280-359) */
+ * (GraphGPU::vertex_per_batch_, graph_gpu.cpp:280-359); NIDO_E_INVALID after a
+ * run with colour-class batches, whose batches are not vertex ranges */
 int nido_graph_batches(nido_graph g, int64_t* cuts);
 /* k_v (vertexWeights_) and m (mass_) of the current graph */
 int nido_graph_vertex_weights(nido_graph g, double* k, double* m);

@@ -305,6 +305,11 @@ class GraphGPU {
   // reference's 8-lane strided rule, for louvain_update and LouvainGPU::run.
   void set_tie_rule(int tie) { tie_ = tie; }
   int tie_rule() const { return tie_; }
+  // Conflict-free batches for LouvainGPU::run: every phase's colour classes
+  // (device colouring of the phase's graph) are its batches, in colour order,
+  // instead of the -b cuts.
+  void set_color_batches(bool on) { color_batches_ = on; }
+  bool color_batches() const { return color_batches_; }
   int nbatches() const { return nbatches_; }
   nido_graph handle() const { return g_; }
   GraphElem original_vertices() const { return nv0_; }
@@ -326,6 +331,7 @@ class GraphGPU {
   GraphElem nv0_ = 0;
   int nbatches_ = 1;
   int tie_ = NIDO_TIE_SMALLEST_ID;
+  bool color_batches_ = false;
 };
 
 class LouvainGPU {
@@ -343,6 +349,7 @@ class LouvainGPU {
     nido_params p{};
     p.nbatches = nbatches_;
     p.tie_mode = graph->tie_rule();
+    p.color_batches = graph->color_batches() ? 1 : 0;
     p.tau = tol_;
     p.tau_phase = tol_phase_;
     p.tau_phase_set = 1;

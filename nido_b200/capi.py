@@ -37,7 +37,8 @@ class _Csr(C.Structure):
 class _Params(C.Structure):
     _fields_ = [("nbatches", C.c_int32), ("tie_mode", C.c_int32), ("tau", C.c_double),
                 ("max_iter", C.c_int64), ("verbose", C.c_int32), ("tune", C.c_int32),
-                ("tau_phase", C.c_double), ("tau_phase_set", C.c_int32), ("host_loop", C.c_int32)]
+                ("tau_phase", C.c_double), ("tau_phase_set", C.c_int32), ("host_loop", C.c_int32),
+                ("color_batches", C.c_int32), ("reserved", C.c_int32)]
 
 
 class RunStats(C.Structure):
@@ -422,12 +423,16 @@ class Graph:
         return b.value
 
     def run(self, tau: float = 1e-6, max_iter: int = 500, tie: int = NIDO_TIE_SMALLEST_ID,
-            verbose: bool = False, tune: bool = False, host_loop: bool = False, tau_phase: float | None = None):
+            verbose: bool = False, tune: bool = False, host_loop: bool = False, tau_phase: float | None = None,
+            color_batches: bool = False):
         """LouvainGPU::run; returns (clustering of the input vertices, RunStats).
         host_loop: drive each phase's iterations from the host (one readback per
-        iteration) instead of the device-resident loop."""
+        iteration) instead of the device-resident loop.  color_batches: every
+        phase's colour classes are its batches (conflict-free) instead of the
+        -b cuts."""
         p = _Params(self.nbatches, tie, tau, max_iter, int(verbose), int(tune),
-                    0.0 if tau_phase is None else tau_phase, int(tau_phase is not None), int(host_loop))
+                    0.0 if tau_phase is None else tau_phase, int(tau_phase is not None), int(host_loop),
+                    int(color_batches))
         out = np.empty(self.nv0, np.int64)
         st = RunStats()
         _check(lib().nido_run(self.h, C.byref(p), _p64(out), C.byref(st)))

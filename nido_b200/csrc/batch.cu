@@ -627,6 +627,8 @@ extern "C" int nido_batch_run(nido_batch B, const nido_params* p, int64_t* out_c
   nido_graph_s* g = B->g;
   if (p->nbatches != g->nbatches)
     return nido_set_error(NIDO_E_INVALID, "params.nbatches (%d) differs from the batch's (%d)", p->nbatches, g->nbatches);
+  if (p->color_batches)
+    return nido_set_error(NIDO_E_INVALID, "colour-class batches are for one-graph runs (nido_run)");
   if (p->tie_mode != NIDO_TIE_SMALLEST_ID && p->tie_mode != NIDO_TIE_NIDO)
     return nido_set_error(NIDO_E_INVALID, "unknown tie mode %d", p->tie_mode);
   NIDO_CUDA_TRY(cudaSetDevice(g->ctx->device));

@@ -65,6 +65,15 @@ __global__ void k_jpl_round(const int64_t* __restrict__ off, const int32_t* __re
   }
 }
 
+// largest colour + 1 (rem zeroed by the caller's last round, which found none left)
+__global__ void k_max_color(const int32_t* __restrict__ c, int64_t n, unsigned long long* __restrict__ out) {
+  unsigned long long m = 0;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    m = max(m, (unsigned long long)(c[i] + 1));
+  m = __reduce_max_sync(NIDO_FULL_MASK, (unsigned)m);
+  if ((threadIdx.x & 31) == 0 && m) atomicMax(out, m);
+}
+
 __global__ void k_copy_i32(const int32_t* __restrict__ x, int32_t* __restrict__ y, int64_t n) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
     y[i] = x[i];
@@ -136,6 +145,43 @@ int check_csr(const nido_csr* in) {
 }
 
 }  // namespace
+
+// JPL colouring of the graph's current (possibly coarse) CSR into colors
+// (device, nv entries); *ncolors = largest colour + 1.  Temporaries come from
+// the scratch arena, which is free again on return.
+int color_current_graph(nido_graph_s* g, uint64_t seed, int32_t* colors, int64_t* ncolors) {
+  cudaStream_t s = g->ctx->stream;
+  const int64_t nv = g->nv;
+  *ncolors = 0;
+  if (nv == 0) return NIDO_OK;
+  Arena ar(g->scratch, g->scratch_bytes);
+  int32_t* c1 = ar.take<int32_t>(nv);
+  unsigned long long* rem = ar.take<unsigned long long>(1);
+  if (!c1 || !rem) return nido_set_error(NIDO_E_NOMEM, "scratch arena too small (colouring)");
+  NIDO_CUDA_TRY(cudaMemsetAsync(colors, 0xff, 4 * nv, s));
+  NIDO_CUDA_TRY(cudaMemsetAsync(c1, 0xff, 4 * nv, s));
+  // every round colours at least the uncoloured vertex of largest (priority,
+  // id), so nv rounds always suffice
+  for (int64_t round = 0; round <= nv; ++round) {
+    NIDO_CUDA_TRY(cudaMemsetAsync(rem, 0, 8, s));
+    k_jpl_round<<<kSMs * 16, 256, 0, s>>>(g->off, g->adj, nv, seed, colors, c1, rem);
+    NIDO_LAUNCH_CHECK();
+    k_copy_i32<<<kSMs * 8, 256, 0, s>>>(c1, colors, nv);
+    NIDO_LAUNCH_CHECK();
+    unsigned long long r = 0;
+    NIDO_CUDA_TRY(cudaMemcpyAsync(&r, rem, 8, cudaMemcpyDeviceToHost, s));
+    NIDO_CUDA_TRY(cudaStreamSynchronize(s));
+    if (r == 0) break;
+  }
+  NIDO_CUDA_TRY(cudaMemsetAsync(rem, 0, 8, s));
+  k_max_color<<<kSMs * 4, 256, 0, s>>>(colors, nv, rem);
+  NIDO_LAUNCH_CHECK();
+  unsigned long long mx = 0;
+  NIDO_CUDA_TRY(cudaMemcpyAsync(&mx, rem, 8, cudaMemcpyDeviceToHost, s));
+  NIDO_CUDA_TRY(cudaStreamSynchronize(s));
+  *ncolors = (int64_t)mx;
+  return NIDO_OK;
+}
 }  // namespace nido
 
 using namespace nido;

@@ -282,7 +282,7 @@ extern "C" int nido_graph_free(nido_graph g) {
                   (void*)g->hub_nseg, (void*)g->hub_toff, (void*)g->hub_done, (void*)g->hub_slices,
                   (void*)g->hub_slice_first, (void*)g->hub_res, (void*)g->hub_item_first,
                   (void*)g->hub_part, (void*)g->hub_cl_v, (void*)g->agg_buf, (void*)g->pm32,
-                  (void*)g->loop_buf})
+                  (void*)g->loop_buf, (void*)g->vcolor})
     nido::raw_free(ctx, p);
   for (nido_graph_s::MoveGraph& mg : g->move_graphs)
     if (mg.exec) cudaGraphExecDestroy(mg.exec);
@@ -306,6 +306,7 @@ int graph_create(nido_ctx ctx, int64_t nv, int64_t ne, int32_t nbatches, nido_gr
   g->nv0 = g->nv = g->cap_v = nv;
   g->ne = g->ne0 = g->cap_e = ne;
   g->nbatches = nbatches;
+  g->nb_user = nbatches;
   const int64_t V = nv, E = ne;
   int st = NIDO_OK;
 #define ALLOC(p, n) if (st == NIDO_OK) st = dev_alloc(ctx, &g->p, (n))
@@ -513,6 +514,8 @@ extern "C" int nido_graph_download(nido_graph g, int64_t* off, int64_t* adj, dou
 }
 
 extern "C" int nido_graph_batches(nido_graph g, int64_t* cuts) {
+  if (g && g->color_mode)
+    return nido_set_error(NIDO_E_INVALID, "colour-class batches are not vertex ranges: no cut points");
   if (!g || !cuts) return nido_set_error(NIDO_E_INVALID, "null argument");
   if (!g->bins_valid) NIDO_TRY(nido::build_batches(g));
   std::copy(g->cuts.begin(), g->cuts.end(), cuts);
@@ -614,7 +617,7 @@ extern "C" int nido_update_community_weights(nido_graph g, int32_t batch) {
   if (!g) return nido_set_error(NIDO_E_INVALID, "null graph");
   if (batch < 0 || batch >= g->nbatches) return nido_set_error(NIDO_E_INVALID, "batch out of range");
   if (!g->bins_valid) NIDO_TRY(nido::build_batches(g));
-  return nido::launch_commit(g, g->cuts[batch], g->cuts[batch + 1]);
+  return nido::launch_commit_batch(g, batch);
 }
 
 extern "C" int nido_update_community_ids(nido_graph g, int32_t batch) {
@@ -895,8 +898,14 @@ struct SectionTimer {
 // than tau.
 extern "C" int nido_run(nido_graph g, const nido_params* p, int64_t* out_comm, nido_run_stats* stats) {
   if (!g || !p) return nido_set_error(NIDO_E_INVALID, "null argument");
-  if (p->nbatches != g->nbatches)
-    return nido_set_error(NIDO_E_INVALID, "params.nbatches (%d) differs from the graph's (%d)", p->nbatches, g->nbatches);
+  if (p->nbatches != g->nb_user)
+    return nido_set_error(NIDO_E_INVALID, "params.nbatches (%d) differs from the graph's (%d)", p->nbatches, g->nb_user);
+  if (p->color_batches != 0 && p->color_batches != 1)
+    return nido_set_error(NIDO_E_INVALID, "color_batches must be 0 or 1 (got %d)", p->color_batches);
+  if ((p->color_batches != 0) != g->color_mode) {
+    g->color_mode = p->color_batches != 0;  // the batches of every phase follow this run's choice
+    g->bins_valid = false;
+  }
   if (p->tie_mode != NIDO_TIE_SMALLEST_ID && p->tie_mode != NIDO_TIE_NIDO)
     return nido_set_error(NIDO_E_INVALID, "unknown tie mode %d", p->tie_mode);
   NIDO_CUDA_TRY(cudaSetDevice(g->ctx->device));
@@ -992,7 +1001,7 @@ extern "C" int nido_run(nido_graph g, const nido_params* p, int64_t* out_comm, n
       }
       for (int b = 0; b < g->nbatches; ++b) {
         NIDO_TRY(nido::launch_move(g, b, p->tie_mode, ev[2 * b], ev[2 * b + 1]));
-        NIDO_TRY(nido::launch_commit(g, g->cuts[b], g->cuts[b + 1]));
+        NIDO_TRY(nido::launch_commit_batch(g, b));
       }
       st.move_launches += g->nbatches;
       st.edges_scanned += (double)g->ne;

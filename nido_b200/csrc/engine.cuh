@@ -99,7 +99,13 @@ struct nido_graph_s {
   int64_t nv0 = 0;           // original vertex count
   int64_t nv = 0, ne = 0;    // current phase
   int64_t cap_v = 0, cap_e = 0;
-  int nbatches = 1;
+  int nbatches = 1;          // batches of the current phase
+  int nb_user = 1;           // the -b the graph was uploaded with
+  // conflict-free batches: every phase colours the current graph (JPL, seed
+  // kColorBatchSeed) and its colour classes are the batches, in colour order
+  bool color_mode = false;
+  int32_t* vcolor = nullptr; // colour of every current vertex (color_mode)
+  int64_t cap_vcolor = 0;
   // every weight of the current phase integral and every vertex's sum of |w|
   // below 2^31 (set with k_v each phase; the move phase then sums in int32)
   bool int_weights = false;
@@ -255,6 +261,11 @@ cudaError_t pinned_buffer(nido_ctx_s* ctx, size_t bytes, void** p);
 int device_alloc(nido_ctx_s* ctx, void** p, size_t bytes);
 void device_free(nido_ctx_s* ctx, void* p, size_t bytes);
 int build_batches(nido_graph_s* g);                     // cuts (host) + tier lists
+// the commit of batch b: the vertex range [cuts[b], cuts[b+1]), or with
+// colour-class batches the batch's vertices in the tier lists
+int launch_commit_batch(nido_graph_s* g, int b);
+constexpr uint64_t kColorBatchSeed = 1;
+int color_current_graph(nido_graph_s* g, uint64_t seed, int32_t* colors, int64_t* ncolors);  // color.cu
 // move phase (move.cu)
 // ev_start / ev_end (may be null) are recorded around the tier kernels
 int launch_move(nido_graph_s* g, int batch, int tie, cudaEvent_t ev_start, cudaEvent_t ev_end);

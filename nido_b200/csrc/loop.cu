@@ -156,7 +156,7 @@ int device_phase_loop(nido_graph_s* g, int tie, double tau, int64_t max_iter, bo
         NIDO_TRY(launch_move_tiers(g, b, tie));
         k_lap<<<1, 1, 0, s>>>(&ctl->t_move, &ctl->move_ns);
         NIDO_LAUNCH_CHECK();
-        NIDO_TRY(launch_commit(g, g->cuts[b], g->cuts[b + 1]));
+        NIDO_TRY(launch_commit_batch(g, b));
       }
       k_stamp<<<1, 1, 0, s>>>(&ctl->t_q);
       NIDO_LAUNCH_CHECK();

@@ -2,7 +2,9 @@
 //   nido_louvain -f graph.bin [-b nbatches] [-t threshold] [-i maxIter] [-c] [-o out]
 // Same options, defaults (types.hpp:24-38) and stdout lines.  -r (random BA
 // graph) is not provided; -p accepts only the default "1 1".  --tie=nido
-// selects the reference's tie rule for parity runs.
+// selects the reference's tie rule for parity runs; --color-batches sweeps
+// every phase's colour classes as conflict-free batches instead of the -b
+// cuts.
 #include <getopt.h>
 #include <omp.h>
 #include <stdio.h>
@@ -23,8 +25,11 @@ int main(int argc, char** argv) {
   long long maxLoops = 500;
   double tau = 1.0E-06;
   int tie = NIDO_TIE_SMALLEST_ID;
-  for (int i = 1; i < argc; ++i)
+  bool color_batches = false;
+  for (int i = 1; i < argc; ++i) {
     if (strcmp(argv[i], "--tie=nido") == 0) { tie = NIDO_TIE_NIDO; argv[i] = (char*)"--"; }
+    if (strcmp(argv[i], "--color-batches") == 0) { color_batches = true; argv[i] = (char*)"--"; }
+  }
   int ret;
   optind = 1;
   while ((ret = getopt(argc, argv, "f:p:r:cb:i:t:ho:")) != -1) {
@@ -72,12 +77,14 @@ int main(int argc, char** argv) {
     printf("Coloring Time: %g s\n", omp_get_wtime() - t0);
     GraphGPU graph_gpu(&graph, nbatches, ctx);
     graph_gpu.set_tie_rule(tie);
+    graph_gpu.set_color_batches(color_batches);
     LouvainGPU louvain(maxLoops, tau, nbatches);
     louvain.run(&graph_gpu);
     if (output_communities) graph_gpu.dump_partition(outFileName, new_orders);
   } else {  // the file streams to the device
     GraphGPU graph_gpu(inputFileName, nbatches, ctx);
     graph_gpu.set_tie_rule(tie);
+    graph_gpu.set_color_batches(color_batches);
     printf("#Batches: %d\n#Threshold: %g\nMax #iterations: %lld\n#NGPUs: 1\n", nbatches, tau, maxLoops);
     printf("--------------------------------------\n");
     LouvainGPU louvain(maxLoops, tau, nbatches);

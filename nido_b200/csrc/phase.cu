@@ -179,6 +179,44 @@ __global__ void k_commit(int64_t v0, int64_t v1, const double* __restrict__ k,
   }
 }
 
+// The vertices of one batch as ranges of perm (one per degree tier).
+struct PermSpans {
+  int64_t start[kNumTiers];
+  int64_t pre[kNumTiers + 1];  // prefix of the range lengths
+};
+
+// k_commit over the vertices of PermSpans (a colour-class batch); movers of a
+// warp with the same old (new) community add their k_v first, as k_commit does
+__global__ void k_commit_spans(PermSpans r, const int32_t* __restrict__ perm, const double* __restrict__ k,
+                               int32_t* __restrict__ comm, int32_t* __restrict__ newc, double* __restrict__ a) {
+  const int64_t total = r.pre[kNumTiers];
+  const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+  for (int64_t base = blockIdx.x * (int64_t)blockDim.x + (threadIdx.x & ~31); base < total; base += stride) {
+    const int64_t x = base + (threadIdx.x & 31);
+    const bool in = x < total;
+    int v = 0;
+    int32_t src = 0, dst = 0;
+    double kv = 0.;
+    if (in) {
+      int t = 0;
+      while (r.pre[t + 1] <= x) ++t;
+      v = perm[r.start[t] + (x - r.pre[t])];
+      src = comm[v];
+      dst = newc[v];
+    }
+    const bool mv = in && src != dst;
+    if (mv) kv = k[v];
+    if (__any_sync(NIDO_FULL_MASK, mv)) {
+      warp_community_add(a, src, -kv, mv);
+      warp_community_add(a, dst, kv, mv);
+    }
+    if (in) {
+      comm[v] = dst;
+      newc[v] = src;
+    }
+  }
+}
+
 // ---- modularity -------------------------------------------------------------------
 // Sum of w[j] over j = j0, j0+step, ... < e with comm[adj[j]] == own, added in
 // that order; four edges' loads (bounds-guarded) are issued before any is
@@ -367,7 +405,7 @@ __global__ void k_tier_keys(const int64_t* __restrict__ off, int64_t nv, const i
                             int64_t* __restrict__ counts, unsigned long long* __restrict__ maxdeg,
                             const int32_t* __restrict__ gid, const int64_t* __restrict__ gbase,
                             const int64_t* __restrict__ gcuts, const int32_t* __restrict__ gactive,
-                            int32_t* __restrict__ vbatch, TierThresholds thr) {
+                            int32_t* __restrict__ vbatch, const int32_t* __restrict__ vcolor, TierThresholds thr) {
   const int lane = threadIdx.x & 31;
   const uint32_t skip = (uint32_t)(kNumTiers * nb);
   unsigned long long md = 0;
@@ -386,9 +424,13 @@ __global__ void k_tier_keys(const int64_t* __restrict__ off, int64_t nv, const i
         active = gactive[g] != 0;
       }
       int lo = 0, hi = nb;  // batch b with c[b] <= x < c[b+1]
-      while (hi - lo > 1) {
-        const int mid = (lo + hi) / 2;
-        if (c[mid] <= x) lo = mid; else hi = mid;
+      if (vcolor) {
+        lo = vcolor[v];  // colour-class batches
+      } else {
+        while (hi - lo > 1) {
+          const int mid = (lo + hi) / 2;
+          if (c[mid] <= x) lo = mid; else hi = mid;
+        }
       }
       if (vbatch) vbatch[v] = lo;
       const int64_t d = off[v + 1] - off[v];
@@ -452,6 +494,26 @@ int launch_commit(nido_graph_s* g, int64_t v0, int64_t v1) {
   if (v1 <= v0) return NIDO_OK;
   k_commit<<<grid_for(v1 - v0, kThreads), kThreads, 0, g->ctx->stream>>>(v0, v1, g->k, g->comm,
                                                                          g->newc, g->a, nullptr, nullptr);
+  NIDO_LAUNCH_CHECK();
+  return NIDO_OK;
+}
+
+int launch_commit_batch(nido_graph_s* g, int b) {
+  if (b < 0 || b >= g->nbatches) return nido_set_error(NIDO_E_INVALID, "batch %d out of range", b);
+  if (!g->color_mode || g->gid) return launch_commit(g, g->cuts[b], g->cuts[b + 1]);
+  // a colour class is not a vertex range: commit the batch's vertices from
+  // the tier lists, every (tier, batch) range of perm
+  PermSpans r{};
+  int64_t tot = 0;
+  const int nb = g->nbatches;
+  for (int t = 0; t < kNumTiers; ++t) {
+    r.start[t] = g->tier_off[(size_t)t * nb + b];
+    r.pre[t] = tot;
+    tot += g->tier_off[(size_t)t * nb + b + 1] - r.start[t];
+  }
+  r.pre[kNumTiers] = tot;
+  if (tot == 0) return NIDO_OK;
+  k_commit_spans<<<grid_for(tot, kThreads), kThreads, 0, g->ctx->stream>>>(r, g->perm, g->k, g->comm, g->newc, g->a);
   NIDO_LAUNCH_CHECK();
   return NIDO_OK;
 }
@@ -598,6 +660,23 @@ int launch_modularity_dev(nido_graph_s* g) {
 
 int build_batches(nido_graph_s* g) {
   cudaStream_t s = g->ctx->stream;
+  const bool multi = g->gid != nullptr;  // many graphs: per-graph cuts in g->gcuts
+  const bool colored = g->color_mode && !multi;
+  if (colored) {
+    // conflict-free batches: the colour classes of the current graph
+    if (g->cap_vcolor < g->nv) {
+      raw_free(g->ctx, g->vcolor);
+      g->vcolor = nullptr;
+      g->cap_vcolor = 0;
+      NIDO_CUDA_TRY(raw_alloc(g->ctx, (void**)&g->vcolor, sizeof(int32_t) * (size_t)std::max<int64_t>(g->nv, 1)));
+      g->cap_vcolor = std::max<int64_t>(g->nv, 1);
+    }
+    int64_t nc = 0;
+    NIDO_TRY(color_current_graph(g, kColorBatchSeed, g->vcolor, &nc));
+    g->nbatches = (int)std::max<int64_t>(nc, 1);
+  } else if (!multi) {
+    g->nbatches = g->nb_user;
+  }
   const int nb = g->nbatches;
   const int64_t nv = g->nv;
   Arena ar(g->scratch, g->scratch_bytes);
@@ -611,8 +690,7 @@ int build_batches(nido_graph_s* g) {
   uint32_t* vals2 = ar.take<uint32_t>(nv);
   int64_t* rtemp = ar.take<int64_t>(std::max(radix_temp_elems(nv), scan_temp_elems(nkeys)));
   if (!rtemp) return nido_set_error(NIDO_E_NOMEM, "scratch arena too small (batches)");
-  const bool multi = g->gid != nullptr;  // many graphs: per-graph cuts in g->gcuts
-  if (!multi) {
+  if (!multi && !colored) {
     k_batch_cuts<<<1, 1, 0, s>>>(g->off, nv, nb, dcuts, dparts);
     NIDO_LAUNCH_CHECK();
   }
@@ -621,7 +699,7 @@ int build_batches(nido_graph_s* g) {
   if (nv > 0) {
     k_tier_keys<<<grid_for(nv, kThreads), kThreads, 0, s>>>(g->off, nv, dcuts, nb, keys, (uint32_t*)g->perm,
                                                            counts, maxdeg, g->gid, g->gbase, g->gcuts,
-                                                           g->gactive, g->vbatch,
+                                                           g->gactive, g->vbatch, colored ? g->vcolor : nullptr,
                                                            TierThresholds{g->cfg.warp_max, g->cfg.ctas_max,
                                                                           g->cfg.ctam_max, g->cfg.ctal_max,
                                                                           g->cfg.ctax_max});
@@ -634,7 +712,7 @@ int build_batches(nido_graph_s* g) {
   g->cuts.assign(nb + 1, 0);
   g->tier_off.assign(nkeys + 1, 0);
   unsigned long long md = 0;
-  if (!multi)
+  if (!multi && !colored)
     NIDO_CUDA_TRY(cudaMemcpyAsync(g->cuts.data(), dcuts, sizeof(int64_t) * (nb + 1), cudaMemcpyDeviceToHost, s));
   NIDO_CUDA_TRY(cudaMemcpyAsync(g->tier_off.data(), counts, sizeof(int64_t) * (nkeys + 1), cudaMemcpyDeviceToHost, s));
   NIDO_CUDA_TRY(cudaMemcpyAsync(&md, maxdeg, sizeof(md), cudaMemcpyDeviceToHost, s));

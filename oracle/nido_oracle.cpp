@@ -253,6 +253,83 @@ extern "C" void orc_move_gain(int64_t nv, const int64_t* off, const int64_t* adj
   }
 }
 
+// The move step over the vertices of a list (a colour class).
+static void move_list(int64_t nv, const int64_t* off, const int64_t* adj, const double* w, const int64_t* comm,
+                      const double* a, const double* k, double m, const std::vector<int64_t>& list, int tie,
+                      int64_t* newcomm) {
+#pragma omp parallel
+  {
+    MoveScratch s;
+    s.acc.assign(nv, 0.);
+    s.seen.assign(nv, 0);
+#pragma omp for schedule(dynamic, 256)
+    for (int64_t i = 0; i < (int64_t)list.size(); ++i)
+      move_one(list[i], off, adj, w, comm, a, k, m, tie, s, newcomm, nullptr);
+  }
+}
+
+static void commit_list(const std::vector<int64_t>& list, int64_t* comm, int64_t* newcomm, const double* k,
+                        double* a) {
+  for (int64_t v : list) {
+    const int64_t src = comm[v], dst = newcomm[v];
+    if (src != dst) { a[src] += -k[v]; a[dst] += k[v]; }
+  }
+  for (int64_t v : list) { int64_t t = comm[v]; comm[v] = newcomm[v]; newcomm[v] = t; }
+}
+
+// Jones-Plassmann-Luby colouring as the engine runs it (color.cu): in rounds,
+// every uncoloured vertex whose (hashed priority, id) beats all its uncoloured
+// neighbours takes the smallest colour no coloured neighbour has; a round
+// sees only the colours of earlier rounds.  Deterministic for a seed.
+static inline uint64_t jpl_prio(uint64_t seed, int64_t v) {
+  uint64_t z = seed + 0x9E3779B97F4A7C15ull * (uint64_t)(v + 1);
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+
+extern "C" int64_t orc_color_jpl(int64_t nv, const int64_t* off, const int64_t* adj, uint64_t seed,
+                                 int64_t* colors) {
+  std::vector<int64_t> cin(nv, -1), cout(nv, -1);
+  int64_t left = nv;
+  while (left > 0) {
+#pragma omp parallel for schedule(dynamic, 1024)
+    for (int64_t v = 0; v < nv; ++v) {
+      if (cin[v] >= 0) continue;
+      const uint64_t pv = jpl_prio(seed, v);
+      bool beaten = false;
+      for (int64_t j = off[v]; j < off[v + 1] && !beaten; ++j) {
+        const int64_t u = adj[j];
+        if (u == v || cin[u] >= 0) continue;
+        const uint64_t pu = jpl_prio(seed, u);
+        if (pu > pv || (pu == pv && u > v)) beaten = true;
+      }
+      if (beaten) continue;
+      std::vector<char> used;
+      for (int64_t j = off[v]; j < off[v + 1]; ++j) {
+        const int64_t c = cin[adj[j]];
+        if (c < 0) continue;
+        if ((int64_t)used.size() <= c) used.resize(c + 1, 0);
+        used[c] = 1;
+      }
+      int64_t c = 0;
+      while (c < (int64_t)used.size() && used[c]) ++c;
+      cout[v] = c;
+    }
+    left = 0;
+    for (int64_t v = 0; v < nv; ++v) {
+      cin[v] = cout[v];
+      left += cin[v] < 0;
+    }
+  }
+  int64_t nc = 0;
+  for (int64_t v = 0; v < nv; ++v) {
+    colors[v] = cin[v];
+    nc = std::max(nc, cin[v] + 1);
+  }
+  return nc;
+}
+
 extern "C" void orc_move(int64_t nv, const int64_t* off, const int64_t* adj, const double* w,
                          const int64_t* comm, const double* a, const double* k, double m,
                          int64_t v0, int64_t v1, int tie, int64_t* newcomm) {
@@ -440,10 +517,24 @@ extern "C" int orc_louvain(int64_t nv0, const int64_t* off0, const int64_t* adj0
                             clustering, st);
 }
 
+extern "C" int orc_louvain_ex(int64_t nv0, const int64_t* off0, const int64_t* adj0, const double* w0,
+                              int nbatches, double tau, int64_t max_loops, int tie, int verbose, int max_phases,
+                              int color_batches, int64_t* clustering, orc_stats* st);
+
 extern "C" int orc_louvain_capped(int64_t nv0, const int64_t* off0, const int64_t* adj0,
                                   const double* w0, int nbatches, double tau, int64_t max_loops,
                                   int tie, int verbose, int max_phases, int64_t* clustering,
                                   orc_stats* st) {
+  return orc_louvain_ex(nv0, off0, adj0, w0, nbatches, tau, max_loops, tie, verbose, max_phases, 0, clustering,
+                        st);
+}
+
+// With color_batches, every phase colours its graph (orc_color_jpl, seed 1)
+// and its colour classes, in colour order and ascending id within a class,
+// are the batches instead of the -b cuts.
+extern "C" int orc_louvain_ex(int64_t nv0, const int64_t* off0, const int64_t* adj0, const double* w0,
+                              int nbatches, double tau, int64_t max_loops, int tie, int verbose, int max_phases,
+                              int color_batches, int64_t* clustering, orc_stats* st) {
   if (nbatches < 1) return -1;
   memset(st, 0, sizeof(*st));
   std::vector<int64_t> off(off0, off0 + nv0 + 1), adj(adj0, adj0 + off0[nv0]);
@@ -460,15 +551,30 @@ extern "C" int orc_louvain_capped(int64_t nv0, const int64_t* off0, const int64_
   while (!done && phases < 200 && phases < max_phases) {
     if (verbose) printf("PHASE #%lld: \n", (long long)phases);
     orc_singleton(nv, k.data(), comm.data(), newcomm.data(), a.data());
+    std::vector<std::vector<int64_t>> classes;
+    if (color_batches) {
+      std::vector<int64_t> col(nv);
+      const int64_t nc = orc_color_jpl(nv, off.data(), adj.data(), 1, col.data());
+      classes.assign((size_t)std::max<int64_t>(nc, 1), {});
+      for (int64_t v = 0; v < nv; ++v) classes[col[v]].push_back(v);
+    }
     double Q = orc_modularity(nv, off.data(), adj.data(), w.data(), comm.data(), a.data(), m);
     const double Q_old = Q;
     double dQ = kMaxFloat;
     int64_t loops = 0;
     while (tau < dQ && loops < max_loops) {
+      if (color_batches) {
+        for (const std::vector<int64_t>& cls : classes) {
+          move_list(nv, off.data(), adj.data(), w.data(), comm.data(), a.data(), k.data(), m, cls, tie,
+                    newcomm.data());
+          commit_list(cls, comm.data(), newcomm.data(), k.data(), a.data());
+        }
+      } else {
       for (int b = 0; b < nbatches; ++b) {
         orc_move(nv, off.data(), adj.data(), w.data(), comm.data(), a.data(), k.data(), m,
                  cuts[b], cuts[b + 1], tie, newcomm.data());
         orc_commit(cuts[b], cuts[b + 1], comm.data(), newcomm.data(), k.data(), a.data());
+      }
       }
       const double Qtmp = orc_modularity(nv, off.data(), adj.data(), w.data(), comm.data(), a.data(), m);
       dQ = Qtmp - Q;

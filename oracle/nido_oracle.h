@@ -121,6 +121,15 @@ double orc_partition_modularity(int64_t nv, const int64_t* off, const int64_t* a
 /* Normalised mutual information of two labelings (arithmetic-mean normaliser). */
 double orc_nmi(int64_t n, const int64_t* a, const int64_t* b);
 
+/* Jones-Plassmann-Luby colouring as the engine runs it (hashed priorities,
+ * rounds that see only earlier rounds' colours); returns the colour count. */
+int64_t orc_color_jpl(int64_t nv, const int64_t* off, const int64_t* adj, uint64_t seed, int64_t* colors);
+/* orc_louvain_capped plus color_batches: every phase's JPL colour classes
+ * (seed 1) are its batches, in colour order, instead of the -b cuts. */
+int orc_louvain_ex(int64_t nv0, const int64_t* off0, const int64_t* adj0, const double* w0, int nbatches,
+                   double tau, int64_t max_loops, int tie, int verbose, int max_phases, int color_batches,
+                   int64_t* clustering, orc_stats* st);
+
 #ifdef __cplusplus
 }
 #endif

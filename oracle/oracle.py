@@ -60,6 +60,10 @@ def lib() -> C.CDLL:
                                   C.c_int, _i64p, C.POINTER(Stats)]
         L.orc_louvain_capped.argtypes = [C.c_int64, _i64p, _i64p, _f64p, C.c_int, C.c_double, C.c_int64,
                                          C.c_int, C.c_int, C.c_int, _i64p, C.POINTER(Stats)]
+        L.orc_color_jpl.argtypes = [C.c_int64, _i64p, _i64p, C.c_uint64, _i64p]
+        L.orc_color_jpl.restype = C.c_int64
+        L.orc_louvain_ex.argtypes = [C.c_int64, _i64p, _i64p, _f64p, C.c_int, C.c_double, C.c_int64, C.c_int,
+                                     C.c_int, C.c_int, C.c_int, _i64p, C.c_void_p]
         L.orc_partition_modularity.argtypes = [C.c_int64, _i64p, _i64p, _f64p, _i64p]
         L.orc_partition_modularity.restype = C.c_double
         L.orc_nmi.argtypes = [C.c_int64, _i64p, _i64p]
@@ -181,15 +185,24 @@ def color_nido_seq(off, adj):
 
 
 def louvain(off, adj, w, nbatches=2, tau=1e-6, max_loops=500, tie=TIE_SMALLEST_ID, verbose=False,
-            max_phases=200):
+            max_phases=200, color_batches=False):
     off, adj, w = _i(off), _i(adj), _f(w)
     cl = np.empty(len(off) - 1, np.int64)
     st = Stats()
-    rc = lib().orc_louvain_capped(len(off) - 1, _p(off), _p(adj), _pf(w), nbatches, tau, max_loops, tie,
-                                  int(verbose), max_phases, _p(cl), C.byref(st))
+    rc = lib().orc_louvain_ex(len(off) - 1, _p(off), _p(adj), _pf(w), nbatches, tau, max_loops, tie,
+                              int(verbose), max_phases, int(color_batches), _p(cl),
+                              C.cast(C.byref(st), C.c_void_p))
     if rc:
         raise ValueError("orc_louvain failed")
     return cl, st
+
+
+def color_jpl(off, adj, seed=1):
+    """The engine's Jones-Plassmann-Luby colouring: (colours, colour count)."""
+    off, adj = _i(off), _i(adj)
+    c = np.empty(len(off) - 1, np.int64)
+    nc = lib().orc_color_jpl(len(off) - 1, _p(off), _p(adj), seed, _p(c))
+    return c, nc
 
 
 def partition_modularity(off, adj, w, part):
