@@ -270,21 +270,36 @@ typedef struct {
   double latency_ms;   /* submit -> result in host memory */
   double device_ms;    /* device-event time of the run */
   int64_t hbm_bytes;   /* reservation held against the budget while it ran */
+  int32_t host_edges;  /* 1: admitted over budget, edges in mapped host memory */
+  int32_t pad;
 } nido_request_info;
 /* Device bytes reserved for a graph of this size while it runs: the upload,
  * work buffers and scratch, plus the hub-table and coarsening-plan regions,
  * which are processed in waves and so bounded by max(8M, 4*nv) and
  * max(4M, 4*nv) slots. */
 int64_t nido_graph_footprint(int64_t nv, int64_t ne, int32_t nbatches);
+/* Over-budget graphs (no reference counterpart in this form; the reference
+ * streams edge windows per batch, graph_gpu.cpp:362-417, 967-1042): when a
+ * context with a budget cannot hold a graph's edges in HBM but can hold the
+ * rest, the upload keeps the three CSR copies' edge arrays (12 bytes an edge
+ * each) in page-locked host memory mapped into the device's address space,
+ * and every kernel streams them over the host link as it reads them.  Results
+ * are the in-HBM run's.  This is the HBM such a graph reserves. */
+int64_t nido_graph_footprint_streamed(int64_t nv, int64_t ne, int32_t nbatches);
+/* 1 when the graph's edges are in mapped host memory (see above) */
+int nido_graph_host_edges(nido_graph g, int32_t* host_edges);
 /* Device bytes a graph holds now (upload, scratch, hub tables, plan). */
 int nido_graph_device_bytes(nido_graph g, int64_t* bytes);
 /* nworkers threads, each with its own stream; requests are admitted in
  * arrival order while their footprints fit in the budget (0: all free HBM
- * less 1 GiB; never more than that). */
+ * less 1 GiB; never more than that).  A request whose footprint exceeds the
+ * whole budget runs with its edges in mapped host memory when its streamed
+ * footprint fits (nido_request_info.host_edges). */
 int nido_server_create(int device, size_t hbm_budget_bytes, int32_t nworkers, nido_server* out);
 /* Queues a run of g with p.  g's arrays and out_comm (nv entries, may be
  * NULL) must stay valid until nido_server_wait returns for *ticket.  A
- * request larger than the whole budget is refused (NIDO_E_TOO_LARGE). */
+ * request whose streamed footprint exceeds the whole budget is refused
+ * (NIDO_E_TOO_LARGE). */
 int nido_server_submit(nido_server s, const nido_csr* g, const nido_params* p, int64_t* out_comm,
                        int64_t* ticket);
 /* *state: 0 queued, 1 running, 2 finished */

@@ -66,7 +66,7 @@ class RequestInfo(C.Structure):
     _fields_ = [("status", C.c_int32), ("worker", C.c_int32), ("final_q", C.c_double),
                 ("phases", C.c_int64), ("total_loops", C.c_int64), ("queue_ms", C.c_double),
                 ("run_ms", C.c_double), ("latency_ms", C.c_double), ("device_ms", C.c_double),
-                ("hbm_bytes", C.c_int64)]
+                ("hbm_bytes", C.c_int64), ("host_edges", C.c_int32), ("pad", C.c_int32)]
 
 
 def lib() -> C.CDLL:
@@ -119,6 +119,8 @@ def lib() -> C.CDLL:
             "nido_batch_size": (C.c_int, [vp, C.POINTER(C.c_int32), _i64p, _i64p]),
             "nido_batch_free": (C.c_int, [vp]),
             "nido_graph_footprint": (C.c_int64, [C.c_int64, C.c_int64, C.c_int32]),
+            "nido_graph_footprint_streamed": (C.c_int64, [C.c_int64, C.c_int64, C.c_int32]),
+            "nido_graph_host_edges": (C.c_int, [vp, C.POINTER(C.c_int32)]),
             "nido_get_tier_config": (C.c_int, [vp, C.POINTER(TierConfig)]),
             "nido_set_tier_config": (C.c_int, [vp, C.POINTER(TierConfig)]),
             "nido_tune": (C.c_int, [vp, C.c_int32, C.c_int32, C.POINTER(TierConfig), _f64p]),
@@ -417,6 +419,12 @@ class Graph:
         _check(lib().nido_tune(self.h, tie, sweeps, C.byref(c), C.byref(ms)))
         return c, ms.value
 
+    def host_edges(self) -> bool:
+        """True when the graph's edges are in mapped host memory (over budget)."""
+        x = C.c_int32()
+        _check(lib().nido_graph_host_edges(self.h, C.byref(x)))
+        return bool(x.value)
+
     def device_bytes(self) -> int:
         b = C.c_int64()
         _check(lib().nido_graph_device_bytes(self.h, C.byref(b)))
@@ -506,6 +514,10 @@ class Batch:
 
 def graph_footprint(nv: int, ne: int, nbatches: int = 2) -> int:
     return int(lib().nido_graph_footprint(nv, ne, nbatches))
+
+
+def graph_footprint_streamed(nv: int, ne: int, nbatches: int = 2) -> int:
+    return int(lib().nido_graph_footprint_streamed(nv, ne, nbatches))
 
 
 class Server:

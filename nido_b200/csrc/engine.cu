@@ -113,6 +113,29 @@ int dev_alloc(nido_ctx ctx, T** p, int64_t n) {
   return NIDO_OK;
 }
 
+// Page-locked host memory mapped into the device's address space (with
+// unified addressing the host pointer is also the device pointer).
+template <typename T>
+int host_alloc(T** p, int64_t n) {
+  const size_t bytes = sizeof(T) * (size_t)(n > 0 ? n : 1);
+  void* h = nullptr;
+  const cudaError_t e = cudaHostAlloc(&h, bytes, cudaHostAllocMapped | cudaHostAllocPortable);
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    cudaGetLastError();
+    return nido_set_error(NIDO_E_NOMEM, "cudaHostAlloc(%zu) failed: %s", bytes, cudaGetErrorString(e));
+  }
+  void* d = nullptr;
+  const cudaError_t e2 = cudaHostGetDevicePointer(&d, h, 0);
+  if (e2 != cudaSuccess || d != h) {
+    cudaFreeHost(h);
+    *p = nullptr;
+    return nido_set_error(NIDO_E_CUDA, "mapped host memory is not addressable at its host address");
+  }
+  *p = static_cast<T*>(h);
+  return NIDO_OK;
+}
+
 void dev_free(nido_ctx ctx, void* p, size_t bytes) {
   if (p) {
     nido::raw_free(ctx, p);
@@ -270,8 +293,13 @@ extern "C" int nido_graph_free(nido_graph g) {
   const int64_t V = g->cap_v, E = g->cap_e;
   dev_free(ctx, g->off0, 8 * (V + 1)); dev_free(ctx, g->offA, 8 * (V + 1));
   dev_free(ctx, g->off2, 8 * (V + 1));
-  dev_free(ctx, g->adj0, 4 * E); dev_free(ctx, g->adjA, 4 * E); dev_free(ctx, g->adj2, 4 * E);
-  dev_free(ctx, g->w0, 8 * E); dev_free(ctx, g->wA, 8 * E); dev_free(ctx, g->w2, 8 * E);
+  if (g->host_edges) {
+    for (void* p : {(void*)g->adj0, (void*)g->adjA, (void*)g->adj2, (void*)g->w0, (void*)g->wA, (void*)g->w2})
+      if (p) cudaFreeHost(p);
+  } else {
+    dev_free(ctx, g->adj0, 4 * E); dev_free(ctx, g->adjA, 4 * E); dev_free(ctx, g->adj2, 4 * E);
+    dev_free(ctx, g->w0, 8 * E); dev_free(ctx, g->wA, 8 * E); dev_free(ctx, g->w2, 8 * E);
+  }
   dev_free(ctx, g->k, 8 * V); dev_free(ctx, g->a, 8 * V);
   dev_free(ctx, g->comm, 4 * V); dev_free(ctx, g->newc, 4 * V);
   dev_free(ctx, g->clus, 4 * g->nv0); dev_free(ctx, g->perm, 4 * V);
@@ -309,10 +337,21 @@ int graph_create(nido_ctx ctx, int64_t nv, int64_t ne, int32_t nbatches, nido_gr
   g->nb_user = nbatches;
   const int64_t V = nv, E = ne;
   int st = NIDO_OK;
+  // Over the context's budget, the graph keeps its edge arrays in mapped
+  // page-locked host memory when what is left (vertex state, offsets,
+  // scratch) fits: every kernel then reads the edges over the host link.
+  {
+    const size_t edge_bytes = 36 * (size_t)std::max<int64_t>(E, 1);
+    const size_t vert_bytes = (size_t)nido_graph_footprint_streamed(nv, ne, nbatches);
+    g->host_edges = ctx->budget && ctx->used + edge_bytes + vert_bytes > ctx->budget &&
+                    ctx->used + vert_bytes <= ctx->budget;
+  }
 #define ALLOC(p, n) if (st == NIDO_OK) st = dev_alloc(ctx, &g->p, (n))
+#define EALLOC(p, n) if (st == NIDO_OK) st = g->host_edges ? host_alloc(&g->p, (n)) : dev_alloc(ctx, &g->p, (n))
   ALLOC(off0, V + 1); ALLOC(offA, V + 1); ALLOC(off2, V + 1);
-  ALLOC(adj0, E); ALLOC(adjA, E); ALLOC(adj2, E);
-  ALLOC(w0, E); ALLOC(wA, E); ALLOC(w2, E);
+  EALLOC(adj0, E); EALLOC(adjA, E); EALLOC(adj2, E);
+  EALLOC(w0, E); EALLOC(wA, E); EALLOC(w2, E);
+#undef EALLOC
   ALLOC(k, V); ALLOC(a, V);
   ALLOC(comm, V); ALLOC(newc, V);
   ALLOC(clus, V); ALLOC(perm, V);
@@ -400,8 +439,9 @@ extern "C" int nido_graph_upload(nido_ctx ctx, int64_t nv, int64_t ne, const int
   NIDO_TRY(graph_create(ctx, nv, ne, nbatches, &g));
   cudaStream_t s = ctx->stream;
   cudaError_t e = cudaMemcpyAsync(g->off, off, 8 * (nv + 1), cudaMemcpyHostToDevice, s);
-  if (e == cudaSuccess && ne > 0) e = cudaMemcpyAsync(staged_ids(g), adj, 8 * ne, cudaMemcpyHostToDevice, s);
-  if (e == cudaSuccess && ne > 0) e = cudaMemcpyAsync(g->w, w, 8 * ne, cudaMemcpyHostToDevice, s);
+  // cudaMemcpyDefault: the edge arrays are device or mapped host memory
+  if (e == cudaSuccess && ne > 0) e = cudaMemcpyAsync(staged_ids(g), adj, 8 * ne, cudaMemcpyDefault, s);
+  if (e == cudaSuccess && ne > 0) e = cudaMemcpyAsync(g->w, w, 8 * ne, cudaMemcpyDefault, s);
   if (e != cudaSuccess) return fail_graph(g, nido_set_error(NIDO_E_CUDA, "upload: %s", cudaGetErrorString(e)));
   const int st = graph_finish(g);
   if (st != NIDO_OK) return fail_graph(g, st);
@@ -481,12 +521,18 @@ extern "C" int nido_graph_upload_vite(nido_ctx ctx, const char* path, int32_t nb
 
 extern "C" int nido_graph_device_bytes(nido_graph g, int64_t* bytes) {
   if (!g || !bytes) return nido_set_error(NIDO_E_INVALID, "null argument");
-  const int64_t V = g->cap_v, E = g->cap_e;
+  const int64_t V = g->cap_v, E = g->host_edges ? 0 : g->cap_e;  // mapped host edges hold no HBM
   int64_t b = 24 * (V + 1) + 36 * E + 28 * V + 4 * g->nv0 + 128 + (int64_t)g->scratch_bytes;
   b += 12 * g->gslab + 8 * g->hub_cap_items + 4 * (g->hub_cap_hubs_v + g->hub_cap_hubs_c + g->hub_cap_hubs_s +
                                                    g->hub_cap_hubs_d) +
        8 * (g->hub_cap_hubs_t + g->hub_cap_slices + g->hub_cap_first) + g->hub_cap_res + (int64_t)g->agg_buf_bytes + 4 * g->pm32_cap;
   *bytes = b;
+  return NIDO_OK;
+}
+
+extern "C" int nido_graph_host_edges(nido_graph g, int32_t* host_edges) {
+  if (!g || !host_edges) return nido_set_error(NIDO_E_INVALID, "null argument");
+  *host_edges = g->host_edges ? 1 : 0;
   return NIDO_OK;
 }
 
@@ -502,12 +548,12 @@ extern "C" int nido_graph_download(nido_graph g, int64_t* off, int64_t* adj, dou
   cudaStream_t s = g->ctx->stream;
   NIDO_CUDA_TRY(cudaSetDevice(g->ctx->device));
   if (off) NIDO_CUDA_TRY(cudaMemcpyAsync(off, g->off, 8 * (g->nv + 1), cudaMemcpyDeviceToHost, s));
-  if (w && g->ne) NIDO_CUDA_TRY(cudaMemcpyAsync(w, g->w, 8 * g->ne, cudaMemcpyDeviceToHost, s));
+  if (w && g->ne) NIDO_CUDA_TRY(cudaMemcpyAsync(w, g->w, 8 * g->ne, cudaMemcpyDefault, s));
   if (adj && g->ne) {
     int64_t* tmp = reinterpret_cast<int64_t*>(g->w2);  // ne doubles, free outside coarsening
     k_widen<<<kGrid, 256, 0, s>>>(g->adj, g->ne, tmp);
     NIDO_LAUNCH_CHECK();
-    NIDO_CUDA_TRY(cudaMemcpyAsync(adj, tmp, 8 * g->ne, cudaMemcpyDeviceToHost, s));
+    NIDO_CUDA_TRY(cudaMemcpyAsync(adj, tmp, 8 * g->ne, cudaMemcpyDefault, s));
   }
   NIDO_CUDA_TRY(cudaStreamSynchronize(s));
   return NIDO_OK;

@@ -216,6 +216,10 @@ struct nido_graph_s {
   std::vector<MoveGraph> move_graphs;
   int64_t plan_epoch = 0;
   bool use_graphs = true;
+  // over-budget graphs: the edge arrays (adj0/w0, adjA/wA, adj2/w2) live in
+  // page-locked host memory mapped into the device's address space, and the
+  // kernels stream them over the host link as they read them
+  bool host_edges = false;
   // device-resident iteration loop (loop.cu): its control block and per-loop log
   char* loop_buf = nullptr;
   size_t loop_bytes = 0;

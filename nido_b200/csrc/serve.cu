@@ -43,6 +43,7 @@ struct Request {
   int64_t bytes = 0;
   int state = 0;  // 0 queued, 1 running, 2 finished
   bool claimed = false;  // a nido_server_wait is blocked on it
+  bool streamed = false; // admitted over budget: edges in mapped host memory
   nido_request_info info{};
   std::string err;
   double t_submit = 0, t_start = 0;
@@ -93,7 +94,11 @@ void worker_loop(nido_server_s* S, int wid) {
     nido_graph g = nullptr;
     nido_run_stats st;
     memset(&st, 0, sizeof(st));
+    // a streamed request's context budget is its reservation, which leaves
+    // the edge arrays to mapped host memory
+    if (r->streamed) ctx->budget = (size_t)r->bytes;
     int rc = nido_graph_upload(ctx, r->g.nv, r->g.ne, r->g.off, r->g.adj, r->g.w, r->p.nbatches, &g);
+    ctx->budget = 0;
     if (rc == NIDO_OK) rc = nido_run(g, &r->p, r->out, &st);
     std::string err = rc == NIDO_OK ? std::string() : std::string(nido_last_error());
     nido_graph_free(g);
@@ -115,6 +120,7 @@ void worker_loop(nido_server_s* S, int wid) {
       in.device_ms = st.total_ms;
       in.hbm_bytes = r->bytes;
       in.worker = wid;
+      in.host_edges = r->streamed ? 1 : 0;
     }
     S->cv_work.notify_all();  // memory came back: the head may fit now
     S->cv_done.notify_all();
@@ -129,6 +135,12 @@ void worker_loop(nido_server_s* S, int wid) {
 // plan's region for giant communities, one wave at 16 bytes a slot (at most
 // 4M slots or one table of up to 4*nv), grown by a quarter, plus its
 // per-vertex and per-segment lists; and the hub work lists.
+// The same with the edge arrays (three CSR copies of 12 bytes an edge) in
+// mapped host memory, as over-budget graphs keep them.
+extern "C" int64_t nido_graph_footprint_streamed(int64_t nv, int64_t ne, int32_t nbatches) {
+  return nido_graph_footprint(nv, ne, nbatches) - 36 * std::max<int64_t>(ne, 1);
+}
+
 extern "C" int64_t nido_graph_footprint(int64_t nv, int64_t ne, int32_t nbatches) {
   (void)nbatches;
   const int64_t V = std::max<int64_t>(nv, 1), E = std::max<int64_t>(ne, 1);
@@ -207,6 +219,7 @@ extern "C" int nido_server_submit(nido_server S, const nido_csr* g, const nido_p
   if (!S || !g || !p || !ticket) return nido_set_error(NIDO_E_INVALID, "nido_server_submit: null argument");
   if (p->nbatches < 1) return nido_set_error(NIDO_E_INVALID, "nbatches must be >= 1");
   const int64_t bytes = nido_graph_footprint(g->nv, g->ne, p->nbatches);
+  const int64_t bytes_streamed = nido_graph_footprint_streamed(g->nv, g->ne, p->nbatches);
   Request* r = new (std::nothrow) Request();
   if (!r) return nido_set_error(NIDO_E_NOMEM, "host allocation failed");
   r->g = *g;
@@ -218,9 +231,16 @@ extern "C" int nido_server_submit(nido_server S, const nido_csr* g, const nido_p
   {
     std::lock_guard<std::mutex> lk(S->mu);
     if (bytes > S->budget) {
-      delete r;
-      return nido_set_error(NIDO_E_TOO_LARGE, "request needs %lld bytes; the HBM budget is %lld",
-                            (long long)bytes, (long long)S->budget);
+      // over the budget in HBM: admitted with its edges in mapped host memory
+      // when the rest fits, refused otherwise
+      if (bytes_streamed > S->budget) {
+        delete r;
+        return nido_set_error(NIDO_E_TOO_LARGE, "request needs %lld bytes (%lld with its edges on the host); "
+                              "the HBM budget is %lld", (long long)bytes, (long long)bytes_streamed,
+                              (long long)S->budget);
+      }
+      r->bytes = bytes_streamed;
+      r->streamed = true;
     }
     if (S->stop) {
       delete r;
