@@ -312,6 +312,7 @@ def run_ours(args, world, rank, local):
         "graph_size": {"nv": G.nv, "ne": G.ne}, "device_layout": "int32 ids, int64 offsets, FP64 weights",
         "edges_scanned_per_s": world * edges_per_run * args.steps / sec,
         "move_sweeps_per_run": sweeps / args.steps, "final_q": final_q,
+        "loop_graph_build_ms_per_run": sum(s.host_ms[7] for s in stats) / n,
         "breakdown_ms_per_run": breakdown,
         "e2e": {"value": world * args.steps / (e2e_ms * 1e-3), "unit": "graphs/s",
                 "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
@@ -457,6 +458,7 @@ def run_many(args, world, rank, local):
         "clocks": clocks,
         "gpu_launches": launches,
         "kernel_launches_per_step": launches / args.steps,
+        "loop_graph_build_ms_per_step": sum(r[4].host_ms[7] for r in runs) / len(runs),
         "latency_ms": serving["latency_ms"] if serving else None,
         "serving": ({k: serving[k] for k in ("graphs_per_s", "requests", "latency_ms", "overlap", "workload")}
                     if serving else None),

@@ -92,7 +92,8 @@ typedef struct {
   /* host wall time per section (ms): [0] restart from the uploaded graph,
    * [1] enqueueing moves and commits, [2] modularity including the wait for
    * the device, [3] aggregation, [4] per-phase preparation after
-   * aggregation, [5] download of the clustering, [6] autotuning */
+   * aggregation, [5] download of the clustering, [6] autotuning, [7] capture
+   * and instantiation of the device-resident loop graphs */
   double host_ms[8];
   double q_phase[200];
   int64_t loops_phase[200];

@@ -782,6 +782,7 @@ extern "C" int nido_batch_run(nido_batch B, const nido_params* p, int64_t* out_c
         return NIDO_OK;
       }
       const uint64_t l0 = nido_launch_count();
+      const auto tb0 = std::chrono::steady_clock::now();
       NIDO_CUDA_TRY(cudaStreamBeginCaptureToGraph(s, cp.conditional.phGraph_out[0], nullptr, nullptr, 0,
                                                   cudaStreamCaptureModeThreadLocal));
       auto body = [&]() -> int {
@@ -818,6 +819,7 @@ extern "C" int nido_batch_run(nido_batch B, const nido_params* p, int64_t* out_c
         lg.exec = nullptr;
         return nido_set_error(NIDO_E_CUDA, "sweep-loop graph instantiation failed: %s", cudaGetErrorString(ie));
       }
+      st.host_ms[7] += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tb0).count();
       NIDO_CUDA_TRY(cudaGraphLaunch(lg.exec, s));
       BatchCtl hc;
       NIDO_CUDA_TRY(cudaMemcpyAsync(&hc, ctl, sizeof(hc), cudaMemcpyDeviceToHost, s));

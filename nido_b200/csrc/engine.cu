@@ -1021,6 +1021,7 @@ extern "C" int nido_run(nido_graph g, const nido_params* p, int64_t* out_comm, n
         loops = r.loops;
         st.move_ms += r.move_ms;
         st.q_ms += r.q_ms;
+        st.host_ms[7] += r.build_ms;
         st.move_launches += g->nbatches * loops;
         st.edges_scanned += (double)g->ne * (double)loops;
         st.move_bytes += (16.0 * (double)g->ne + 32.0 * (double)g->nv) * (double)loops;

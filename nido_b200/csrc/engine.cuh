@@ -285,6 +285,7 @@ struct PhaseLoop {
   double q_old = 0., q = 0.;
   int64_t loops = 0;
   double move_ms = 0., q_ms = 0.;
+  double build_ms = 0.;     // host time to capture and instantiate the loop graph
   std::vector<double> log;  // Qtmp, dQ of every iteration (with want_log)
 };
 int device_phase_loop(nido_graph_s* g, int tie, double tau, int64_t max_iter, bool want_log, PhaseLoop* r,

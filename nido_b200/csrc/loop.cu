@@ -15,6 +15,7 @@
 // runs after everything before it has finished).
 #include <string.h>
 
+#include <chrono>
 #include <vector>
 
 #include "common.cuh"
@@ -128,6 +129,7 @@ int device_phase_loop(nido_graph_s* g, int tie, double tau, int64_t max_iter, bo
   NIDO_LAUNCH_CHECK();
   uint64_t body_kernels = 0;
   GraphHolder gh;
+  const auto tb0 = std::chrono::steady_clock::now();
   if (max_iter > 0) {
     NIDO_CUDA_TRY(cudaGraphCreate(&gh.graph, 0));
     cudaGraphConditionalHandle h;
@@ -179,6 +181,7 @@ int device_phase_loop(nido_graph_s* g, int tie, double tau, int64_t max_iter, bo
       gh.exec = nullptr;
       return nido_set_error(NIDO_E_CUDA, "phase-loop graph instantiation failed: %s", cudaGetErrorString(ie));
     }
+    r->build_ms = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - tb0).count();
     NIDO_CUDA_TRY(cudaGraphLaunch(gh.exec, s));
   }
   LoopCtl hc;
