@@ -26,10 +26,13 @@ int main(int argc, char** argv) {
   double tau = 1.0E-06;
   int tie = NIDO_TIE_SMALLEST_ID;
   bool color_batches = false;
+  int kept = 1;  // the long options are taken out before getopt sees the rest
   for (int i = 1; i < argc; ++i) {
-    if (strcmp(argv[i], "--tie=nido") == 0) { tie = NIDO_TIE_NIDO; argv[i] = (char*)"--"; }
-    if (strcmp(argv[i], "--color-batches") == 0) { color_batches = true; argv[i] = (char*)"--"; }
+    if (strcmp(argv[i], "--tie=nido") == 0) tie = NIDO_TIE_NIDO;
+    else if (strcmp(argv[i], "--color-batches") == 0) color_batches = true;
+    else argv[kept++] = argv[i];
   }
+  argc = kept;
   int ret;
   optind = 1;
   while ((ret = getopt(argc, argv, "f:p:r:cb:i:t:ho:")) != -1) {

@@ -205,13 +205,56 @@ struct Table {
   int* nocc;
   unsigned mask;
   bool ints = false;  // shared-memory tables of integer-weight phases
+  // integer-weight phases in shared memory: one 64-bit word a slot, the
+  // community id in the high half (-1: empty) and the int32 sum in the low
+  // half, so an insert and its first add are one compare-and-swap (keys and
+  // vals are unused then)
+  unsigned long long* slots = nullptr;
 };
+
+constexpr unsigned long long kEmptySlot = 0xFFFFFFFF00000000ull;
+__device__ __forceinline__ int slot_key(unsigned long long x) { return (int)(x >> 32); }
+__device__ __forceinline__ int slot_sum(unsigned long long x) { return (int)(unsigned)x; }
 
 __device__ __forceinline__ int* int_slot(const Table& t, unsigned h) { return reinterpret_cast<int*>(t.vals + h); }
 
 // e_vc of a slot of a shared-memory table
 __device__ __forceinline__ double table_val(const Table& t, int slot) {
+  if (t.slots) return (double)slot_sum(t.slots[slot]);
   return t.ints ? (double)*int_slot(t, (unsigned)slot) : t.vals[slot];
+}
+
+__device__ __forceinline__ int table_key(const Table& t, int slot) {
+  return t.slots ? slot_key(t.slots[slot]) : t.keys[slot];
+}
+
+// Adds the integer w to key c's sum in a packed table, inserting c when
+// absent (the insert carries w); returns the slot.  Sums are int32 adds on
+// the slot's low half, exact in any order (integer weights, every vertex's
+// sum of |w| below 2^31).
+__device__ __forceinline__ int table_add_packed(const Table& t, int c, int w, bool& isnew, unsigned long long* err) {
+  unsigned h = hash_slot(c, t.mask);
+  volatile unsigned long long* vs = t.slots;
+  isnew = false;
+  for (unsigned probe = 0; probe <= t.mask; ++probe) {
+    int k = slot_key(vs[h]);
+    if (k == -1) {
+      const unsigned long long mine = ((unsigned long long)(unsigned)c << 32) | (unsigned)w;
+      const unsigned long long old = atomicCAS(&t.slots[h], kEmptySlot, mine);
+      if (old == kEmptySlot) {
+        isnew = true;
+        return (int)h;
+      }
+      k = slot_key(old);
+    }
+    if (k == c) {
+      atomicAdd(reinterpret_cast<int*>(&t.slots[h]), w);
+      return (int)h;
+    }
+    h = (h + 1) & t.mask;
+  }
+  atomicAdd(err, 1ull);
+  return -1;
 }
 
 // Adds e to key c's value, inserting c when absent; returns the slot and
@@ -302,6 +345,21 @@ __device__ __forceinline__ void accumulate_edges(const MoveArgs& p, int v, int64
       c[k] = u[k] >= 0 ? p.comm[u[k]] : -1;
       if (u[k] == v) wt[k] = 0.;
     }
+    if (!kGlobal && t.slots) {
+      // packed integer table: every lane adds its own edge (native 32-bit
+      // shared-memory atomics, exact in any order), no fold across lanes
+#pragma unroll
+      for (int k = 0; k < kUnroll; ++k) {
+        const bool ok = u[k] >= 0;
+        if (!__any_sync(NIDO_FULL_MASK, ok)) break;
+        bool isnew = false;
+        int slot = -1;
+        if (ok) slot = table_add_packed(t, c[k], __double2int_rn(wt[k]), isnew, p.err);
+        occ_append(t, isnew, slot);
+        __syncwarp();
+      }
+      continue;
+    }
 #pragma unroll
     for (int k = 0; k < kUnroll; ++k) {
       const bool ok = u[k] >= 0;
@@ -390,8 +448,14 @@ __device__ __forceinline__ void scan_entries(const MoveArgs& p, double m, const 
       cc[k] = -1;
       if (ii < n) {
         const int slot = t.occ ? t.occ[ii] : ii;
-        cc[k] = cg ? __ldcg(&t.keys[slot]) : t.keys[slot];
-        val[k] = cg ? __ldcg(&t.vals[slot]) : table_val(t, slot);
+        if (t.slots) {
+          const unsigned long long x = t.slots[slot];
+          cc[k] = slot_key(x);
+          val[k] = (double)slot_sum(x);
+        } else {
+          cc[k] = cg ? __ldcg(&t.keys[slot]) : t.keys[slot];
+          val[k] = cg ? __ldcg(&t.vals[slot]) : table_val(t, slot);
+        }
       }
     }
 #pragma unroll
@@ -418,13 +482,14 @@ __device__ __forceinline__ void nido_tie_entries(const MoveArgs& p, double m, co
   g = -NIDO_MAX_FLOAT; tk = kNoKey; cand = -1;
   for (int i = t0; i < n; i += step) {
     const int slot = t.occ ? t.occ[i] : i;
-    const int cc = cg ? __ldcg(&t.keys[slot]) : t.keys[slot];
+    const int cc = cg ? __ldcg(&t.keys[slot]) : table_key(t, slot);
     if (cc < 0 || cc == own) continue;
     const double val = cg ? __ldcg(&t.vals[slot]) : table_val(t, slot);
     if (gain_of(val, ki, p.a[cc], m) != gm) continue;
     unsigned rank = 0;
     for (int q = 0; q < n; ++q) {
-      const int kq = cg ? __ldcg(&t.keys[t.occ ? t.occ[q] : q]) : t.keys[t.occ ? t.occ[q] : q];
+      const int sq = t.occ ? t.occ[q] : q;
+      const int kq = cg ? __ldcg(&t.keys[sq]) : table_key(t, sq);
       rank += (kq >= 0 && kq < cc) ? 1u : 0u;
     }
     const unsigned long long key = nido_key(rank);
@@ -440,18 +505,31 @@ __device__ __forceinline__ void decide(const MoveArgs& p, double m, int v, int o
 }
 
 // ---- 32 < degree <= 256: one warp per vertex, table in shared memory -----------
+// Shared memory of the tables: FP64 tables hold 8-byte values, 4-byte keys
+// and a 4-byte occupied list (16 bytes a slot); packed integer tables 8-byte
+// slots and the occupied list (12 bytes a slot).
+constexpr size_t table_bytes(int slots, bool ints) { return (size_t)slots * (ints ? 12 : 16); }
+
 template <int kCap, bool kMulti, bool kInts>
 __global__ void __launch_bounds__(256) k_move_warp(const int32_t* __restrict__ list, int64_t n, MoveArgs p) {
   extern __shared__ double smem[];
   __shared__ int nocc_s[8];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
   Table t;
-  t.vals = smem + (size_t)wid * kCap;
-  t.keys = reinterpret_cast<int*>(smem + 8 * kCap) + (size_t)wid * 2 * kCap;
-  t.occ = t.keys + kCap;
+  if constexpr (kInts) {
+    t.slots = reinterpret_cast<unsigned long long*>(smem) + (size_t)wid * kCap;
+    t.keys = nullptr;
+    t.vals = nullptr;
+    t.occ = reinterpret_cast<int*>(smem + 8 * kCap) + (size_t)wid * kCap;
+    for (int i = lane; i < kCap; i += 32) t.slots[i] = kEmptySlot;
+  } else {
+    t.vals = smem + (size_t)wid * kCap;
+    t.keys = reinterpret_cast<int*>(smem + 8 * kCap) + (size_t)wid * 2 * kCap;
+    t.occ = t.keys + kCap;
+    for (int i = lane; i < kCap; i += 32) { t.keys[i] = -1; t.vals[i] = 0.; }
+  }
   t.nocc = &nocc_s[wid];
   t.ints = kInts;
-  for (int i = lane; i < kCap; i += 32) { t.keys[i] = -1; t.vals[i] = 0.; }
   if (lane == 0) *t.nocc = 0;
   __syncwarp();
   const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -479,8 +557,12 @@ __global__ void __launch_bounds__(256) k_move_warp(const int32_t* __restrict__ l
     __syncwarp();
     for (int i = lane; i < nu; i += 32) {
       const int slot = t.occ[i];
-      t.keys[slot] = -1;
-      t.vals[slot] = 0.;
+      if constexpr (kInts) {
+        t.slots[slot] = kEmptySlot;
+      } else {
+        t.keys[slot] = -1;
+        t.vals[slot] = 0.;
+      }
     }
     if (lane == 0) *t.nocc = 0;
     __syncwarp();
@@ -563,21 +645,31 @@ __device__ __forceinline__ void block_evaluate(const MoveArgs& p, double m, cons
 // ---- 256 < degree <= 2048: one CTA per vertex, table in shared memory ----------
 // kOcc: keep a list of occupied slots (16 bytes a slot) so evaluation and
 // clearing touch only used slots; without it (12 bytes a slot, for the
-// largest table) both walk the vertex's whole table.
+// largest FP64 table) both walk the vertex's whole table.  Packed integer
+// tables (kInts) always keep the list: 12 bytes a slot with it.
 template <int kThreads, int kCap, bool kMulti, bool kInts, bool kOcc = true>
 __global__ void __launch_bounds__(kThreads) k_move_cta(const int32_t* __restrict__ list, int64_t n, MoveArgs p) {
+  constexpr bool kList = kOcc || kInts;
   extern __shared__ double smem[];
   __shared__ double sg[32];
   __shared__ unsigned long long stk[32];
   __shared__ int sc[32];
   __shared__ int nocc_s;
   Table t;
-  t.vals = smem;
-  t.keys = reinterpret_cast<int*>(smem + kCap);
-  t.occ = kOcc ? t.keys + kCap : nullptr;
+  if constexpr (kInts) {
+    t.slots = reinterpret_cast<unsigned long long*>(smem);
+    t.keys = nullptr;
+    t.vals = nullptr;
+    t.occ = reinterpret_cast<int*>(smem + kCap);
+    for (int i = threadIdx.x; i < kCap; i += kThreads) t.slots[i] = kEmptySlot;
+  } else {
+    t.vals = smem;
+    t.keys = reinterpret_cast<int*>(smem + kCap);
+    t.occ = kOcc ? t.keys + kCap : nullptr;
+    for (int i = threadIdx.x; i < kCap; i += kThreads) { t.keys[i] = -1; t.vals[i] = 0.; }
+  }
   t.nocc = &nocc_s;
   t.ints = kInts;
-  for (int i = threadIdx.x; i < kCap; i += kThreads) { t.keys[i] = -1; t.vals[i] = 0.; }
   if (threadIdx.x == 0) nocc_s = 0;
   __syncthreads();
   const int wid = threadIdx.x >> 5;
@@ -601,7 +693,7 @@ __global__ void __launch_bounds__(kThreads) k_move_cta(const int32_t* __restrict
     t.mask = min((unsigned)kCap, next_pow2_cap(eend - s)) - 1;
     accumulate_edges<true, 4>(p, v, s + (int64_t)wid * 32, eend, kThreads, t);
     __syncthreads();
-    const int nu = kOcc ? nocc_s : (int)(t.mask + 1);
+    const int nu = kList ? nocc_s : (int)(t.mask + 1);
     int64_t sn = 0, en = 0;
     int ownn = 0;
     double kin = 0.;
@@ -617,9 +709,13 @@ __global__ void __launch_bounds__(kThreads) k_move_cta(const int32_t* __restrict
     if (threadIdx.x == 0) nocc_s = 0;
     const double aownn = nt < n ? p.a[ownn] : 0.;
     for (int i = threadIdx.x; i < nu; i += kThreads) {
-      const int slot = kOcc ? t.occ[i] : i;
-      t.keys[slot] = -1;
-      t.vals[slot] = 0.;
+      const int slot = kList ? t.occ[i] : i;
+      if constexpr (kInts) {
+        t.slots[slot] = kEmptySlot;
+      } else {
+        t.keys[slot] = -1;
+        t.vals[slot] = 0.;
+      }
     }
     __syncthreads();
     v = vn;
@@ -1169,10 +1265,10 @@ int64_t resident(K kernel, int threads, size_t smem, int sms) {
 
 template <bool kMulti, bool kInts>
 int set_smem_mode() {
-  NIDO_TRY(set_smem(k_move_warp<kWarpCap, kMulti, kInts>, (size_t)8 * kWarpCap * 16));
-  NIDO_TRY(set_smem(k_move_cta<kCtaSThreads, kCtaSCap, kMulti, kInts>, (size_t)kCtaSCap * 16));
-  NIDO_TRY(set_smem(k_move_cta<kCtaMThreads, kCtaMCap, kMulti, kInts>, (size_t)kCtaMCap * 16));
-  NIDO_TRY(set_smem(k_move_cta<kCtaLThreads, kCtaLCap, kMulti, kInts>, (size_t)kCtaLCap * 16));
+  NIDO_TRY(set_smem(k_move_warp<kWarpCap, kMulti, kInts>, 8 * table_bytes(kWarpCap, kInts)));
+  NIDO_TRY(set_smem(k_move_cta<kCtaSThreads, kCtaSCap, kMulti, kInts>, table_bytes(kCtaSCap, kInts)));
+  NIDO_TRY(set_smem(k_move_cta<kCtaMThreads, kCtaMCap, kMulti, kInts>, table_bytes(kCtaMCap, kInts)));
+  NIDO_TRY(set_smem(k_move_cta<kCtaLThreads, kCtaLCap, kMulti, kInts>, table_bytes(kCtaLCap, kInts)));
   NIDO_TRY(set_smem(k_move_cta<1024, kCtaXCap, kMulti, kInts, false>, (size_t)kCtaXCap * 12));
   int dev = 0, sms = kSMs;
   NIDO_CUDA_TRY(cudaGetDevice(&dev));
@@ -1184,10 +1280,10 @@ int set_smem_mode() {
   R.g8 = resident(k_move_group<8, kMulti>, 256, 0, sms);
   R.g16 = resident(k_move_group<16, kMulti>, 256, 0, sms);
   R.g32 = resident(k_move_group<32, kMulti>, 256, 0, sms);
-  R.warp = resident(k_move_warp<kWarpCap, kMulti, kInts>, 256, (size_t)8 * kWarpCap * 16, sms);
-  R.ctas = resident(k_move_cta<kCtaSThreads, kCtaSCap, kMulti, kInts>, kCtaSThreads, (size_t)kCtaSCap * 16, sms);
-  R.ctam = resident(k_move_cta<kCtaMThreads, kCtaMCap, kMulti, kInts>, kCtaMThreads, (size_t)kCtaMCap * 16, sms);
-  R.ctal = resident(k_move_cta<kCtaLThreads, kCtaLCap, kMulti, kInts>, kCtaLThreads, (size_t)kCtaLCap * 16, sms);
+  R.warp = resident(k_move_warp<kWarpCap, kMulti, kInts>, 256, 8 * table_bytes(kWarpCap, kInts), sms);
+  R.ctas = resident(k_move_cta<kCtaSThreads, kCtaSCap, kMulti, kInts>, kCtaSThreads, table_bytes(kCtaSCap, kInts), sms);
+  R.ctam = resident(k_move_cta<kCtaMThreads, kCtaMCap, kMulti, kInts>, kCtaMThreads, table_bytes(kCtaMCap, kInts), sms);
+  R.ctal = resident(k_move_cta<kCtaLThreads, kCtaLCap, kMulti, kInts>, kCtaLThreads, table_bytes(kCtaLCap, kInts), sms);
   R.ctax = resident(k_move_cta<1024, kCtaXCap, kMulti, kInts, false>, 1024, (size_t)kCtaXCap * 12, sms);
   R.hubmv = resident(k_move_hub<kMulti>, kHubThreads, 0, sms);
   R.hubins = resident(k_hub_insert, kHubThreads, 0, sms);
@@ -1303,17 +1399,17 @@ int launch_tiers(nido_graph_s* g, int batch, int tie, const MoveArgs& p) {
         k_move_group<32, kMulti><<<grid_cap((n + 7) / 8, R.g32), 256, 0, s>>>(list, n, p);
         break;
       case kTierWarp:
-        k_move_warp<kWarpCap, kMulti, kInts><<<grid_cap((n + 7) / 8, R.warp), 256, (size_t)8 * kWarpCap * 16, s>>>(
+        k_move_warp<kWarpCap, kMulti, kInts><<<grid_cap((n + 7) / 8, R.warp), 256, 8 * table_bytes(kWarpCap, kInts), s>>>(
             list, n, p);
         break;
       case kTierCtaS:
-        k_move_cta<kCtaSThreads, kCtaSCap, kMulti, kInts><<<grid_cap(n, R.ctas), kCtaSThreads, (size_t)kCtaSCap * 16, s>>>(list, n, p);
+        k_move_cta<kCtaSThreads, kCtaSCap, kMulti, kInts><<<grid_cap(n, R.ctas), kCtaSThreads, table_bytes(kCtaSCap, kInts), s>>>(list, n, p);
         break;
       case kTierCtaM:
-        k_move_cta<kCtaMThreads, kCtaMCap, kMulti, kInts><<<grid_cap(n, R.ctam), kCtaMThreads, (size_t)kCtaMCap * 16, s>>>(list, n, p);
+        k_move_cta<kCtaMThreads, kCtaMCap, kMulti, kInts><<<grid_cap(n, R.ctam), kCtaMThreads, table_bytes(kCtaMCap, kInts), s>>>(list, n, p);
         break;
       case kTierCtaL:
-        k_move_cta<kCtaLThreads, kCtaLCap, kMulti, kInts><<<grid_cap(n, R.ctal), kCtaLThreads, (size_t)kCtaLCap * 16, s>>>(list, n, p);
+        k_move_cta<kCtaLThreads, kCtaLCap, kMulti, kInts><<<grid_cap(n, R.ctal), kCtaLThreads, table_bytes(kCtaLCap, kInts), s>>>(list, n, p);
         break;
       case kTierCtaX:
         k_move_cta<1024, kCtaXCap, kMulti, kInts, false><<<grid_cap(n, R.ctax), 1024, (size_t)kCtaXCap * 12, s>>>(list, n, p);

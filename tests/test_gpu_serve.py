@@ -90,8 +90,12 @@ def test_admission_respects_budget(nido_lib):
         th.join()
         assert all(r <= budget for _, r, _, _ in seen)
         assert all(i.status == 0 and i.hbm_bytes == f for i, f in zip(infos, fps))
+        # a request whose HBM footprint exceeds the budget even with its edges
+        # in host memory is refused (one that fits that way is admitted:
+        # test_gpu_overbudget.py)
+        big = nido_lib.gen_rmat(1 << 22, 1 << 22, wmode=nido_lib.W_ONE, seed=3)
+        assert nido_lib.graph_footprint_streamed(big.nv, big.ne, 2) > budget
         with pytest.raises(nido_lib.NidoError) as e:
-            big = nido_lib.gen_rmat(1 << 20, 16 << 20, wmode=nido_lib.W_ONE, seed=3)
             srv.submit(big)
         assert e.value.code == -5  # NIDO_E_TOO_LARGE
 
