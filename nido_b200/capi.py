@@ -432,19 +432,27 @@ class Graph:
 
     def run(self, tau: float = 1e-6, max_iter: int = 500, tie: int = NIDO_TIE_SMALLEST_ID,
             verbose: bool = False, tune: bool = False, host_loop: bool = False, tau_phase: float | None = None,
-            color_batches: bool = False):
+            color_batches: bool = False, device_loop: bool = False):
         """LouvainGPU::run; returns (clustering of the input vertices, RunStats).
-        host_loop: drive each phase's iterations from the host (one readback per
-        iteration) instead of the device-resident loop.  color_batches: every
+        host_loop / device_loop: force who drives each phase's iterations (the
+        host, one readback per iteration, or the device-resident loop graph);
+        neither: the library picks by the phase's size.  color_batches: every
         phase's colour classes are its batches (conflict-free) instead of the
         -b cuts."""
         p = _Params(self.nbatches, tie, tau, max_iter, int(verbose), int(tune),
-                    0.0 if tau_phase is None else tau_phase, int(tau_phase is not None), int(host_loop),
-                    int(color_batches))
+                    0.0 if tau_phase is None else tau_phase, int(tau_phase is not None),
+                    _loop_mode(host_loop, device_loop), int(color_batches))
         out = np.empty(self.nv0, np.int64)
         st = RunStats()
         _check(lib().nido_run(self.h, C.byref(p), _p64(out), C.byref(st)))
         return out, st
+
+
+def _loop_mode(host_loop: bool, device_loop: bool) -> int:
+    """nido_params.host_loop: 1 host, 2 device, 0 chosen by the library."""
+    if host_loop and device_loop:
+        raise ValueError("host_loop and device_loop are exclusive")
+    return 1 if host_loop else (2 if device_loop else 0)
 
 
 def pack_graphs(graphs: list[Csr]):
@@ -498,10 +506,10 @@ class Batch:
         self.close()
 
     def run(self, tau: float = 1e-6, max_iter: int = 500, tie: int = NIDO_TIE_SMALLEST_ID,
-            tune: bool = False, host_loop: bool = False):
+            tune: bool = False, host_loop: bool = False, device_loop: bool = False):
         """Returns (per-graph clusterings, final Q per graph, phases per graph,
         loops per graph, RunStats)."""
-        p = _Params(self.nbatches, tie, tau, max_iter, 0, int(tune), 0.0, 0, int(host_loop))
+        p = _Params(self.nbatches, tie, tau, max_iter, 0, int(tune), 0.0, 0, _loop_mode(host_loop, device_loop))
         out = np.empty(self.nv, np.int64)
         q = np.empty(self.ngraphs, np.float64)
         ph = np.empty(self.ngraphs, np.int64)

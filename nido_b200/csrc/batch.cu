@@ -629,6 +629,8 @@ extern "C" int nido_batch_run(nido_batch B, const nido_params* p, int64_t* out_c
     return nido_set_error(NIDO_E_INVALID, "params.nbatches (%d) differs from the batch's (%d)", p->nbatches, g->nbatches);
   if (p->color_batches)
     return nido_set_error(NIDO_E_INVALID, "colour-class batches are for one-graph runs (nido_run)");
+  if (p->host_loop < 0 || p->host_loop > 2)
+    return nido_set_error(NIDO_E_INVALID, "host_loop must be 0, 1 or 2 (got %d)", p->host_loop);
   if (p->tie_mode != NIDO_TIE_SMALLEST_ID && p->tie_mode != NIDO_TIE_NIDO)
     return nido_set_error(NIDO_E_INVALID, "unknown tie mode %d", p->tie_mode);
   NIDO_CUDA_TRY(cudaSetDevice(g->ctx->device));
@@ -836,7 +838,9 @@ extern "C" int nido_batch_run(nido_batch B, const nido_params* p, int64_t* out_c
     };
     while (n_iter > 0) {
       bool ran_on_device = false;
-      if (!p->host_loop && g->ctx->device_loop) {
+      const bool want_device =
+          p->host_loop == 2 || (p->host_loop == 0 && listed_e <= NIDO_DEVICE_LOOP_MAX_EDGES);
+      if (want_device && g->ctx->device_loop) {
         bool unsupported = false;
         NIDO_TRY(device_sweeps(&unsupported));
         if (unsupported) g->ctx->device_loop = false;

@@ -946,6 +946,8 @@ extern "C" int nido_run(nido_graph g, const nido_params* p, int64_t* out_comm, n
   if (!g || !p) return nido_set_error(NIDO_E_INVALID, "null argument");
   if (p->nbatches != g->nb_user)
     return nido_set_error(NIDO_E_INVALID, "params.nbatches (%d) differs from the graph's (%d)", p->nbatches, g->nb_user);
+  if (p->host_loop < 0 || p->host_loop > 2)
+    return nido_set_error(NIDO_E_INVALID, "host_loop must be 0, 1 or 2 (got %d)", p->host_loop);
   if (p->color_batches != 0 && p->color_batches != 1)
     return nido_set_error(NIDO_E_INVALID, "color_batches must be 0 or 1 (got %d)", p->color_batches);
   if ((p->color_batches != 0) != g->color_mode) {
@@ -1006,7 +1008,8 @@ extern "C" int nido_run(nido_graph g, const nido_params* p, int64_t* out_comm, n
     NIDO_TRY(nido::launch_singleton(g));
     double Q = 0., Q_old = 0.;
     int64_t loops = 0;
-    bool host_loop = p->host_loop != 0 || !g->ctx->device_loop || (p->verbose && p->max_iter > nido::kLoopLogCap);
+    const bool want_device = p->host_loop == 2 || (p->host_loop == 0 && g->ne <= NIDO_DEVICE_LOOP_MAX_EDGES);
+    bool host_loop = !want_device || !g->ctx->device_loop || (p->verbose && p->max_iter > nido::kLoopLogCap);
     if (!host_loop) {
       // the phase's iteration loop as one device-resident CUDA graph
       nido::PhaseLoop r;

@@ -36,7 +36,7 @@ def bits(x):
 def test_device_loop_equals_host_loop(nido_lib, ctx, gs, gname, nb, tie):
     G = gs[gname]
     with nido_lib.Graph(ctx, G, nb) as g:
-        cd, sd = g.run(tie=tie)
+        cd, sd = g.run(tie=tie, device_loop=True)
         ch, sh = g.run(tie=tie, host_loop=True)
     assert np.array_equal(cd, ch)
     assert sd.phases == sh.phases and sd.total_loops == sh.total_loops
@@ -55,7 +55,7 @@ def test_device_loop_limits(nido_lib, ctx, gs, max_iter, tau):
     negative tau keeps iterating until the cap, undo steps included)."""
     G = gs["rmat_s14_int"]
     with nido_lib.Graph(ctx, G, 2) as g:
-        cd, sd = g.run(tau=tau, max_iter=max_iter)
+        cd, sd = g.run(tau=tau, max_iter=max_iter, device_loop=True)
         ch, sh = g.run(tau=tau, max_iter=max_iter, host_loop=True)
     assert np.array_equal(cd, ch)
     assert sd.phases == sh.phases and sd.total_loops == sh.total_loops
@@ -66,7 +66,7 @@ def test_device_loop_limits(nido_lib, ctx, gs, max_iter, tau):
 def test_device_loop_lognormal_within_tolerance(nido_lib, ctx, orc):
     G = nido_lib.gen_sbm(30000, cmin=16, cmax=2048, avg_degree=20.0, wmode=nido_lib.W_LOGNORMAL, seed=34)
     with nido_lib.Graph(ctx, G, 2) as g:
-        cd, sd = g.run()
+        cd, sd = g.run(device_loop=True)
         ch, sh = g.run(host_loop=True)
     assert abs(sd.final_q - sh.final_q) <= 1e-3
     assert orc.nmi(cd, ch) >= 0.95
@@ -76,7 +76,7 @@ def test_device_loop_prints_the_reference_lines(nido_lib, ctx, gs, capfd):
     G = gs["planted_int"]
     with nido_lib.Graph(ctx, G, 2) as g:
         capfd.readouterr()
-        g.run(verbose=True)
+        g.run(verbose=True, device_loop=True)
         dev = capfd.readouterr().out
         g.run(verbose=True, host_loop=True)
         host = capfd.readouterr().out
@@ -92,7 +92,7 @@ def test_batched_device_loop_equals_host_loop(nido_lib, ctx, gs, nb, tie):
         nido_lib.gen_rmat(1 << int(s), int(d) << int(s), wmode=nido_lib.W_INT8, seed=400 + i)
         for i, (s, d) in enumerate(zip(rng.integers(6, 12, 12), rng.integers(4, 20, 12)))]
     with nido_lib.Batch(ctx, many, nb) as b:
-        pd, qd, phd, lod, sd = b.run(tie=tie)
+        pd, qd, phd, lod, sd = b.run(tie=tie, device_loop=True)
         ph_, qh, phh, loh, sh = b.run(tie=tie, host_loop=True)
     for x, y in zip(pd, ph_):
         assert np.array_equal(x, y)
@@ -101,3 +101,22 @@ def test_batched_device_loop_equals_host_loop(nido_lib, ctx, gs, nb, tie):
     assert sd.total_loops == sh.total_loops and sd.move_bytes == sh.move_bytes
     # far fewer host round trips: the device loop launches its sweeps as graphs
     assert sd.move_ms > 0
+
+
+def test_default_picks_the_loop_by_phase_size(nido_lib, ctx, gs):
+    """With neither option the device drives phases of at most
+    NIDO_DEVICE_LOOP_MAX_EDGES (16 Mi) edges and the host the larger ones;
+    the loop graphs' build time shows which ran.  Results do not depend on it."""
+    small = gs["rmat_s14_int"]
+    with nido_lib.Graph(ctx, small, 2) as g:
+        cl, st = g.run()
+        assert st.host_ms[7] > 0  # loop graphs were built
+        ch, sh = g.run(host_loop=True)
+        assert sh.host_ms[7] == 0 and np.array_equal(cl, ch)
+    big = nido_lib.gen_rmat(1 << 20, 16 << 20, wmode=nido_lib.W_INT8, seed=36)
+    assert big.ne > (16 << 20)
+    with nido_lib.Graph(ctx, big, 2) as g:
+        cl, st = g.run()
+        assert st.ne_phase[0] == big.ne and st.phases >= 2
+        cd, sd = g.run(device_loop=True)
+    assert np.array_equal(cl, cd) and st.final_q == sd.final_q
