@@ -220,7 +220,9 @@ typedef struct {
   int32_t cta_s_max_degree;  /* 128-thread CTA, 1024 slots; <= 768 */
   int32_t cta_m_max_degree;  /* 256-thread CTA, 2048 slots; <= 1536 */
   int32_t cta_l_max_degree;  /* 256-thread CTA, 4096 slots; <= 3072 (default 2048) */
-  int32_t cta_x_max_degree;  /* 1024-thread CTA, 16384 slots; <= 12288; above: hub tier */
+  int32_t cta_x_max_degree;  /* <= 12288; above: hub tier.  Degrees up to 6144 of this
+                                range run on 512-thread CTAs with 8192 slots (two an
+                                SM), the rest on 1024-thread CTAs with 16384 slots */
   int32_t hub_clusters;      /* 1: in integer-weight phases with the smallest-id rule,
                                 hubs run on thread-block clusters of 2..16 CTAs whose
                                 distributed shared memory holds the hub's table (when

@@ -30,6 +30,7 @@ enum Tier {
   kTierCtaS,    // d <= 768  : one 128-thread CTA, shared-memory hash (1024 slots)
   kTierCtaM,    // d <= 1536 : one 256-thread CTA, shared-memory hash (2048 slots)
   kTierCtaL,    // d <= 3072 : one 256-thread CTA, shared-memory hash (4096 slots)
+  kTierCtaXA,   // d <= 6144 : one 512-thread CTA, shared-memory hash (8192 slots, 96 KB: two CTAs an SM)
   kTierCtaX,    // d <= 12288: one 1024-thread CTA, shared-memory hash (16384 slots, 192 KB, load <= 3/4)
   kTierHub,     // larger    : 2048-edge segments on many CTAs, hash in global memory (L2)
   kNumTiers
@@ -41,6 +42,7 @@ constexpr int kWarpMaxDeg = 192;
 constexpr int kCtaSMaxDeg = 768;
 constexpr int kCtaMMaxDeg = 1536;
 constexpr int kCtaLMaxDeg = 3072;
+constexpr int kCtaXAMaxDeg = 6144;  // table load up to 3/4 in the 8192 slots
 constexpr int kCtaXMaxDeg = 12288;  // table load up to 3/4 in the 16384 slots
 constexpr int kHubSeg = 2048;        // edges of one hub segment (move and modularity)
 

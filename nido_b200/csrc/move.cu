@@ -1234,7 +1234,9 @@ constexpr int kCtaLThreads = 256;
 constexpr int kCtaSCap = 1024;
 constexpr int kCtaMCap = 2048;
 constexpr int kCtaLCap = 4096;
-constexpr int kCtaXCap = 16384;   // 1024-thread CTA-XL tier (no occupied list)
+constexpr int kCtaXAThreads = 512;
+constexpr int kCtaXACap = 8192;   // 512-thread CTA-XA tier, two CTAs an SM (occupied list in integer phases)
+constexpr int kCtaXCap = 16384;   // 1024-thread CTA-XL tier (occupied list in integer phases)
 
 template <typename K>
 int set_smem(K kernel, size_t bytes) {
@@ -1249,7 +1251,7 @@ namespace {
 // more would leave a partial wave at the end.
 struct Resident {
   int64_t g4 = kSMs, g8 = kSMs, g16 = kSMs, g32 = kSMs, warp = kSMs, ctas = kSMs, ctam = kSMs, ctal = kSMs,
-          ctax = kSMs, hubmv = kSMs, hubins = kSMs, hubsl = kSMs;
+          ctaxa = kSMs, ctax = kSMs, hubmv = kSMs, hubins = kSMs, hubsl = kSMs;
 };
 Resident g_resident[2][2];  // [many graphs][integer tables]
 
@@ -1269,6 +1271,7 @@ int set_smem_mode() {
   NIDO_TRY(set_smem(k_move_cta<kCtaSThreads, kCtaSCap, kMulti, kInts>, table_bytes(kCtaSCap, kInts)));
   NIDO_TRY(set_smem(k_move_cta<kCtaMThreads, kCtaMCap, kMulti, kInts>, table_bytes(kCtaMCap, kInts)));
   NIDO_TRY(set_smem(k_move_cta<kCtaLThreads, kCtaLCap, kMulti, kInts>, table_bytes(kCtaLCap, kInts)));
+  NIDO_TRY(set_smem(k_move_cta<kCtaXAThreads, kCtaXACap, kMulti, kInts, false>, (size_t)kCtaXACap * 12));
   NIDO_TRY(set_smem(k_move_cta<1024, kCtaXCap, kMulti, kInts, false>, (size_t)kCtaXCap * 12));
   int dev = 0, sms = kSMs;
   NIDO_CUDA_TRY(cudaGetDevice(&dev));
@@ -1284,6 +1287,8 @@ int set_smem_mode() {
   R.ctas = resident(k_move_cta<kCtaSThreads, kCtaSCap, kMulti, kInts>, kCtaSThreads, table_bytes(kCtaSCap, kInts), sms);
   R.ctam = resident(k_move_cta<kCtaMThreads, kCtaMCap, kMulti, kInts>, kCtaMThreads, table_bytes(kCtaMCap, kInts), sms);
   R.ctal = resident(k_move_cta<kCtaLThreads, kCtaLCap, kMulti, kInts>, kCtaLThreads, table_bytes(kCtaLCap, kInts), sms);
+  R.ctaxa = resident(k_move_cta<kCtaXAThreads, kCtaXACap, kMulti, kInts, false>, kCtaXAThreads,
+                     (size_t)kCtaXACap * 12, sms);
   R.ctax = resident(k_move_cta<1024, kCtaXCap, kMulti, kInts, false>, 1024, (size_t)kCtaXCap * 12, sms);
   R.hubmv = resident(k_move_hub<kMulti>, kHubThreads, 0, sms);
   R.hubins = resident(k_hub_insert, kHubThreads, 0, sms);
@@ -1410,6 +1415,10 @@ int launch_tiers(nido_graph_s* g, int batch, int tie, const MoveArgs& p) {
         break;
       case kTierCtaL:
         k_move_cta<kCtaLThreads, kCtaLCap, kMulti, kInts><<<grid_cap(n, R.ctal), kCtaLThreads, table_bytes(kCtaLCap, kInts), s>>>(list, n, p);
+        break;
+      case kTierCtaXA:
+        k_move_cta<kCtaXAThreads, kCtaXACap, kMulti, kInts, false>
+            <<<grid_cap(n, R.ctaxa), kCtaXAThreads, (size_t)kCtaXACap * 12, s>>>(list, n, p);
         break;
       case kTierCtaX:
         k_move_cta<1024, kCtaXCap, kMulti, kInts, false><<<grid_cap(n, R.ctax), 1024, (size_t)kCtaXCap * 12, s>>>(list, n, p);

@@ -389,6 +389,7 @@ __device__ __forceinline__ int tier_of(int64_t d, const TierThresholds& thr) {
   if (d <= thr.ctas) return kTierCtaS;
   if (d <= thr.ctam) return kTierCtaM;
   if (d <= thr.ctal) return kTierCtaL;
+  if (d <= thr.ctax && d <= kCtaXAMaxDeg) return kTierCtaXA;  // two 512-thread CTAs an SM
   if (d <= thr.ctax) return kTierCtaX;
   return kTierHub;
 }
