@@ -458,6 +458,10 @@ def run_many(args, world, rank, local):
         "clocks": clocks,
         "gpu_launches": launches,
         "kernel_launches_per_step": launches / args.steps,
+        "breakdown_ms_per_step": {"move": move_ms / len(runs), "modularity": sum(r[4].q_ms for r in runs) / len(runs),
+                                  "aggregation": sum(r[4].agg_ms for r in runs) / len(runs),
+                                  "other": ms_max / args.steps - (move_ms + sum(r[4].q_ms + r[4].agg_ms
+                                                                               for r in runs)) / len(runs)},
         "loop_graph_build_ms_per_step": sum(r[4].host_ms[7] for r in runs) / len(runs),
         "latency_ms": serving["latency_ms"] if serving else None,
         "serving": ({k: serving[k] for k in ("graphs_per_s", "requests", "latency_ms", "overlap", "workload")}

@@ -639,14 +639,16 @@ extern "C" int nido_batch_run(nido_batch B, const nido_params* p, int64_t* out_c
   memset(&st, 0, sizeof(st));
   const uint64_t launches0 = nido_launch_count();
   struct RunEvents {  // destroyed on every return, early ones included
-    cudaEvent_t t0 = nullptr, t1 = nullptr;
+    cudaEvent_t t0 = nullptr, t1 = nullptr, a0 = nullptr, a1 = nullptr;
     ~RunEvents() {
-      if (t0) cudaEventDestroy(t0);
-      if (t1) cudaEventDestroy(t1);
+      for (cudaEvent_t e : {t0, t1, a0, a1})
+        if (e) cudaEventDestroy(e);
     }
   } re;
   NIDO_CUDA_TRY(cudaEventCreate(&re.t0));
   NIDO_CUDA_TRY(cudaEventCreate(&re.t1));
+  NIDO_CUDA_TRY(cudaEventCreate(&re.a0));
+  NIDO_CUDA_TRY(cudaEventCreate(&re.a1));
   cudaEvent_t t0 = re.t0, t1 = re.t1;
   std::vector<cudaEvent_t>& ev = g->ctx->move_ev;
   while (ev.size() < 2) {
@@ -910,7 +912,9 @@ extern "C" int nido_batch_run(nido_batch B, const nido_params* p, int64_t* out_c
     k_drop<<<grid_for(g->nv, kThreads), kThreads, 0, s>>>(g->nv, B->gid, B->gagg, g->comm);
     NIDO_LAUNCH_CHECK();
     int done = 0;
+    NIDO_CUDA_TRY(cudaEventRecord(re.a0, s));
     NIDO_TRY(launch_aggregation(g, &done));
+    NIDO_CUDA_TRY(cudaEventRecord(re.a1, s));
     std::swap(g->gbase, g->gbase2);  // the clustering is in the new numbering either way
     k_post_agg<<<grid_for(np, 128), 128, 0, s>>>(B->plist, np, g->gbase2, g->gbase, B->gagg, B->gfin);
     NIDO_LAUNCH_CHECK();
@@ -918,6 +922,11 @@ extern "C" int nido_batch_run(nido_batch B, const nido_params* p, int64_t* out_c
     // finished too (their vertices leave the union at the next coarsening)
     NIDO_CUDA_TRY(cudaMemcpyAsync(flags.data(), B->gfin, sizeof(int32_t) * ng, cudaMemcpyDeviceToHost, s));
     NIDO_CUDA_TRY(cudaStreamSynchronize(s));
+    {
+      float ams = 0.f;
+      NIDO_CUDA_TRY(cudaEventElapsedTime(&ams, re.a0, re.a1));
+      st.agg_ms += ams;
+    }
     {
       std::vector<int32_t> em;
       for (int32_t i = 0; i < ng; ++i)
