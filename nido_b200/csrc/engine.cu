@@ -297,8 +297,8 @@ extern "C" int nido_graph_free(nido_graph g) {
     for (void* p : {(void*)g->adj0, (void*)g->adjA, (void*)g->adj2, (void*)g->w0, (void*)g->wA, (void*)g->w2})
       if (p) cudaFreeHost(p);
   } else {
-    dev_free(ctx, g->adj0, 4 * E); dev_free(ctx, g->adjA, 4 * E); dev_free(ctx, g->adj2, 4 * E);
-    dev_free(ctx, g->w0, 8 * E); dev_free(ctx, g->wA, 8 * E); dev_free(ctx, g->w2, 8 * E);
+    dev_free(ctx, g->adj0, 4 * (E + 4)); dev_free(ctx, g->adjA, 4 * (E + 4)); dev_free(ctx, g->adj2, 4 * (E + 4));
+    dev_free(ctx, g->w0, 8 * (E + 4)); dev_free(ctx, g->wA, 8 * (E + 4)); dev_free(ctx, g->w2, 8 * (E + 4));
   }
   dev_free(ctx, g->k, 8 * V); dev_free(ctx, g->a, 8 * V);
   dev_free(ctx, g->comm, 4 * V); dev_free(ctx, g->newc, 4 * V);
@@ -349,8 +349,10 @@ int graph_create(nido_ctx ctx, int64_t nv, int64_t ne, int32_t nbatches, nido_gr
 #define ALLOC(p, n) if (st == NIDO_OK) st = dev_alloc(ctx, &g->p, (n))
 #define EALLOC(p, n) if (st == NIDO_OK) st = g->host_edges ? host_alloc(&g->p, (n)) : dev_alloc(ctx, &g->p, (n))
   ALLOC(off0, V + 1); ALLOC(offA, V + 1); ALLOC(off2, V + 1);
-  EALLOC(adj0, E); EALLOC(adjA, E); EALLOC(adj2, E);
-  EALLOC(w0, E); EALLOC(wA, E); EALLOC(w2, E);
+  // 4 spare entries: the move kernels' bulk copies widen an edge range to
+  // 16-byte boundaries and may read up to 3 ids and 1 weight past its end
+  EALLOC(adj0, E + 4); EALLOC(adjA, E + 4); EALLOC(adj2, E + 4);
+  EALLOC(w0, E + 4); EALLOC(wA, E + 4); EALLOC(w2, E + 4);
 #undef EALLOC
   ALLOC(k, V); ALLOC(a, V);
   ALLOC(comm, V); ALLOC(newc, V);

@@ -323,9 +323,12 @@ __device__ __forceinline__ unsigned next_pow2_cap(int64_t d) {
 // then the communities) before any is merged, so each warp keeps several
 // dependent gathers in flight.  Chunks are merged in order.  Every lane of the
 // warp takes part.
+// The edges come from global memory, or (sadj non-null) from a copy of the
+// vertex's ranges in shared memory: edge j at sadj[j - a0] and sw[j - w0].
 template <bool kAtomicVals, int kUnroll, bool kGlobal = false>
 __device__ __forceinline__ void accumulate_edges(const MoveArgs& p, int v, int64_t first, int64_t eend,
-                                                 int64_t stride, const Table& t) {
+                                                 int64_t stride, const Table& t, const int32_t* sadj = nullptr,
+                                                 const double* sw = nullptr, int64_t a0 = 0, int64_t w0 = 0) {
   const int lane = threadIdx.x & 31;
   for (int64_t base = first; base < eend; base += kUnroll * stride) {
     int u[kUnroll], c[kUnroll];
@@ -336,8 +339,13 @@ __device__ __forceinline__ void accumulate_edges(const MoveArgs& p, int v, int64
       u[k] = -1;
       wt[k] = 0.;
       if (j < eend) {
-        u[k] = p.adj[j];
-        wt[k] = p.w[j];
+        if (sadj) {
+          u[k] = sadj[j - a0];
+          wt[k] = sw[j - w0];
+        } else {
+          u[k] = p.adj[j];
+          wt[k] = p.w[j];
+        }
       }
     }
 #pragma unroll
@@ -642,19 +650,112 @@ __device__ __forceinline__ void block_evaluate(const MoveArgs& p, double m, cons
   }
 }
 
+// ---- staged adjacency: 1-D bulk copies (TMA) of a vertex's edge ranges --------
+// One thread copies the next vertex's ids and weights from this GPU's global
+// memory into shared memory with cp.async.bulk, completed on an mbarrier,
+// while the block still evaluates the current vertex; the block then reads
+// the edges from shared memory.  Copies start and end on 16-byte boundaries:
+// the id range is widened to multiples of 4 ids and the weight range to
+// multiples of 2 weights (the edge arrays carry 4 spare entries so the widened
+// end stays inside them).  No multicast.
+__device__ __forceinline__ unsigned smem_u32(const void* ptr) { return (unsigned)__cvta_generic_to_shared(ptr); }
+
+__device__ __forceinline__ void mbar_init(unsigned long long* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(unsigned long long* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred P;\n mbarrier.try_wait.parity.shared::cta.b64 P, [%1], %2;\n selp.u32 %0, 1, 0, P;\n}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// bounded wait: gives up (false) after kMbarTries attempts instead of spinning
+// forever; the caller counts the failure in p.err
+constexpr int kMbarTries = 1 << 20;
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity) {
+  for (int i = 0; i < kMbarTries; ++i)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
+
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+
+// shared memory of one staged vertex of degree <= kDeg: ids then weights
+template <int kDeg>
+struct Stage {
+  static constexpr int kIds = kDeg + 8;     // widened by up to 3 ids each side
+  static constexpr int kWts = kDeg + 4;     // widened by up to 1 weight each side
+  static constexpr size_t kBytes = (size_t)kIds * 4 + (size_t)kWts * 8;
+};
+
+// Thread 0: copy the edges [s, e) into the stage (ids at sadj, weights at
+// sw) on bar; *a0 / *w0 receive the first id / weight index held.
+__device__ __forceinline__ void stage_edges(const MoveArgs& p, int64_t s, int64_t e, int32_t* sadj, double* sw,
+                                            unsigned long long* bar, int64_t* a0, int64_t* w0) {
+  const int64_t ia = s & ~(int64_t)3, ib = (e + 3) & ~(int64_t)3;
+  const int64_t wa = s & ~(int64_t)1, wb = (e + 1) & ~(int64_t)1;
+  const unsigned bi = (unsigned)(4 * (ib - ia)), bw = (unsigned)(8 * (wb - wa));
+  *a0 = ia;
+  *w0 = wa;
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // earlier reads of the stage come first
+  mbar_arrive_expect_tx(bar, bi + bw);
+  if (bi) bulk_g2s(sadj, p.adj + ia, bi, bar);
+  if (bw) bulk_g2s(sw, p.w + wa, bw, bar);
+}
+
 // ---- 256 < degree <= 2048: one CTA per vertex, table in shared memory ----------
 // kOcc: keep a list of occupied slots (16 bytes a slot) so evaluation and
 // clearing touch only used slots; without it (12 bytes a slot, for the
 // largest FP64 table) both walk the vertex's whole table.  Packed integer
 // tables (kInts) always keep the list: 12 bytes a slot with it.
-template <int kThreads, int kCap, bool kMulti, bool kInts, bool kOcc = true>
+// kStageDeg > 0: the tier's vertices (degree <= kStageDeg) have their edges
+// staged in shared memory behind the table (see stage_edges), one vertex
+// ahead: the copy of vertex i+1 runs while vertex i is evaluated.
+template <int kThreads, int kCap, bool kMulti, bool kInts, bool kOcc = true, int kStageDeg = 0>
 __global__ void __launch_bounds__(kThreads) k_move_cta(const int32_t* __restrict__ list, int64_t n, MoveArgs p) {
   constexpr bool kList = kOcc || kInts;
-  extern __shared__ double smem[];
+  constexpr bool kStaged = kStageDeg > 0;
+  extern __shared__ __align__(128) double smem[];
   __shared__ double sg[32];
   __shared__ unsigned long long stk[32];
   __shared__ int sc[32];
   __shared__ int nocc_s;
+  __shared__ unsigned long long stage_bar;
+  __shared__ long long stage_off[2];  // first id and weight index held by the stage
+  int32_t* sadj = nullptr;
+  double* sw = nullptr;
+  if constexpr (kStaged) {
+    char* st = reinterpret_cast<char*>(smem) + table_bytes(kCap, kInts);
+    sadj = reinterpret_cast<int32_t*>(st);
+    sw = reinterpret_cast<double*>(st + (size_t)Stage<kStageDeg>::kIds * 4);
+    if (threadIdx.x == 0) {
+      mbar_init(&stage_bar, 1);
+      if (blockIdx.x < n) {  // the first vertex's edges start on their way at once
+        const int v0 = list[blockIdx.x];
+        int64_t a0, w0;
+        stage_edges(p, p.off[v0], p.off[v0 + 1], sadj, sw, &stage_bar, &a0, &w0);
+        stage_off[0] = a0;
+        stage_off[1] = w0;
+      }
+    }
+  }
+  unsigned stage_parity = 0;
   Table t;
   if constexpr (kInts) {
     t.slots = reinterpret_cast<unsigned long long*>(smem);
@@ -690,16 +791,35 @@ __global__ void __launch_bounds__(kThreads) k_move_cta(const int32_t* __restrict
   for (; task < n; task += gridDim.x) {
     const int64_t nt = task + gridDim.x;
     const int vn = nt < n ? list[nt] : 0;
-    t.mask = min((unsigned)kCap, next_pow2_cap(eend - s)) - 1;
-    accumulate_edges<true, 4>(p, v, s + (int64_t)wid * 32, eend, kThreads, t);
-    __syncthreads();
-    const int nu = kList ? nocc_s : (int)(t.mask + 1);
     int64_t sn = 0, en = 0;
-    int ownn = 0;
-    double kin = 0.;
     if (nt < n) {
       sn = p.off[vn];
       en = p.off[vn + 1];
+    }
+    t.mask = min((unsigned)kCap, next_pow2_cap(eend - s)) - 1;
+    if constexpr (kStaged) {
+      if (!mbar_wait(&stage_bar, stage_parity)) atomicAdd(p.err, 1ull);
+      stage_parity ^= 1u;
+      accumulate_edges<true, 4>(p, v, s + (int64_t)wid * 32, eend, kThreads, t, sadj, sw, stage_off[0],
+                                stage_off[1]);
+    } else {
+      accumulate_edges<true, 4>(p, v, s + (int64_t)wid * 32, eend, kThreads, t);
+    }
+    __syncthreads();
+    if constexpr (kStaged) {
+      // every thread has read the stage (and stage_off): the next vertex's
+      // edges go into it while this one is evaluated
+      if (threadIdx.x == 0 && nt < n) {
+        int64_t a0, w0;
+        stage_edges(p, sn, en, sadj, sw, &stage_bar, &a0, &w0);
+        stage_off[0] = a0;
+        stage_off[1] = w0;
+      }
+    }
+    const int nu = kList ? nocc_s : (int)(t.mask + 1);
+    int ownn = 0;
+    double kin = 0.;
+    if (nt < n) {
       ownn = p.comm[vn];
       kin = p.k[vn];
     }
@@ -1234,6 +1354,9 @@ constexpr int kCtaLThreads = 256;
 constexpr int kCtaSCap = 1024;
 constexpr int kCtaMCap = 2048;
 constexpr int kCtaLCap = 4096;
+// CTA-S and CTA-M with staged edges: table plus one vertex's widened ranges
+constexpr size_t smem_s_staged(bool ints) { return table_bytes(kCtaSCap, ints) + Stage<kCtaSMaxDeg>::kBytes; }
+constexpr size_t smem_m_staged(bool ints) { return table_bytes(kCtaMCap, ints) + Stage<kCtaMMaxDeg>::kBytes; }
 constexpr int kCtaXAThreads = 512;
 constexpr int kCtaXACap = 8192;   // 512-thread CTA-XA tier, two CTAs an SM (occupied list in integer phases)
 constexpr int kCtaXCap = 16384;   // 1024-thread CTA-XL tier (occupied list in integer phases)
@@ -1251,7 +1374,7 @@ namespace {
 // more would leave a partial wave at the end.
 struct Resident {
   int64_t g4 = kSMs, g8 = kSMs, g16 = kSMs, g32 = kSMs, warp = kSMs, ctas = kSMs, ctam = kSMs, ctal = kSMs,
-          ctaxa = kSMs, ctax = kSMs, hubmv = kSMs, hubins = kSMs, hubsl = kSMs;
+          ctaxa = kSMs, ctax = kSMs, hubmv = kSMs, hubins = kSMs, hubsl = kSMs, ctas_st = kSMs, ctam_st = kSMs;
 };
 Resident g_resident[2][2];  // [many graphs][integer tables]
 
@@ -1270,6 +1393,8 @@ int set_smem_mode() {
   NIDO_TRY(set_smem(k_move_warp<kWarpCap, kMulti, kInts>, 8 * table_bytes(kWarpCap, kInts)));
   NIDO_TRY(set_smem(k_move_cta<kCtaSThreads, kCtaSCap, kMulti, kInts>, table_bytes(kCtaSCap, kInts)));
   NIDO_TRY(set_smem(k_move_cta<kCtaMThreads, kCtaMCap, kMulti, kInts>, table_bytes(kCtaMCap, kInts)));
+  NIDO_TRY(set_smem(k_move_cta<kCtaSThreads, kCtaSCap, kMulti, kInts, true, kCtaSMaxDeg>, smem_s_staged(kInts)));
+  NIDO_TRY(set_smem(k_move_cta<kCtaMThreads, kCtaMCap, kMulti, kInts, true, kCtaMMaxDeg>, smem_m_staged(kInts)));
   NIDO_TRY(set_smem(k_move_cta<kCtaLThreads, kCtaLCap, kMulti, kInts>, table_bytes(kCtaLCap, kInts)));
   NIDO_TRY(set_smem(k_move_cta<kCtaXAThreads, kCtaXACap, kMulti, kInts, false>, (size_t)kCtaXACap * 12));
   NIDO_TRY(set_smem(k_move_cta<1024, kCtaXCap, kMulti, kInts, false>, (size_t)kCtaXCap * 12));
@@ -1286,6 +1411,10 @@ int set_smem_mode() {
   R.warp = resident(k_move_warp<kWarpCap, kMulti, kInts>, 256, 8 * table_bytes(kWarpCap, kInts), sms);
   R.ctas = resident(k_move_cta<kCtaSThreads, kCtaSCap, kMulti, kInts>, kCtaSThreads, table_bytes(kCtaSCap, kInts), sms);
   R.ctam = resident(k_move_cta<kCtaMThreads, kCtaMCap, kMulti, kInts>, kCtaMThreads, table_bytes(kCtaMCap, kInts), sms);
+  R.ctas_st = resident(k_move_cta<kCtaSThreads, kCtaSCap, kMulti, kInts, true, kCtaSMaxDeg>, kCtaSThreads,
+                       smem_s_staged(kInts), sms);
+  R.ctam_st = resident(k_move_cta<kCtaMThreads, kCtaMCap, kMulti, kInts, true, kCtaMMaxDeg>, kCtaMThreads,
+                       smem_m_staged(kInts), sms);
   R.ctal = resident(k_move_cta<kCtaLThreads, kCtaLCap, kMulti, kInts>, kCtaLThreads, table_bytes(kCtaLCap, kInts), sms);
   R.ctaxa = resident(k_move_cta<kCtaXAThreads, kCtaXACap, kMulti, kInts, false>, kCtaXAThreads,
                      (size_t)kCtaXACap * 12, sms);
@@ -1384,6 +1513,9 @@ int launch_tiers(nido_graph_s* g, int batch, int tie, const MoveArgs& p) {
   NIDO_CUDA_TRY(cudaEventRecord(ctx->fork_ev, main_s));
   for (int i = 0; i < 2; ++i) NIDO_CUDA_TRY(cudaStreamWaitEvent(ctx->aux[i], ctx->fork_ev, 0));
   const int nb = g->nbatches;
+  // edges staged in shared memory by bulk copies from this GPU's memory (not
+  // for edges kept in mapped host memory)
+  const bool staged = !g->host_edges;
   for (int t = kNumTiers - 1; t >= 0; --t) {  // longest chains first
     const cudaStream_t s = t == kTierHub ? ctx->aux[0] : (t >= kTierCtaS ? ctx->aux[1] : main_s);
     const int64_t b0 = g->tier_off[(size_t)t * nb + batch], b1 = g->tier_off[(size_t)t * nb + batch + 1];
@@ -1408,10 +1540,20 @@ int launch_tiers(nido_graph_s* g, int batch, int tie, const MoveArgs& p) {
             list, n, p);
         break;
       case kTierCtaS:
-        k_move_cta<kCtaSThreads, kCtaSCap, kMulti, kInts><<<grid_cap(n, R.ctas), kCtaSThreads, table_bytes(kCtaSCap, kInts), s>>>(list, n, p);
+        if (staged)
+          k_move_cta<kCtaSThreads, kCtaSCap, kMulti, kInts, true, kCtaSMaxDeg>
+              <<<grid_cap(n, R.ctas_st), kCtaSThreads, smem_s_staged(kInts), s>>>(list, n, p);
+        else
+          k_move_cta<kCtaSThreads, kCtaSCap, kMulti, kInts>
+              <<<grid_cap(n, R.ctas), kCtaSThreads, table_bytes(kCtaSCap, kInts), s>>>(list, n, p);
         break;
       case kTierCtaM:
-        k_move_cta<kCtaMThreads, kCtaMCap, kMulti, kInts><<<grid_cap(n, R.ctam), kCtaMThreads, table_bytes(kCtaMCap, kInts), s>>>(list, n, p);
+        if (staged)
+          k_move_cta<kCtaMThreads, kCtaMCap, kMulti, kInts, true, kCtaMMaxDeg>
+              <<<grid_cap(n, R.ctam_st), kCtaMThreads, smem_m_staged(kInts), s>>>(list, n, p);
+        else
+          k_move_cta<kCtaMThreads, kCtaMCap, kMulti, kInts>
+              <<<grid_cap(n, R.ctam), kCtaMThreads, table_bytes(kCtaMCap, kInts), s>>>(list, n, p);
         break;
       case kTierCtaL:
         k_move_cta<kCtaLThreads, kCtaLCap, kMulti, kInts><<<grid_cap(n, R.ctal), kCtaLThreads, table_bytes(kCtaLCap, kInts), s>>>(list, n, p);
