@@ -41,9 +41,9 @@ PEAKS_FALLBACK = {"hbm_gbs": 6650.0}
 
 # DRAM bytes the move kernels move per algorithmic byte (16 B per edge +
 # 32 B per vertex per sweep): ncu dram__bytes_read.sum + dram__bytes_write.sum
-# over every move kernel of one whole R-MAT scale 20 run (84 sweeps), 26.19 GB
-# against 20.71 GB algorithmic, cold cache per kernel (an upper bound).
-MOVE_TRAFFIC_PER_ALGO_BYTE = 1.26
+# of one-kernel, two-launch captures of the warp, CTA-S, CTA-M, CTA-XA and
+# CTA-XL tiers on R-MAT scale 20, edge-weighted (cold cache per launch).
+MOVE_TRAFFIC_PER_ALGO_BYTE = 1.01
 
 
 def peaks():
@@ -321,7 +321,7 @@ def run_ours(args, world, rank, local):
                      "traffic": MOVE_TRAFFIC_PER_ALGO_BYTE * move_bytes / sweeps,
                      "algorithmic_bytes": move_bytes / sweeps,
                      "kernel": "move phase (degree-tier kernels of one sweep; per-sweep bytes)",
-                     "traffic_kind": "ncu DRAM bytes per algorithmic byte on R-MAT scale 20, scaled",
+                     "traffic_kind": "ncu DRAM bytes per algorithmic byte of the move-tier kernels (one-kernel captures, R-MAT scale 20), scaled",
                      "peak_kind": pk_kind},
         "cpu_baseline": cpu,
         "clocks": clocks,
@@ -452,7 +452,7 @@ def run_many(args, world, rank, local):
                      "traffic": MOVE_TRAFFIC_PER_ALGO_BYTE * move_bytes / max(1, sum(r[4].total_loops for r in runs)),
                      "algorithmic_bytes": move_bytes / max(1, sum(r[4].total_loops for r in runs)),
                      "kernel": "move phase (degree-tier kernels of one sweep over all graphs; per-sweep bytes)",
-                     "traffic_kind": "ncu DRAM bytes per algorithmic byte on R-MAT scale 20, scaled",
+                     "traffic_kind": "ncu DRAM bytes per algorithmic byte of the move-tier kernels (one-kernel captures, R-MAT scale 20), scaled",
                      "peak_kind": pk_kind},
         "cpu_baseline": cpu,
         "clocks": clocks,
