@@ -306,7 +306,7 @@ extern "C" int nido_graph_free(nido_graph g) {
   dev_free(ctx, g->dm, 64); dev_free(ctx, g->dcount, 64);
   dev_free(ctx, g->scratch, g->scratch_bytes);
   // hub-tier buffers are sized per phase outside the budget accounting
-  for (void* p : {(void*)g->gkeys, (void*)g->gvals, (void*)g->hub_items, (void*)g->hub_v, (void*)g->hub_capv,
+  for (void* p : {(void*)g->gkeys, (void*)g->gvals, (void*)g->gpacked, (void*)g->hub_items, (void*)g->hub_v, (void*)g->hub_capv,
                   (void*)g->hub_nseg, (void*)g->hub_toff, (void*)g->hub_done, (void*)g->hub_slices,
                   (void*)g->hub_slice_first, (void*)g->hub_res, (void*)g->hub_item_first,
                   (void*)g->hub_part, (void*)g->hub_cl_v, (void*)g->agg_buf, (void*)g->pm32,
@@ -525,7 +525,7 @@ extern "C" int nido_graph_device_bytes(nido_graph g, int64_t* bytes) {
   if (!g || !bytes) return nido_set_error(NIDO_E_INVALID, "null argument");
   const int64_t V = g->cap_v, E = g->host_edges ? 0 : g->cap_e;  // mapped host edges hold no HBM
   int64_t b = 24 * (V + 1) + 36 * E + 28 * V + 4 * g->nv0 + 128 + (int64_t)g->scratch_bytes;
-  b += 12 * g->gslab + 8 * g->hub_cap_items + 4 * (g->hub_cap_hubs_v + g->hub_cap_hubs_c + g->hub_cap_hubs_s +
+  b += 12 * g->gslab + 8 * g->gslab_packed + 8 * g->hub_cap_items + 4 * (g->hub_cap_hubs_v + g->hub_cap_hubs_c + g->hub_cap_hubs_s +
                                                    g->hub_cap_hubs_d) +
        8 * (g->hub_cap_hubs_t + g->hub_cap_slices + g->hub_cap_first) + g->hub_cap_res + (int64_t)g->agg_buf_bytes + 4 * g->pm32_cap;
   *bytes = b;

@@ -147,6 +147,10 @@ struct nido_graph_s {
   int32_t* gkeys = nullptr;
   double* gvals = nullptr;
   int64_t gslab = 0;
+  // the same region as packed 64-bit slots (id, int32 sum) for integer-weight
+  // phases; gslab_need is the current plan's size
+  unsigned long long* gpacked = nullptr;
+  int64_t gslab_packed = 0, gslab_need = 0;
   int2* hub_items = nullptr;
   int32_t* hub_v = nullptr;
   int32_t* hub_capv = nullptr;

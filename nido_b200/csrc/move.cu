@@ -439,6 +439,67 @@ __device__ __forceinline__ void merge_edges_global(const MoveArgs& p, int v, int
   }
 }
 
+// merge_edges_global for packed integer tables (integer-weight phases): one
+// 64-bit slot per community (id, int32 sum), so a new community is one
+// compare-and-swap that also carries its first sum, an existing one one
+// 32-bit add.  Equal communities within a chunk are still folded onto one
+// lane first (fewer L2 atomics).
+template <int kUnroll>
+__device__ __forceinline__ void merge_edges_packed(const MoveArgs& p, int v, int64_t first, int64_t eend,
+                                                   int64_t stride, unsigned long long* slots, unsigned mask) {
+  const int lane = threadIdx.x & 31;
+  for (int64_t base = first; base < eend; base += kUnroll * stride) {
+    int u[kUnroll], c[kUnroll], x[kUnroll];
+    double wt[kUnroll];
+    unsigned h[kUnroll];
+#pragma unroll
+    for (int k = 0; k < kUnroll; ++k) {
+      const int64_t j = base + k * stride + lane;
+      u[k] = -1;
+      wt[k] = 0.;
+      if (j < eend) {
+        u[k] = p.adj[j];
+        wt[k] = p.w[j];
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < kUnroll; ++k) {
+      c[k] = u[k] >= 0 ? p.comm[u[k]] : -1;
+      if (u[k] == v) wt[k] = 0.;
+    }
+    unsigned pending = 0u;
+#pragma unroll
+    for (int k = 0; k < kUnroll; ++k) {
+      const bool ok = u[k] >= 0;
+      const unsigned peers = __match_any_sync(NIDO_FULL_MASK, c[k]);
+      x[k] = __double2int_rn(fold_peers(peers, ok, wt[k]));
+      if (ok && lane == __ffs(peers) - 1) pending |= 1u << k;
+      h[k] = ok ? hash_slot(c[k], mask) : 0u;
+    }
+    for (unsigned probe = 0; pending != 0u && probe <= mask; ++probe) {
+      unsigned long long old[kUnroll];
+#pragma unroll
+      for (int k = 0; k < kUnroll; ++k)
+        old[k] = (pending >> k & 1u)
+                     ? atomicCAS(&slots[h[k]], kEmptySlot, ((unsigned long long)(unsigned)c[k] << 32) | (unsigned)x[k])
+                     : 0ull;
+#pragma unroll
+      for (int k = 0; k < kUnroll; ++k) {
+        if (!(pending >> k & 1u)) continue;
+        if (old[k] == kEmptySlot) {
+          pending &= ~(1u << k);
+        } else if (slot_key(old[k]) == c[k]) {
+          atomicAdd(reinterpret_cast<int*>(&slots[h[k]]), x[k]);
+          pending &= ~(1u << k);
+        } else {
+          h[k] = (h[k] + 1) & mask;
+        }
+      }
+    }
+    if (pending != 0u) atomicAdd(p.err, 1ull);
+  }
+}
+
 // Scan entries i = t0, t0+step, ... of the occupied list (or of all slots when
 // occ is null): e_own and the best (gain, tie key, community) of this thread.
 // Entries are taken four at a time so that their a_c gathers are in flight
@@ -997,6 +1058,84 @@ __global__ void __launch_bounds__(kHubThreads) k_hub_slices(const int2* __restri
   }
 }
 
+// k_hub_insert / k_hub_slices on packed integer tables
+__global__ void __launch_bounds__(kHubThreads) k_hub_insert_packed(const int2* __restrict__ items, int64_t n,
+                                                                   const int32_t* __restrict__ hub_v,
+                                                                   const int64_t* __restrict__ hub_toff,
+                                                                   const int32_t* __restrict__ hub_cap,
+                                                                   unsigned long long* gslots, MoveArgs p) {
+  const int wid = threadIdx.x >> 5;
+  for (int64_t it = blockIdx.x; it < n; it += gridDim.x) {
+    const int2 item = items[it];
+    const int h = item.x;
+    const int v = hub_v[h];
+    const int64_t s = p.off[v], eend = p.off[v + 1];
+    const int64_t s0 = s + (int64_t)item.y * kHubSeg;
+    merge_edges_packed<4>(p, v, s0 + (int64_t)wid * 32, min(eend, s0 + kHubSeg), kHubThreads, gslots + hub_toff[h],
+                          (unsigned)hub_cap[h] - 1);
+  }
+}
+
+template <bool kMulti>
+__global__ void __launch_bounds__(kHubThreads) k_hub_slices_packed(const int2* __restrict__ slices, int64_t n,
+                                                                   const int32_t* __restrict__ hub_v,
+                                                                   const int64_t* __restrict__ hub_toff,
+                                                                   const int32_t* __restrict__ hub_cap,
+                                                                   unsigned long long* gslots, MoveArgs p,
+                                                                   SliceResult* __restrict__ res) {
+  __shared__ double sg[32];
+  __shared__ unsigned long long stk[32];
+  __shared__ int sc[32];
+  for (int64_t it = blockIdx.x; it < n; it += gridDim.x) {
+    const int2 sl = slices[it];
+    const int len = min(kHubSlice, hub_cap[sl.x] - sl.y * kHubSlice);
+    const int v = hub_v[sl.x];
+    unsigned long long* slots = gslots + hub_toff[sl.x] + (int64_t)sl.y * kHubSlice;
+    const int own = p.comm[v];
+    const double ki = p.k[v];
+    const double m = vertex_mass<kMulti>(p, v);
+    double g = -NIDO_MAX_FLOAT, eown = 0.;
+    unsigned long long tk = kNoKey;
+    int cand = -1;
+    constexpr int U = 4;
+    for (int i0 = threadIdx.x; i0 < len; i0 += U * kHubThreads) {
+      int cc[U];
+      double val[U], ac[U];
+#pragma unroll
+      for (int k = 0; k < U; ++k) {
+        const int i = i0 + k * kHubThreads;
+        cc[k] = -1;
+        if (i < len) {
+          const unsigned long long x = __ldcg(&slots[i]);
+          cc[k] = slot_key(x);
+          val[k] = (double)slot_sum(x);
+        }
+      }
+#pragma unroll
+      for (int k = 0; k < U; ++k) ac[k] = (cc[k] >= 0 && cc[k] != own) ? p.a[cc[k]] : 0.;
+#pragma unroll
+      for (int k = 0; k < U; ++k) {
+        if (cc[k] < 0) continue;
+        slots[i0 + k * kHubThreads] = kEmptySlot;
+        if (cc[k] == own) {
+          eown = val[k];
+        } else {
+          const double gg = gain_of(val[k], ki, ac[k], m);
+          if (better(gg, (unsigned)cc[k], g, tk)) { g = gg; tk = (unsigned)cc[k]; cand = cc[k]; }
+        }
+      }
+    }
+    eown = block_sum(eown, sg);
+    block_best(g, tk, cand, sg, stk, sc);
+    if (threadIdx.x == 0) res[it] = SliceResult{g, eown, tk, cand, 0};
+  }
+}
+
+__global__ void k_fill_u64(unsigned long long* __restrict__ x, int64_t n, unsigned long long val) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    x[i] = val;
+}
+
 template <bool kMulti>
 __global__ void k_hub_combine(int64_t nh, const int32_t* __restrict__ hub_v, const int64_t* __restrict__ slice_first,
                               const SliceResult* __restrict__ res, MoveArgs p) {
@@ -1288,6 +1427,7 @@ int plan_hubs(nido_graph_s* g) {
   ifirst[nh] = (int64_t)items.size();
   g->hub_nitems = (int64_t)items.size();
   const int64_t toff = maxslots;
+  g->gslab_need = toff;
   NIDO_TRY(ensure(g, &g->hub_v, &g->hub_cap_hubs_v, nh));
   NIDO_TRY(ensure(g, &g->hub_capv, &g->hub_cap_hubs_c, nh));
   NIDO_TRY(ensure(g, &g->hub_nseg, &g->hub_cap_hubs_s, nh));
@@ -1313,6 +1453,17 @@ int plan_hubs(nido_graph_s* g) {
     NIDO_CUDA_TRY(cudaMemsetAsync(g->gkeys, 0xff, sizeof(int32_t) * (size_t)toff, s));
     NIDO_CUDA_TRY(cudaMemsetAsync(g->gvals, 0, sizeof(double) * (size_t)toff, s));
     g->gslab = toff;
+  }
+  // packed tables for integer-weight phases (smallest-id rule), kept empty
+  // between waves by the slice scans like the FP64 ones
+  if (g->int_weights && toff > g->gslab_packed) {
+    raw_free(g->ctx, g->gpacked);
+    g->gpacked = nullptr;
+    g->gslab_packed = 0;
+    NIDO_CUDA_TRY(raw_alloc(g->ctx, (void**)&g->gpacked, sizeof(unsigned long long) * (size_t)toff));
+    k_fill_u64<<<grid_cap((toff + 255) / 256, kSMs * 8), 256, 0, s>>>(g->gpacked, toff, kEmptySlot);
+    NIDO_LAUNCH_CHECK();
+    g->gslab_packed = toff;
   }
   NIDO_CUDA_TRY(cudaMemcpyAsync(g->hub_v, hv.data(), sizeof(int32_t) * nh, cudaMemcpyHostToDevice, s));
   NIDO_CUDA_TRY(cudaMemcpyAsync(g->hub_capv, hcap.data(), sizeof(int32_t) * nh, cudaMemcpyHostToDevice, s));
@@ -1585,13 +1736,22 @@ int launch_tiers(nido_graph_s* g, int batch, int tie, const MoveArgs& p) {
             NIDO_LAUNCH_CHECK();
             continue;
           }
-          k_hub_insert<<<grid_cap(w.i1 - w.i0, R.hubins), kHubThreads, 0, s>>>(
-              items, w.i1 - w.i0, g->hub_v, g->hub_toff, g->hub_capv, g->gkeys, g->gvals, p);
-          NIDO_LAUNCH_CHECK();
-          k_hub_slices<kMulti><<<grid_cap(w.s1 - w.s0, R.hubsl), kHubThreads, 0, s>>>(
-              g->hub_slices + w.s0, w.s1 - w.s0, g->hub_v, g->hub_toff, g->hub_capv, g->gkeys, g->gvals, p,
-              res + w.s0);
-          NIDO_LAUNCH_CHECK();
+          if (kInts && g->gpacked && g->gslab_packed >= g->gslab_need) {
+            k_hub_insert_packed<<<grid_cap(w.i1 - w.i0, R.hubins), kHubThreads, 0, s>>>(
+                items, w.i1 - w.i0, g->hub_v, g->hub_toff, g->hub_capv, g->gpacked, p);
+            NIDO_LAUNCH_CHECK();
+            k_hub_slices_packed<kMulti><<<grid_cap(w.s1 - w.s0, R.hubsl), kHubThreads, 0, s>>>(
+                g->hub_slices + w.s0, w.s1 - w.s0, g->hub_v, g->hub_toff, g->hub_capv, g->gpacked, p, res + w.s0);
+            NIDO_LAUNCH_CHECK();
+          } else {
+            k_hub_insert<<<grid_cap(w.i1 - w.i0, R.hubins), kHubThreads, 0, s>>>(
+                items, w.i1 - w.i0, g->hub_v, g->hub_toff, g->hub_capv, g->gkeys, g->gvals, p);
+            NIDO_LAUNCH_CHECK();
+            k_hub_slices<kMulti><<<grid_cap(w.s1 - w.s0, R.hubsl), kHubThreads, 0, s>>>(
+                g->hub_slices + w.s0, w.s1 - w.s0, g->hub_v, g->hub_toff, g->hub_capv, g->gkeys, g->gvals, p,
+                res + w.s0);
+            NIDO_LAUNCH_CHECK();
+          }
           k_hub_combine<kMulti><<<grid_cap((w.h1 - w.h0 + 7) / 8, kSMs * 4), 256, 0, s>>>(
               w.h1 - w.h0, g->hub_v + w.h0, g->hub_slice_first + w.h0, res, p);
           NIDO_LAUNCH_CHECK();

@@ -131,7 +131,8 @@ void worker_loop(nido_server_s* S, int wid) {
 
 // Upload (three CSR copies, per-vertex state, scratch as nido_graph_upload
 // sizes them); the hub-table region, one wave of tables at 12 bytes a slot
-// (at most 8M slots, or one table of up to 4*nv slots); the coarsening
+// plus its packed 8-byte copy for integer phases (at most 8M slots, or one
+// table of up to 4*nv slots); the coarsening
 // plan's region for giant communities, one wave at 16 bytes a slot (at most
 // 4M slots or one table of up to 4*nv), grown by a quarter, plus its
 // per-vertex and per-segment lists; and the hub work lists.
@@ -146,7 +147,7 @@ extern "C" int64_t nido_graph_footprint(int64_t nv, int64_t ne, int32_t nbatches
   const int64_t V = std::max<int64_t>(nv, 1), E = std::max<int64_t>(ne, 1);
   int64_t b = 24 * (V + 1) + 36 * E + 32 * V + 128;
   b += 64 * (V + 1) + (1 << 20) + 8 * (nido::radix_temp_elems(V) + nido::scan_temp_elems(E + 1));
-  b += 12 * std::max<int64_t>((int64_t)8 << 20, 4 * V);
+  b += 20 * std::max<int64_t>((int64_t)8 << 20, 4 * V);  // FP64 and packed hub tables
   b += 20 * std::max<int64_t>((int64_t)4 << 20, 4 * V) + 40 * V + E / 32;
   b += 4 * (E / 32 + 2);  // member index of the coarsening's 32-position blocks
   b += E;  // first-position bitmaps and word prefixes of the giant segments
