@@ -208,8 +208,10 @@ def run_ours(args, world, rank, local):
     ctx = capi.Context(local)
     stream = torch.cuda.ExternalStream(ctx.stream())
     g = capi.Graph(ctx, G, wl["nbatches"])
+    outbuf = np.empty(G.nv, np.int64)  # page-locked result buffer, reused every step
+    capi.host_register(outbuf)
     for _ in range(args.warmup):
-        g.run(tau=wl["tau"])
+        g.run(tau=wl["tau"], out=outbuf)
     barrier(world)
     torch.cuda.synchronize()
     ctx.sync()
@@ -218,7 +220,7 @@ def run_ours(args, world, rank, local):
     l0 = capi.lib().nido_launch_count()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    stats = [g.run(tau=wl["tau"])[1] for _ in range(args.steps)]
+    stats = [g.run(tau=wl["tau"], out=outbuf)[1] for _ in range(args.steps)]
     e1.record(stream)
     ctx.sync()
     torch.cuda.synchronize()
@@ -257,12 +259,12 @@ def run_ours(args, world, rank, local):
     f0.record(stream)
     for _ in range(args.steps):
         with capi.Graph(ctx, G, wl["nbatches"]) as g2:
-            part, _ = g2.run(tau=wl["tau"])
+            part, _ = g2.run(tau=wl["tau"], out=outbuf)
     f1.record(stream)
     ctx.sync()
     torch.cuda.synchronize()
     e2e_ms = reduce_max(f0.elapsed_time(f1), world)
-    for a in (G.off, G.adj, G.w):
+    for a in (G.off, G.adj, G.w, outbuf):
         capi.host_unregister(a)
 
     color = None
@@ -351,8 +353,10 @@ def run_many(args, world, rank, local):
     ctx = capi.Context(local)
     stream = torch.cuda.ExternalStream(ctx.stream())
     B = capi.Batch(ctx, nbatches=wl["nbatches"], packed=(vbase, U))
+    outbuf = np.empty(U.nv, np.int64)  # page-locked result buffer, reused every step
+    capi.host_register(outbuf)
     for _ in range(args.warmup):
-        res = B.run(tau=wl["tau"])
+        res = B.run(tau=wl["tau"], out=outbuf)
     barrier(world)
     ctx.sync()
     sampler = ClockSampler(local)
@@ -360,7 +364,7 @@ def run_many(args, world, rank, local):
     l0 = capi.lib().nido_launch_count()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    runs = [B.run(tau=wl["tau"]) for _ in range(args.steps)]
+    runs = [B.run(tau=wl["tau"], out=outbuf) for _ in range(args.steps)]
     e1.record(stream)
     ctx.sync()
     launches = int(capi.lib().nido_launch_count() - l0)
@@ -400,11 +404,11 @@ def run_many(args, world, rank, local):
     f0.record(stream)
     for _ in range(args.steps):
         with capi.Batch(ctx, nbatches=wl["nbatches"], packed=(vbase, U)) as b2:
-            b2.run(tau=wl["tau"])
+            b2.run(tau=wl["tau"], out=outbuf)
     f1.record(stream)
     ctx.sync()
     e2e_ms = reduce_max(f0.elapsed_time(f1), world)
-    for a in (U.off, U.adj, U.w):
+    for a in (U.off, U.adj, U.w, outbuf):
         capi.host_unregister(a)
 
     cpu = None
@@ -463,6 +467,10 @@ def run_many(args, world, rank, local):
                                   "other": ms_max / args.steps - (move_ms + sum(r[4].q_ms + r[4].agg_ms
                                                                                for r in runs)) / len(runs)},
         "loop_graph_build_ms_per_step": sum(r[4].host_ms[7] for r in runs) / len(runs),
+        "host_sections_ms_per_step": {
+            k: sum(r[4].host_ms[i] for r in runs) / len(runs)
+            for i, k in enumerate(("reset", "sweeps", "list_rebuilds", "phase_end_aggregation_emit",
+                                   "phase_setup", "download"))},
         "latency_ms": serving["latency_ms"] if serving else None,
         "serving": ({k: serving[k] for k in ("graphs_per_s", "requests", "latency_ms", "overlap", "workload")}
                     if serving else None),

@@ -101,7 +101,12 @@ typedef struct {
    * [1] enqueueing moves and commits, [2] modularity including the wait for
    * the device, [3] aggregation, [4] per-phase preparation after
    * aggregation, [5] download of the clustering, [6] autotuning, [7] capture
-   * and instantiation of the device-resident loop graphs */
+   * and instantiation of the device-resident loop graphs.  Batched runs
+   * (nido_batch_run): [0] reset, [1] sweeps (moves, commits, modularity,
+   * loop control and their readbacks; [7] is part of it), [2] tier-list
+   * rebuilds after graphs stop iterating, [3] phase end, aggregation and
+   * emits, [4] phase set-up (graph ids, masses, cuts, lists, singleton
+   * start, Q_old), [5] download of the results */
   double host_ms[8];
   double q_phase[200];
   int64_t loops_phase[200];
@@ -229,6 +234,11 @@ typedef struct {
                                 every hub of the phase fits: degree <= 196,608);
                                 0 (default): hub tables in global memory */
   int64_t hub_wave_slots;    /* hub-table slots processed together (L2 residency) */
+  int32_t staged_edges;      /* 1: the CTA-S and CTA-M tiers copy the next vertex's ids and
+                                weights into shared memory with 1-D bulk copies (TMA) while
+                                the current vertex is evaluated; 0 (default): they read
+                                them from global memory (faster on R-MAT scale 22) */
+  int32_t reserved;          /* must be 0 */
 } nido_tier_config;
 /* Thresholds must be non-decreasing, at least 32 and within the capacities
  * above; results on integer weights do not depend on them. */

@@ -56,7 +56,8 @@ _lib = None
 class TierConfig(C.Structure):
     _fields_ = [("warp_max_degree", C.c_int32), ("cta_s_max_degree", C.c_int32),
                 ("cta_m_max_degree", C.c_int32), ("cta_l_max_degree", C.c_int32),
-                ("cta_x_max_degree", C.c_int32), ("hub_clusters", C.c_int32), ("hub_wave_slots", C.c_int64)]
+                ("cta_x_max_degree", C.c_int32), ("hub_clusters", C.c_int32), ("hub_wave_slots", C.c_int64),
+                ("staged_edges", C.c_int32), ("reserved", C.c_int32)]
 
     def as_dict(self):
         return {f: getattr(self, f) for f, _ in self._fields_}
@@ -432,20 +433,30 @@ class Graph:
 
     def run(self, tau: float = 1e-6, max_iter: int = 500, tie: int = NIDO_TIE_SMALLEST_ID,
             verbose: bool = False, tune: bool = False, host_loop: bool = False, tau_phase: float | None = None,
-            color_batches: bool = False, device_loop: bool = False):
+            color_batches: bool = False, device_loop: bool = False, out: np.ndarray | None = None):
         """LouvainGPU::run; returns (clustering of the input vertices, RunStats).
         host_loop / device_loop: force who drives each phase's iterations (the
         host, one readback per iteration, or the device-resident loop graph);
         neither: the library picks by the phase's size.  color_batches: every
         phase's colour classes are its batches (conflict-free) instead of the
-        -b cuts."""
+        -b cuts.  out: an int64 array of nv entries to write the clustering
+        into (page-locked with host_register, the download runs at full link
+        speed); a new array by default."""
         p = _Params(self.nbatches, tie, tau, max_iter, int(verbose), int(tune),
                     0.0 if tau_phase is None else tau_phase, int(tau_phase is not None),
                     _loop_mode(host_loop, device_loop), int(color_batches))
-        out = np.empty(self.nv0, np.int64)
+        out = _out_array(out, self.nv0)
         st = RunStats()
         _check(lib().nido_run(self.h, C.byref(p), _p64(out), C.byref(st)))
         return out, st
+
+
+def _out_array(out, n: int) -> np.ndarray:
+    if out is None:
+        return np.empty(n, np.int64)
+    if out.dtype != np.int64 or out.ndim != 1 or out.shape[0] != n or not out.flags.c_contiguous:
+        raise ValueError(f"out must be a contiguous int64 array of {n} entries")
+    return out
 
 
 def _loop_mode(host_loop: bool, device_loop: bool) -> int:
@@ -506,11 +517,12 @@ class Batch:
         self.close()
 
     def run(self, tau: float = 1e-6, max_iter: int = 500, tie: int = NIDO_TIE_SMALLEST_ID,
-            tune: bool = False, host_loop: bool = False, device_loop: bool = False):
+            tune: bool = False, host_loop: bool = False, device_loop: bool = False, out: np.ndarray | None = None):
         """Returns (per-graph clusterings, final Q per graph, phases per graph,
-        loops per graph, RunStats)."""
+        loops per graph, RunStats).  out: as Graph.run, nv entries (the
+        clusterings are views into it)."""
         p = _Params(self.nbatches, tie, tau, max_iter, 0, int(tune), 0.0, 0, _loop_mode(host_loop, device_loop))
-        out = np.empty(self.nv, np.int64)
+        out = _out_array(out, self.nv)
         q = np.empty(self.ngraphs, np.float64)
         ph = np.empty(self.ngraphs, np.int64)
         lo = np.empty(self.ngraphs, np.int64)

@@ -651,13 +651,26 @@ extern "C" int nido_batch_run(nido_batch B, const nido_params* p, int64_t* out_c
   NIDO_CUDA_TRY(cudaEventCreate(&re.a1));
   cudaEvent_t t0 = re.t0, t1 = re.t1;
   std::vector<cudaEvent_t>& ev = g->ctx->move_ev;
-  while (ev.size() < 2) {
+  while (ev.size() < 4) {
     cudaEvent_t e;
     NIDO_CUDA_TRY(cudaEventCreate(&e));
     ev.push_back(e);
   }
+  // host wall time per section (the slots of nido_run_stats.host_ms for
+  // batched runs); the sections end with a stream synchronisation, so each
+  // includes the device work it waits for
+  auto now_ms = [] {
+    return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now().time_since_epoch()).count();
+  };
+  double tm = now_ms();
+  auto lap = [&](int slot) {
+    const double t = now_ms();
+    st.host_ms[slot] += t - tm;
+    tm = t;
+  };
   NIDO_CUDA_TRY(cudaEventRecord(t0, s));
   NIDO_TRY(batch_reset(B));
+  lap(0);
   const int ng = B->ng, nb = g->nbatches;
   const double tau = p->tau;
   const double tau_phase = p->tau_phase_set ? p->tau_phase : p->tau;
@@ -725,6 +738,8 @@ extern "C" int nido_batch_run(nido_batch B, const nido_params* p, int64_t* out_c
     }
     NIDO_TRY(batch_modularity(B, ql, B->Q));
     NIDO_CUDA_TRY(cudaMemcpyAsync(B->Qold, B->Q, sizeof(double) * ng, cudaMemcpyDeviceToDevice, s));
+    NIDO_CUDA_TRY(cudaStreamSynchronize(s));
+    lap(4);
     int64_t n_iter = p->max_iter > 0 ? np : 0;
     // the commit of every batch's listed vertices of the iterating graphs
     auto commit_batch = [&](int b) -> int {
@@ -831,7 +846,7 @@ extern "C" int nido_batch_run(nido_batch B, const nido_params* p, int64_t* out_c
       if (hc.sweeps > 1) nido_count_launches(body_kernels * (uint64_t)(hc.sweeps - 1));
       st.move_launches += (int64_t)nb * hc.sweeps;
       st.edges_scanned += (double)listed_e * (double)hc.sweeps;
-      st.move_bytes += (16.0 * (double)listed_e + 32.0 * (double)listed_v) * (double)hc.sweeps;
+      st.move_bytes += (16.0 * (double)listed_e + 32.0 * (double)listed_vertices(g)) * (double)hc.sweeps;
       st.total_loops += hc.sweeps;
       st.move_ms += hc.move_ns * 1e-6;
       st.q_ms += hc.q_ns * 1e-6;
@@ -859,9 +874,11 @@ extern "C" int nido_batch_run(nido_batch B, const nido_params* p, int64_t* out_c
       NIDO_CUDA_TRY(cudaEventRecord(ev[1], s));
       st.move_launches += nb;
       st.edges_scanned += (double)listed_e;
-      st.move_bytes += 16.0 * (double)listed_e + 32.0 * (double)listed_v;
+      st.move_bytes += 16.0 * (double)listed_e + 32.0 * (double)listed_vertices(g);
       ++st.total_loops;
+      NIDO_CUDA_TRY(cudaEventRecord(ev[2], s));
       NIDO_TRY(batch_modularity(B, ql, B->qnew));
+      NIDO_CUDA_TRY(cudaEventRecord(ev[3], s));
       NIDO_CUDA_TRY(cudaMemsetAsync(B->counters, 0, sizeof(int64_t) * 4, s));
       k_control<<<grid_for((int64_t)ql.ids.size(), 128), 128, 0, s>>>(
           B->llist, (int)ql.ids.size(), B->qnew, B->Q, B->loops_phase, B->loops_total, B->giter, B->grest, tau,
@@ -872,9 +889,12 @@ extern "C" int nido_batch_run(nido_batch B, const nido_params* p, int64_t* out_c
       float ms = 0.f;
       NIDO_CUDA_TRY(cudaEventElapsedTime(&ms, ev[0], ev[1]));
       st.move_ms += ms;
+      NIDO_CUDA_TRY(cudaEventElapsedTime(&ms, ev[2], ev[3]));
+      st.q_ms += ms;
       if (cnt[1]) NIDO_TRY(restore_listed(nullptr));
       n_iter = (int64_t)cnt[0];
       }
+      lap(1);
       // drop stopped graphs from the tier lists once a quarter of the listed
       // vertices belong to them
       if (n_iter > 0 && 4 * (int64_t)cnt[2] < 3 * listed_v) {
@@ -885,6 +905,7 @@ extern "C" int nido_batch_run(nido_batch B, const nido_params* p, int64_t* out_c
         for (int32_t i : act)
           if (flags[i]) { it.push_back(i); listed_v += base[i + 1] - base[i]; listed_e += edges[i]; }
         NIDO_TRY(batch_list(B, it, base, &ql));
+        lap(2);
       }
     }
     // phase end: aggregate the graphs that gained more than tau
@@ -908,7 +929,10 @@ extern "C" int nido_batch_run(nido_batch B, const nido_params* p, int64_t* out_c
         if (!emitted[i] && !flags[i]) { em.push_back(i); emitted[i] = 1; }
       NIDO_TRY(emit(em));
     }
-    if (cnt[3] == 0) break;
+    if (cnt[3] == 0) {
+      lap(3);
+      break;
+    }
     k_drop<<<grid_for(g->nv, kThreads), kThreads, 0, s>>>(g->nv, B->gid, B->gagg, g->comm);
     NIDO_LAUNCH_CHECK();
     int done = 0;
@@ -933,6 +957,7 @@ extern "C" int nido_batch_run(nido_batch B, const nido_params* p, int64_t* out_c
         if (!emitted[i] && flags[i]) { em.push_back(i); emitted[i] = 1; }
       NIDO_TRY(emit(em));
     }
+    lap(3);
     if (done) break;  // every graph kept its size or collapsed: all finished
   }
   {  // graphs still running when the phase cap ended the loop
@@ -941,6 +966,7 @@ extern "C" int nido_batch_run(nido_batch B, const nido_params* p, int64_t* out_c
       if (!emitted[i]) { em.push_back(i); emitted[i] = 1; }
     NIDO_TRY(emit(em));
   }
+  lap(3);
   NIDO_CUDA_TRY(cudaEventRecord(t1, s));
   NIDO_CUDA_TRY(cudaEventSynchronize(t1));
   float tot = 0.f;
@@ -956,6 +982,7 @@ extern "C" int nido_batch_run(nido_batch B, const nido_params* p, int64_t* out_c
   if (out_phases) NIDO_CUDA_TRY(cudaMemcpyAsync(out_phases, B->phases, sizeof(int64_t) * ng, cudaMemcpyDeviceToHost, s));
   if (out_loops) NIDO_CUDA_TRY(cudaMemcpyAsync(out_loops, B->loops_total, sizeof(int64_t) * ng, cudaMemcpyDeviceToHost, s));
   NIDO_CUDA_TRY(cudaStreamSynchronize(s));
+  lap(5);
   st.kernel_launches = (int64_t)(nido_launch_count() - launches0);
   if (stats) *stats = st;
   return NIDO_OK;

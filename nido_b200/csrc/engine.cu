@@ -847,6 +847,7 @@ int tune_tiers(nido_graph_s* g, int tie, int sweeps, double* best_ms) {
   for (int32_t v : {1024, 768}) { TierConfig c = best; c.ctam_max = v; NIDO_TRY(try_cfg(c)); }
   for (int32_t v : {512, 384}) { TierConfig c = best; c.ctas_max = v; NIDO_TRY(try_cfg(c)); }
   for (int32_t v : {128, 64}) { TierConfig c = best; c.warp_max = v; NIDO_TRY(try_cfg(c)); }
+  { TierConfig c = best; c.staged_edges = !c.staged_edges; NIDO_TRY(try_cfg(c)); }
   if (g->max_degree > best.ctax_max) {
     for (int64_t v : {(int64_t)2 << 20, (int64_t)8 << 20}) { TierConfig c = best; c.hub_wave_slots = v; NIDO_TRY(try_cfg(c)); }
     if (g->int_weights && tie != NIDO_TIE_NIDO) { TierConfig c = best; c.hub_clusters = true; NIDO_TRY(try_cfg(c)); }
@@ -863,7 +864,7 @@ int tune_tiers(nido_graph_s* g, int tie, int sweeps, double* best_ms) {
 extern "C" int nido_get_tier_config(nido_graph g, nido_tier_config* c) {
   if (!g || !c) return nido_set_error(NIDO_E_INVALID, "null argument");
   *c = nido_tier_config{g->cfg.warp_max, g->cfg.ctas_max, g->cfg.ctam_max, g->cfg.ctal_max, g->cfg.ctax_max,
-                        g->cfg.hub_clusters ? 1 : 0, g->cfg.hub_wave_slots};
+                        g->cfg.hub_clusters ? 1 : 0, g->cfg.hub_wave_slots, g->cfg.staged_edges ? 1 : 0, 0};
   return NIDO_OK;
 }
 
@@ -879,6 +880,9 @@ extern "C" int nido_set_tier_config(nido_graph g, const nido_tier_config* c) {
   if (c->hub_clusters != 0 && c->hub_clusters != 1)
     return nido_set_error(NIDO_E_INVALID, "hub_clusters must be 0 or 1 (got %d)", c->hub_clusters);
   t.hub_clusters = c->hub_clusters != 0;
+  if (c->staged_edges != 0 && c->staged_edges != 1)
+    return nido_set_error(NIDO_E_INVALID, "staged_edges must be 0 or 1 (got %d)", c->staged_edges);
+  t.staged_edges = c->staged_edges != 0;
   if (!nido::config_ok(t)) return nido_set_error(NIDO_E_INVALID, "tier thresholds out of range or decreasing");
   g->cfg = t;
   g->bins_valid = false;
@@ -1029,7 +1033,7 @@ extern "C" int nido_run(nido_graph g, const nido_params* p, int64_t* out_comm, n
         st.host_ms[7] += r.build_ms;
         st.move_launches += g->nbatches * loops;
         st.edges_scanned += (double)g->ne * (double)loops;
-        st.move_bytes += (16.0 * (double)g->ne + 32.0 * (double)g->nv) * (double)loops;
+        st.move_bytes += (16.0 * (double)g->ne + 32.0 * (double)nido::listed_vertices(g)) * (double)loops;
         if (p->verbose) {
           printf("LOOP# \tQ \t\tdQ\n----------------------------------------\n0 \t%g \t0\n", Q_old);
           for (size_t i = 0; 2 * i + 1 < r.log.size(); ++i)
@@ -1057,7 +1061,7 @@ extern "C" int nido_run(nido_graph g, const nido_params* p, int64_t* out_comm, n
       }
       st.move_launches += g->nbatches;
       st.edges_scanned += (double)g->ne;
-      st.move_bytes += 16.0 * (double)g->ne + 32.0 * (double)g->nv;
+      st.move_bytes += 16.0 * (double)g->ne + 32.0 * (double)nido::listed_vertices(g);
       lap(1);
       double Qtmp;
       NIDO_TRY(modularity(&Qtmp));

@@ -60,6 +60,9 @@ struct TierConfig {
   int32_t ctax_max = kCtaXMaxDeg;
   int64_t hub_wave_slots = (int64_t)4 << 20;
   bool hub_clusters = false;  // hubs on thread-block clusters where they fit
+  // CTA-S / CTA-M vertices' edges staged in shared memory by bulk copies
+  // (move.cu); off by default: slower on R-MAT scale 22 with a warm L2
+  bool staged_edges = false;
 };
 
 struct nido_ctx_s {
@@ -271,6 +274,10 @@ cudaError_t pinned_buffer(nido_ctx_s* ctx, size_t bytes, void** p);
 int device_alloc(nido_ctx_s* ctx, void** p, size_t bytes);
 void device_free(nido_ctx_s* ctx, void* p, size_t bytes);
 int build_batches(nido_graph_s* g);                     // cuts (host) + tier lists
+// vertices in the tier lists (vertices with at least one edge)
+inline int64_t listed_vertices(const nido_graph_s* g) {
+  return g->tier_off.empty() ? g->nv : g->tier_off[(size_t)kNumTiers * g->nbatches];
+}
 // the commit of batch b: the vertex range [cuts[b], cuts[b+1]), or with
 // colour-class batches the batch's vertices in the tier lists
 int launch_commit_batch(nido_graph_s* g, int b);

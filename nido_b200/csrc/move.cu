@@ -1664,9 +1664,9 @@ int launch_tiers(nido_graph_s* g, int batch, int tie, const MoveArgs& p) {
   NIDO_CUDA_TRY(cudaEventRecord(ctx->fork_ev, main_s));
   for (int i = 0; i < 2; ++i) NIDO_CUDA_TRY(cudaStreamWaitEvent(ctx->aux[i], ctx->fork_ev, 0));
   const int nb = g->nbatches;
-  // edges staged in shared memory by bulk copies from this GPU's memory (not
-  // for edges kept in mapped host memory)
-  const bool staged = !g->host_edges;
+  // edges staged in shared memory by bulk copies from this GPU's memory (a
+  // tier option; never for edges kept in mapped host memory)
+  const bool staged = g->cfg.staged_edges && !g->host_edges;
   for (int t = kNumTiers - 1; t >= 0; --t) {  // longest chains first
     const cudaStream_t s = t == kTierHub ? ctx->aux[0] : (t >= kTierCtaS ? ctx->aux[1] : main_s);
     const int64_t b0 = g->tier_off[(size_t)t * nb + batch], b1 = g->tier_off[(size_t)t * nb + batch + 1];

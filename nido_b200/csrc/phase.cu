@@ -435,7 +435,9 @@ __global__ void k_tier_keys(const int64_t* __restrict__ off, int64_t nv, const i
       }
       if (vbatch) vbatch[v] = lo;
       const int64_t d = off[v + 1] - off[v];
-      key = active ? (uint32_t)(tier_of(d, thr) * nb + lo) : skip;
+      // vertices without edges never move (no neighbour community; their
+      // target stays their own community), so no tier lists them
+      key = (active && d > 0) ? (uint32_t)(tier_of(d, thr) * nb + lo) : skip;
       keys[v] = key;
       vals[v] = (uint32_t)v;
       if (active) md = md > (unsigned long long)d ? md : (unsigned long long)d;
@@ -568,6 +570,8 @@ int launch_q_self(nido_graph_s* g, double* selfv) {
   nido_ctx_s* ctx = g->ctx;
   static const QResident g_qres = q_resident_all();  // once per process (thread-safe)
   const cudaStream_t main_s = ctx->stream;
+  // vertices in no tier list (no edges) have no in-community weight
+  NIDO_CUDA_TRY(cudaMemsetAsync(selfv, 0, sizeof(double) * (size_t)g->nv, main_s));
   NIDO_CUDA_TRY(cudaEventRecord(ctx->fork_ev, main_s));
   for (int i = 0; i < 2; ++i) NIDO_CUDA_TRY(cudaStreamWaitEvent(ctx->aux[i], ctx->fork_ev, 0));
   const int nb = g->nbatches;

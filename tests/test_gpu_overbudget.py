@@ -12,7 +12,7 @@ pytestmark = pytest.mark.gpu
 
 @pytest.fixture(scope="module")
 def big(nido_lib):
-    return nido_lib.gen_rmat(1 << 20, 16 << 20, wmode=nido_lib.W_INT8, seed=51)
+    return nido_lib.gen_rmat(1 << 20, 24 << 20, wmode=nido_lib.W_INT8, seed=51)
 
 
 def test_overbudget_graph_streams_edges_and_matches(nido_lib, ctx, big):

@@ -83,3 +83,18 @@ def test_cluster_hub_tier_vs_oracle(nido_lib, ctx, orc, ctax):
     assert st.phases == st_o.phases and st.total_loops == st_o.total_loops
     assert np.array_equal(np.array(st.q_phase[: st.phases]), np.array(st_o.q_phase[: st_o.phases]))
     assert np.array_equal(cl, want)
+
+
+@pytest.mark.parametrize("tie", [0, 1])
+def test_staged_edges_same_result(nido_lib, ctx, rmat16, tie):
+    """The CTA-S and CTA-M tiers with their edges staged in shared memory by
+    bulk copies give the same partitions as the unstaged default."""
+    with nido_lib.Graph(ctx, rmat16, 2) as g:
+        want, st0 = g.run(tie=tie)
+        c = g.tier_config()
+        assert c.staged_edges == 0
+        c.staged_edges = 1
+        g.set_tier_config(c)
+        assert g.tier_config().staged_edges == 1
+        got, st = g.run(tie=tie)
+    assert np.array_equal(got, want) and st.final_q == st0.final_q
