@@ -542,6 +542,27 @@ __device__ __forceinline__ void scan_entries(const MoveArgs& p, double m, const 
   }
 }
 
+// Warp argmax of (gain, smallest id) under the smallest-id rule (tk is the
+// community id, kNoKey without a candidate) with three 32-bit warp
+// reductions instead of a shuffle tree: the gain as an order-preserving
+// 64-bit key (+0 for -0, which compares equal to it), then the smallest id
+// among the lanes holding the largest gain.  The result is group_best<32>'s.
+// Every lane of the warp must call it; all end with the result.
+__device__ __forceinline__ void warp_best_id(double& g, unsigned long long& tk, int& cand) {
+  const long long b = __double_as_longlong(g + 0.0);
+  const unsigned long long key = b < 0 ? ~(unsigned long long)b : ((unsigned long long)b | 0x8000000000000000ull);
+  const unsigned hi = (unsigned)(key >> 32), lo = (unsigned)key;
+  const unsigned mh = __reduce_max_sync(NIDO_FULL_MASK, hi);
+  const unsigned ml = __reduce_max_sync(NIDO_FULL_MASK, hi == mh ? lo : 0u);
+  const bool top = hi == mh && lo == ml;
+  const unsigned id = tk == kNoKey ? 0xFFFFFFFFu : (unsigned)tk;
+  const unsigned mid = __reduce_min_sync(NIDO_FULL_MASK, top ? id : 0xFFFFFFFFu);
+  const int src = __ffs(__ballot_sync(NIDO_FULL_MASK, top && id == mid)) - 1;
+  g = __shfl_sync(NIDO_FULL_MASK, g, src);
+  tk = __shfl_sync(NIDO_FULL_MASK, tk, src);
+  cand = __shfl_sync(NIDO_FULL_MASK, cand, src);
+}
+
 // The reference's tie rule over the same entries: among communities whose
 // gain equals gm, the smallest (bitrev3(rank mod 8), rank), where rank counts
 // the vertex's neighbour communities with a smaller id.
@@ -620,8 +641,10 @@ __global__ void __launch_bounds__(256) k_move_warp(const int32_t* __restrict__ l
     if (p.tie == NIDO_TIE_NIDO) {
       const double gm = group_max<32>(g);
       nido_tie_entries(p, m, t, nu, lane, 32, own, ki, gm, false, g, tk, cand);
+      group_best<32>(g, tk, cand);
+    } else {
+      warp_best_id(g, tk, cand);
     }
-    group_best<32>(g, tk, cand);
     if (lane == 0) decide(p, m, v, own, ki, aown, eown, g, cand);
     __syncwarp();
     for (int i = lane; i < nu; i += 32) {
@@ -695,8 +718,12 @@ __device__ __forceinline__ void block_evaluate(const MoveArgs& p, double m, cons
   // one reduction for the best entry and e_own (e_own is nonzero in one
   // thread at most, so its sum is exact in any order)
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
-  if (p.tie != NIDO_TIE_NIDO) eown = group_sum<32>(eown);
-  group_best<32>(g, tk, cand);
+  if (p.tie != NIDO_TIE_NIDO) {
+    eown = group_sum<32>(eown);
+    warp_best_id(g, tk, cand);
+  } else {
+    group_best<32>(g, tk, cand);
+  }
   __shared__ double se[32];
   if (lane == 0) { sg[wid] = g; stk[wid] = tk; sc[wid] = cand; se[wid] = eown; }
   __syncthreads();
@@ -705,7 +732,8 @@ __device__ __forceinline__ void block_evaluate(const MoveArgs& p, double m, cons
     tk = lane < nw ? stk[lane] : kNoKey;
     cand = lane < nw ? sc[lane] : -1;
     double e2 = lane < nw ? se[lane] : 0.;
-    group_best<32>(g, tk, cand);
+    if (p.tie != NIDO_TIE_NIDO) warp_best_id(g, tk, cand);
+    else group_best<32>(g, tk, cand);
     e2 = group_sum<32>(e2);
     if (lane == 0) decide(p, m, v, own, ki, aown, p.tie == NIDO_TIE_NIDO ? eown : e2, g, cand);
   }
