@@ -251,7 +251,7 @@ __device__ __forceinline__ int table_add_packed(const Table& t, int c, int w, bo
       atomicAdd(reinterpret_cast<int*>(&t.slots[h]), w);
       return (int)h;
     }
-    h = (h + 1) & t.mask;
+    h = (h + probe + 1) & t.mask;  // triangular steps: every slot once
   }
   atomicAdd(err, 1ull);
   return -1;
@@ -294,7 +294,7 @@ __device__ __forceinline__ int table_add(const Table& t, int c, double e, bool& 
       }
       return (int)h;
     }
-    h = (h + 1) & t.mask;
+    h = (h + probe + 1) & t.mask;  // triangular steps: every slot once
   }
   atomicAdd(err, 1ull);
   return -1;
