@@ -482,7 +482,11 @@ int batch_modularity(nido_batch_s* B, const Lists& ql, double* out) {
 
 // (re)build the degree-tier lists and the modularity layout over the graphs
 // in ids, which become the listed (gactive) graphs
-int batch_list(nido_batch_s* B, const std::vector<int32_t>& ids, const std::vector<int64_t>& base, Lists* ql) {
+// The graphs ids are listed: modularity groups, active flags and the tier
+// lists of their vertices.  relist: ids is a subset of the graphs listed so
+// far in this phase, so the tier lists are compacted instead of rebuilt.
+int batch_list(nido_batch_s* B, const std::vector<int32_t>& ids, const std::vector<int64_t>& base, Lists* ql,
+               bool relist = false) {
   nido_graph_s* g = B->g;
   cudaStream_t s = g->ctx->stream;
   NIDO_CUDA_TRY(cudaMemsetAsync(B->gactive, 0, sizeof(int32_t) * B->ng, s));
@@ -493,6 +497,7 @@ int batch_list(nido_batch_s* B, const std::vector<int32_t>& ids, const std::vect
     NIDO_LAUNCH_CHECK();
   }
   if (ql->off.back() > B->cap_modv) return nido_set_error(NIDO_E_NOMEM, "modularity buffer too small");
+  if (relist && g->bins_valid) return compact_batches(g);
   g->bins_valid = false;
   return build_batches(g);
 }
@@ -904,7 +909,7 @@ extern "C" int nido_batch_run(nido_batch B, const nido_params* p, int64_t* out_c
         listed_v = listed_e = 0;
         for (int32_t i : act)
           if (flags[i]) { it.push_back(i); listed_v += base[i + 1] - base[i]; listed_e += edges[i]; }
-        NIDO_TRY(batch_list(B, it, base, &ql));
+        NIDO_TRY(batch_list(B, it, base, &ql, true));
         lap(2);
       }
     }

@@ -274,6 +274,7 @@ cudaError_t pinned_buffer(nido_ctx_s* ctx, size_t bytes, void** p);
 int device_alloc(nido_ctx_s* ctx, void** p, size_t bytes);
 void device_free(nido_ctx_s* ctx, void* p, size_t bytes);
 int build_batches(nido_graph_s* g);                     // cuts (host) + tier lists
+int compact_batches(nido_graph_s* g);                   // many graphs: drop stopped graphs' vertices
 // vertices in the tier lists (vertices with at least one edge)
 inline int64_t listed_vertices(const nido_graph_s* g) {
   return g->tier_off.empty() ? g->nv : g->tier_off[(size_t)kNumTiers * g->nbatches];

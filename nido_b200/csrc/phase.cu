@@ -450,6 +450,30 @@ __global__ void k_tier_keys(const int64_t* __restrict__ off, int64_t nv, const i
   if (lane == 0 && md) atomicMax(maxdeg, md);
 }
 
+// Keep flags of the listed vertices whose graph still iterates (pos[i] = 1)
+// and, after the scan, their scatter in list order.
+__global__ void k_keep_flags(const int32_t* __restrict__ perm, int64_t n, const int32_t* __restrict__ gid,
+                             const int32_t* __restrict__ gactive, int64_t* __restrict__ pos) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    pos[i] = gactive[gid[perm[i]]] != 0 ? 1 : 0;
+}
+
+__global__ void k_scatter_kept(const int32_t* __restrict__ perm, int64_t n, const int32_t* __restrict__ gid,
+                               const int32_t* __restrict__ gactive, const int64_t* __restrict__ pos,
+                               int32_t* __restrict__ out) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t v = perm[i];
+    if (gactive[gid[v]] != 0) out[pos[i]] = v;
+  }
+}
+
+// new segment offsets: the scanned positions at the old segment starts
+__global__ void k_gather_offsets(const int64_t* __restrict__ old_off, int64_t nseg, const int64_t* __restrict__ pos,
+                                 int64_t* __restrict__ new_off) {
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k <= nseg; k += (int64_t)gridDim.x * blockDim.x)
+    new_off[k] = pos[old_off[k]];
+}
+
 }  // namespace
 
 // k_v of the current phase; its weight flags (dcount[2..3]) are read back by
@@ -732,6 +756,47 @@ int build_batches(nido_graph_s* g) {
   }
   g->max_degree = (int64_t)md;
   g->bins_valid = true;
+  ++g->plan_epoch;
+  return plan_hubs(g);
+}
+
+// Many-graph mode: drop the vertices of graphs that stopped iterating
+// (gactive 0) from the current tier lists.  A stable compaction of the
+// listed vertices (flags, scan, scatter) keeps every (tier, batch) list in its
+// order, so the lists equal what build_batches would list for the same
+// graphs, at the cost of one pass over the listed vertices instead of a key
+// pass over every vertex and a sort.  The largest degree stays the old one
+// (an upper bound).
+int compact_batches(nido_graph_s* g) {
+  if (!g->gid || !g->bins_valid || g->color_mode) {
+    g->bins_valid = false;
+    return build_batches(g);
+  }
+  cudaStream_t s = g->ctx->stream;
+  const int64_t nseg = (int64_t)kNumTiers * g->nbatches;
+  const int64_t n = g->tier_off[(size_t)nseg];
+  if (n == 0) return NIDO_OK;
+  Arena ar(g->scratch, g->scratch_bytes);
+  int64_t* pos = ar.take<int64_t>(n + 1);
+  int32_t* out = ar.take<int32_t>(n);
+  int64_t* segs = ar.take<int64_t>(2 * (nseg + 1));
+  int64_t* rtemp = ar.take<int64_t>(scan_temp_elems(n));
+  if (!pos || !out || !segs || !rtemp) return nido_set_error(NIDO_E_NOMEM, "scratch arena too small (list compaction)");
+  int32_t* perm = reinterpret_cast<int32_t*>(g->perm);
+  k_keep_flags<<<grid_for(n, kThreads), kThreads, 0, s>>>(perm, n, g->gid, g->gactive, pos);
+  NIDO_LAUNCH_CHECK();
+  NIDO_TRY(scan_exclusive_i64(pos, pos, n, rtemp, s));
+  k_scatter_kept<<<grid_for(n, kThreads), kThreads, 0, s>>>(perm, n, g->gid, g->gactive, pos, out);
+  NIDO_LAUNCH_CHECK();
+  NIDO_CUDA_TRY(cudaMemcpyAsync(segs, g->tier_off.data(), sizeof(int64_t) * (nseg + 1), cudaMemcpyHostToDevice, s));
+  k_gather_offsets<<<grid_for(nseg + 1, 128), 128, 0, s>>>(segs, nseg, pos, segs + nseg + 1);
+  NIDO_LAUNCH_CHECK();
+  std::vector<int64_t> off(nseg + 1);
+  NIDO_CUDA_TRY(cudaMemcpyAsync(off.data(), segs + nseg + 1, sizeof(int64_t) * (nseg + 1), cudaMemcpyDeviceToHost, s));
+  NIDO_CUDA_TRY(cudaStreamSynchronize(s));
+  if (off[nseg] > 0)
+    NIDO_CUDA_TRY(cudaMemcpyAsync(perm, out, sizeof(int32_t) * off[nseg], cudaMemcpyDeviceToDevice, s));
+  g->tier_off = off;
   ++g->plan_epoch;
   return plan_hubs(g);
 }
