@@ -122,6 +122,27 @@ __device__ __forceinline__ double group_sum(double x) {
   return x;
 }
 
+// Warp argmax of (gain, smallest id) under the smallest-id rule (tk is the
+// community id, kNoKey without a candidate) with three 32-bit warp
+// reductions instead of a shuffle tree: the gain as an order-preserving
+// 64-bit key (+0 for -0, which compares equal to it), then the smallest id
+// among the lanes holding the largest gain.  The result is group_best<32>'s.
+// Every lane of the warp must call it; all end with the result.
+__device__ __forceinline__ void warp_best_id(double& g, unsigned long long& tk, int& cand) {
+  const long long b = __double_as_longlong(g + 0.0);
+  const unsigned long long key = b < 0 ? ~(unsigned long long)b : ((unsigned long long)b | 0x8000000000000000ull);
+  const unsigned hi = (unsigned)(key >> 32), lo = (unsigned)key;
+  const unsigned mh = __reduce_max_sync(NIDO_FULL_MASK, hi);
+  const unsigned ml = __reduce_max_sync(NIDO_FULL_MASK, hi == mh ? lo : 0u);
+  const bool top = hi == mh && lo == ml;
+  const unsigned id = tk == kNoKey ? 0xFFFFFFFFu : (unsigned)tk;
+  const unsigned mid = __reduce_min_sync(NIDO_FULL_MASK, top ? id : 0xFFFFFFFFu);
+  const int src = __ffs(__ballot_sync(NIDO_FULL_MASK, top && id == mid)) - 1;
+  g = __shfl_sync(NIDO_FULL_MASK, g, src);
+  tk = __shfl_sync(NIDO_FULL_MASK, tk, src);
+  cand = __shfl_sync(NIDO_FULL_MASK, cand, src);
+}
+
 // ---- degree <= 32: registers ---------------------------------------------------
 template <int G, bool kMulti>
 __global__ void __launch_bounds__(256) k_move_group(const int32_t* __restrict__ list, int64_t n,
@@ -182,7 +203,8 @@ __global__ void __launch_bounds__(256) k_move_group(const int32_t* __restrict__ 
       tk = (cand >= 0 && g == gm) ? nido_key(rank) : kNoKey;
       if (tk == kNoKey) { g = -NIDO_MAX_FLOAT; cand = -1; }
     }
-    group_best<G>(g, tk, cand);
+    if (G == 32 && p.tie != NIDO_TIE_NIDO) warp_best_id(g, tk, cand);
+    else group_best<G>(g, tk, cand);
     if (gl == 0 && vok) {
       const double self = self_of(eown, ki, aown, m);
       const double tot = __dsub_rn(g, self);
@@ -542,26 +564,6 @@ __device__ __forceinline__ void scan_entries(const MoveArgs& p, double m, const 
   }
 }
 
-// Warp argmax of (gain, smallest id) under the smallest-id rule (tk is the
-// community id, kNoKey without a candidate) with three 32-bit warp
-// reductions instead of a shuffle tree: the gain as an order-preserving
-// 64-bit key (+0 for -0, which compares equal to it), then the smallest id
-// among the lanes holding the largest gain.  The result is group_best<32>'s.
-// Every lane of the warp must call it; all end with the result.
-__device__ __forceinline__ void warp_best_id(double& g, unsigned long long& tk, int& cand) {
-  const long long b = __double_as_longlong(g + 0.0);
-  const unsigned long long key = b < 0 ? ~(unsigned long long)b : ((unsigned long long)b | 0x8000000000000000ull);
-  const unsigned hi = (unsigned)(key >> 32), lo = (unsigned)key;
-  const unsigned mh = __reduce_max_sync(NIDO_FULL_MASK, hi);
-  const unsigned ml = __reduce_max_sync(NIDO_FULL_MASK, hi == mh ? lo : 0u);
-  const bool top = hi == mh && lo == ml;
-  const unsigned id = tk == kNoKey ? 0xFFFFFFFFu : (unsigned)tk;
-  const unsigned mid = __reduce_min_sync(NIDO_FULL_MASK, top ? id : 0xFFFFFFFFu);
-  const int src = __ffs(__ballot_sync(NIDO_FULL_MASK, top && id == mid)) - 1;
-  g = __shfl_sync(NIDO_FULL_MASK, g, src);
-  tk = __shfl_sync(NIDO_FULL_MASK, tk, src);
-  cand = __shfl_sync(NIDO_FULL_MASK, cand, src);
-}
 
 // The reference's tie rule over the same entries: among communities whose
 // gain equals gm, the smallest (bitrev3(rank mod 8), rank), where rank counts
