@@ -145,7 +145,7 @@ __device__ __forceinline__ void warp_best_id(double& g, unsigned long long& tk, 
 
 // ---- degree <= 32: registers ---------------------------------------------------
 template <int G, bool kMulti>
-__global__ void __launch_bounds__(256) k_move_group(const int32_t* __restrict__ list, int64_t n,
+__global__ void __launch_bounds__(256, 6) k_move_group(const int32_t* __restrict__ list, int64_t n,
                                                     MoveArgs p) {
   constexpr int VPW = 32 / G;
   const int lane = threadIdx.x & 31, gl = lane & (G - 1), gid = lane / G;
@@ -603,7 +603,7 @@ __device__ __forceinline__ void decide(const MoveArgs& p, double m, int v, int o
 constexpr size_t table_bytes(int slots, bool ints) { return (size_t)slots * (ints ? 12 : 16); }
 
 template <int kCap, bool kMulti, bool kInts>
-__global__ void __launch_bounds__(256) k_move_warp(const int32_t* __restrict__ list, int64_t n, MoveArgs p) {
+__global__ void __launch_bounds__(256, 4) k_move_warp(const int32_t* __restrict__ list, int64_t n, MoveArgs p) {
   extern __shared__ double smem[];
   __shared__ int nocc_s[8];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
