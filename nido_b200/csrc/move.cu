@@ -144,6 +144,8 @@ __device__ __forceinline__ void warp_best_id(double& g, unsigned long long& tk, 
 }
 
 // ---- degree <= 32: registers ---------------------------------------------------
+// Six 256-thread blocks an SM (at most 40 registers a thread): the tier waits
+// on its gathers, and more resident warps hide more of them.
 template <int G, bool kMulti>
 __global__ void __launch_bounds__(256, 6) k_move_group(const int32_t* __restrict__ list, int64_t n,
                                                     MoveArgs p) {
@@ -602,8 +604,9 @@ __device__ __forceinline__ void decide(const MoveArgs& p, double m, int v, int o
 // slots and the occupied list (12 bytes a slot).
 constexpr size_t table_bytes(int slots, bool ints) { return (size_t)slots * (ints ? 12 : 16); }
 
+// Five 256-thread blocks an SM (at most 48 registers a thread; a few spill).
 template <int kCap, bool kMulti, bool kInts>
-__global__ void __launch_bounds__(256, 4) k_move_warp(const int32_t* __restrict__ list, int64_t n, MoveArgs p) {
+__global__ void __launch_bounds__(256, 5) k_move_warp(const int32_t* __restrict__ list, int64_t n, MoveArgs p) {
   extern __shared__ double smem[];
   __shared__ int nocc_s[8];
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -818,8 +821,10 @@ __device__ __forceinline__ void stage_edges(const MoveArgs& p, int64_t s, int64_
 // kStageDeg > 0: the tier's vertices (degree <= kStageDeg) have their edges
 // staged in shared memory behind the table (see stage_edges), one vertex
 // ahead: the copy of vertex i+1 runs while vertex i is evaluated.
+// Resident CTAs an SM: ten of 128 threads or five of 256 (at most 48 registers
+// a thread), else the 64-register fill of 1024 threads.
 template <int kThreads, int kCap, bool kMulti, bool kInts, bool kOcc = true, int kStageDeg = 0>
-__global__ void __launch_bounds__(kThreads) k_move_cta(const int32_t* __restrict__ list, int64_t n, MoveArgs p) {
+__global__ void __launch_bounds__(kThreads, kThreads == 128 ? 10 : (kThreads == 256 ? 5 : 1024 / kThreads)) k_move_cta(const int32_t* __restrict__ list, int64_t n, MoveArgs p) {
   constexpr bool kList = kOcc || kInts;
   constexpr bool kStaged = kStageDeg > 0;
   extern __shared__ __align__(128) double smem[];
