@@ -68,12 +68,12 @@ typedef struct {
   int32_t tau_phase_set;
   int32_t host_loop; /* who drives each phase's iteration loop.  2: the device,
                         one CUDA graph per phase with a conditional while node,
-                        read back once per phase; 1: the host, one Q readback per
-                        iteration, as the reference does; 0 (default): the device
-                        for phases of at most NIDO_DEVICE_LOOP_MAX_EDGES edges
-                        (short iterations, where host round trips and launches
-                        dominate), the host above (long iterations, where the
-                        graph's build costs more than the round trips it saves) */
+                        read back once per phase; 1 or 0 (default): the host,
+                        one Q readback per iteration, as the reference does.
+                        Measured on B200 (driver 580) the host loop is the
+                        faster: building the loop graphs costs more than the
+                        round trips they save, for small and large graphs and
+                        for graph sets alike */
   int32_t color_batches; /* 1: conflict-free batches instead of the -b cuts:
                         every phase colours its graph (Jones-Plassmann-Luby,
                         seed 1) and sweeps the colour classes in colour order,
@@ -81,10 +81,6 @@ typedef struct {
                         same batch (one-graph runs only) */
   int32_t reserved;  /* must be 0 */
 } nido_params;
-
-/* params.host_loop = 0: phases (for graph sets: listed edges of a sweep) up to
- * this many edges run their iteration loop on the device */
-#define NIDO_DEVICE_LOOP_MAX_EDGES (16LL << 20)
 
 /* Per-run statistics (the reference prints these, louvain_gpu.cpp:43-131). */
 typedef struct {

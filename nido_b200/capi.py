@@ -435,9 +435,9 @@ class Graph:
             verbose: bool = False, tune: bool = False, host_loop: bool = False, tau_phase: float | None = None,
             color_batches: bool = False, device_loop: bool = False, out: np.ndarray | None = None):
         """LouvainGPU::run; returns (clustering of the input vertices, RunStats).
-        host_loop / device_loop: force who drives each phase's iterations (the
-        host, one readback per iteration, or the device-resident loop graph);
-        neither: the library picks by the phase's size.  color_batches: every
+        host_loop / device_loop: who drives each phase's iterations (the host,
+        one readback per iteration, the default; or the device-resident loop
+        graph, one readback per phase).  color_batches: every
         phase's colour classes are its batches (conflict-free) instead of the
         -b cuts.  out: an int64 array of nv entries to write the clustering
         into (page-locked with host_register, the download runs at full link
@@ -460,7 +460,7 @@ def _out_array(out, n: int) -> np.ndarray:
 
 
 def _loop_mode(host_loop: bool, device_loop: bool) -> int:
-    """nido_params.host_loop: 1 host, 2 device, 0 chosen by the library."""
+    """nido_params.host_loop: 1 host, 2 device, 0 the library's default (host)."""
     if host_loop and device_loop:
         raise ValueError("host_loop and device_loop are exclusive")
     return 1 if host_loop else (2 if device_loop else 0)

@@ -860,8 +860,7 @@ extern "C" int nido_batch_run(nido_batch B, const nido_params* p, int64_t* out_c
     };
     while (n_iter > 0) {
       bool ran_on_device = false;
-      const bool want_device =
-          p->host_loop == 2 || (p->host_loop == 0 && listed_e <= NIDO_DEVICE_LOOP_MAX_EDGES);
+      const bool want_device = p->host_loop == 2;
       if (want_device && g->ctx->device_loop) {
         bool unsupported = false;
         NIDO_TRY(device_sweeps(&unsupported));

@@ -1014,7 +1014,7 @@ extern "C" int nido_run(nido_graph g, const nido_params* p, int64_t* out_comm, n
     NIDO_TRY(nido::launch_singleton(g));
     double Q = 0., Q_old = 0.;
     int64_t loops = 0;
-    const bool want_device = p->host_loop == 2 || (p->host_loop == 0 && g->ne <= NIDO_DEVICE_LOOP_MAX_EDGES);
+    const bool want_device = p->host_loop == 2;
     bool host_loop = !want_device || !g->ctx->device_loop || (p->verbose && p->max_iter > nido::kLoopLogCap);
     if (!host_loop) {
       // the phase's iteration loop as one device-resident CUDA graph
