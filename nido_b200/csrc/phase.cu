@@ -227,19 +227,27 @@ __device__ __forceinline__ double own_weight(const int32_t* __restrict__ adj, co
   double x = 0.;
   for (int64_t j = j0; j < e; j += 4 * (int64_t)step) {
     int u[4];
-    double wt[4];
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
       const int64_t jk = j + k * (int64_t)step;
       u[k] = jk < e ? adj[jk] : -1;
-      wt[k] = jk < e ? w[jk] : 0.;
     }
     int c[4];
 #pragma unroll
     for (int k = 0; k < 4; ++k) c[k] = u[k] >= 0 ? comm[u[k]] : 0;
+    // only in-community edges load their weight: a warp's 32-byte weight
+    // sectors with no such edge are never fetched (most of them while the
+    // communities are small); the sum and its order are unchanged
+    bool in[4];
+    double wt[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      in[k] = u[k] >= 0 && c[k] == own;
+      wt[k] = in[k] ? w[j + k * (int64_t)step] : 0.;
+    }
 #pragma unroll
     for (int k = 0; k < 4; ++k)
-      if (u[k] >= 0 && c[k] == own) x += wt[k];
+      if (in[k]) x += wt[k];
   }
   return x;
 }
