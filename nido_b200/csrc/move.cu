@@ -150,6 +150,7 @@ template <int G, bool kMulti>
 __global__ void __launch_bounds__(256, 6) k_move_group(const int32_t* __restrict__ list, int64_t n,
                                                     MoveArgs p) {
   constexpr int VPW = 32 / G;
+  __shared__ int fold[256];  // integer phases: per-lane group sums
   const int lane = threadIdx.x & 31, gl = lane & (G - 1), gid = lane / G;
   const int64_t warp = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
@@ -178,8 +179,21 @@ __global__ void __launch_bounds__(256, 6) k_move_group(const int32_t* __restrict
     }
     const unsigned long long mkey = ((unsigned long long)(unsigned)gid << 32) | (unsigned)c;
     const unsigned peers = __match_any_sync(NIDO_FULL_MASK, mkey);
-    const bool lead = ok && lane == __ffs(peers) - 1;
-    const double e = fold_peers(peers, ok, wt);
+    const int leader = __ffs(peers) - 1;
+    const bool lead = ok && lane == leader;
+    double e;
+    if (p.ints) {
+      // integer weights: every lane adds its weight into its group leader's
+      // shared-memory slot (int32 adds, exact in any order; equal addresses
+      // are serialised by the atomic unit, not by instructions)
+      fold[threadIdx.x] = 0;
+      __syncwarp();
+      if (ok) atomicAdd(&fold[(threadIdx.x & ~31) + leader], __double2int_rn(wt));
+      __syncwarp();
+      e = (double)fold[threadIdx.x];
+    } else {
+      e = fold_peers(peers, ok, wt);
+    }
     double g = -NIDO_MAX_FLOAT, eown = 0.;
     unsigned long long tk = kNoKey;
     int cand = -1;
@@ -349,10 +363,10 @@ __device__ __forceinline__ double ld_stream(const double* q) {
   return v;
 }
 
+// smallest power of two >= max(64, 2d) (shared-memory tiers: d <= 2^30)
 __device__ __forceinline__ unsigned next_pow2_cap(int64_t d) {
-  unsigned c = 64;
-  while ((int64_t)c < 2 * d) c <<= 1;
-  return c;
+  const unsigned x = (unsigned)max((int64_t)64, 2 * min(d, (int64_t)1 << 30));
+  return 1u << (32 - __clz(x - 1));
 }
 
 // Accumulate the edges [first, eend) of vertex v: the warp takes 32-edge
