@@ -121,3 +121,20 @@ def test_batch_rejects_crossing_edges(nido_lib, ctx):
         nido_lib.Batch(ctx, packed=(vbase, u))
     with pytest.raises(nido_lib.NidoError):
         nido_lib.Batch(ctx, packed=(np.array([0, 4, 3], np.int64), nido_lib.pack_graphs([a, a])[1]))
+
+
+def test_stopped_graphs_leave_the_lists_by_compaction(nido_lib, ctx):
+    """Many small planted graphs that converge in a few sweeps beside one
+    R-MAT graph that iterates longer: once the stopped graphs hold a quarter of
+    the listed vertices their vertices leave the tier lists (a stable
+    compaction, timed in host_ms[2]), and every graph still equals its run
+    alone."""
+    graphs = [nido_lib.gen_planted(32, 64, 12.0, 0.9, nido_lib.W_INT8, 600 + i) for i in range(24)]
+    graphs.append(nido_lib.gen_rmat(1 << 13, 12 << 13, wmode=nido_lib.W_INT8, seed=650))
+    want = plain_runs(nido_lib, ctx, graphs, 2, 0)
+    with nido_lib.Batch(ctx, graphs, 2) as b:
+        parts, q, ph, lo, st = b.run()
+    assert st.host_ms[2] > 0  # the lists were compacted at least once
+    for i, (cl, fq, phases, loops) in enumerate(want):
+        assert np.array_equal(parts[i], cl), f"graph {i}"
+        assert same_q(q[i], fq) and ph[i] == phases and lo[i] == loops, f"graph {i}"

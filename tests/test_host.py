@@ -238,3 +238,17 @@ def test_ctypes_structs_match_header(nido_lib, cname, pyname):
         if n:
             assert ctype._length_ == n, name
         assert C.sizeof(base) == C.sizeof(getattr(C, _CTYPES[htype])), name
+
+
+def test_result_buffer_validation():
+    """run(out=...) takes a contiguous int64 array of the right length (a
+    page-locked one downloads at full link speed) and refuses anything else."""
+    import numpy as np
+
+    from nido_b200 import capi
+    good = np.empty(10, np.int64)
+    assert capi._out_array(good, 10) is good
+    assert capi._out_array(None, 3).shape == (3,)
+    for bad in (np.empty(10, np.int32), np.empty(9, np.int64), np.empty((2, 5), np.int64), np.empty(20, np.int64)[::2]):
+        with pytest.raises(ValueError):
+            capi._out_array(bad, 10)
