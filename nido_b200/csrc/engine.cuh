@@ -85,8 +85,8 @@ struct nido_ctx_s {
   // settings are left alone.
   bool async_alloc = false;
   cudaMemPool_t pool = nullptr;
-  // phase loops run on the device (loop.cu) until the driver turns out to
-  // lack conditional graph nodes
+  // device-resident phase loops (loop.cu, params.host_loop = 2) are possible
+  // until the CUDA driver turns out to lack conditional graph nodes
   bool device_loop = true;
   // otherwise blocks come from cudaMalloc and are kept for reuse when freed
   // (raw_alloc / raw_free): free blocks by size, the size of every block in
