@@ -130,6 +130,13 @@ int nido_ctx_stream(nido_ctx ctx, void** stream);
  * graphs).  This returns the free ones to the driver; released_bytes (may be
  * null) receives their size.  Destroying the context does the same. */
 int nido_ctx_trim(nido_ctx ctx, size_t* released_bytes);
+/* Self-check of the bounded device waits (no reference counterpart): a kernel
+ * waits on a barrier nothing arrives at, with the wait the move kernels use
+ * (an attempt count and about one second of %globaltimer); it must give up.
+ * *gave_up = 1 when it did, *waited_ms the time it waited; the context stays
+ * usable.  Kernels whose bounded waits give up count it in the run's error
+ * counter, which nido_run / nido_batch_run report as a failure. */
+int nido_check_bounded_wait(nido_ctx ctx, int32_t* gave_up, int32_t* waited_ms);
 
 /* ---- graphs ----------------------------------------------------------------- */
 /* Upload a CSR and compute k_v and m.  Replaces the GraphGPU constructor

@@ -97,6 +97,7 @@ def lib() -> C.CDLL:
             "nido_graph_batches": (C.c_int, [vp, _i64p]),
             "nido_graph_vertex_weights": (C.c_int, [vp, _f64p, _f64p]),
             "nido_graph_reset": (C.c_int, [vp]),
+            "nido_check_bounded_wait": (C.c_int, [vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32)]),
             "nido_host_register": (C.c_int, [vp, C.c_size_t]),
             "nido_host_unregister": (C.c_int, [vp]),
             "nido_singleton_partition": (C.c_int, [vp]),
@@ -254,6 +255,13 @@ class Context:
         s = C.c_void_p()
         _check(lib().nido_ctx_stream(self.h, C.byref(s)))
         return s.value or 0
+
+    def check_bounded_wait(self):
+        """nido_check_bounded_wait: (gave_up, waited_ms) of a device wait on a
+        barrier nothing arrives at."""
+        gave_up, ms = C.c_int32(), C.c_int32()
+        _check(lib().nido_check_bounded_wait(self.h, C.byref(gave_up), C.byref(ms)))
+        return bool(gave_up.value), int(ms.value)
 
     def trim(self) -> int:
         """Return the device blocks cached from freed graphs to the driver;

@@ -978,7 +978,9 @@ extern "C" int nido_batch_run(nido_batch B, const nido_params* p, int64_t* out_c
   int64_t nerr = 0;
   NIDO_CUDA_TRY(cudaMemcpyAsync(&nerr, g->dcount + 1, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
   NIDO_CUDA_TRY(cudaStreamSynchronize(s));
-  if (nerr) return nido_set_error(NIDO_E_CUDA, "hash table overflow in %lld probes", (long long)nerr);
+  if (nerr)
+    return nido_set_error(NIDO_E_CUDA, "a move kernel gave up %lld times (hash-table probe limit or bounded wait)",
+                          (long long)nerr);
   st.total_ms = tot;
   st.phases = phase;
   if (out_comm) NIDO_CUDA_TRY(cudaMemcpyAsync(out_comm, B->outc, sizeof(int64_t) * g->nv0, cudaMemcpyDeviceToHost, s));

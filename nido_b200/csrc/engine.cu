@@ -273,6 +273,12 @@ extern "C" int nido_ctx_trim(nido_ctx ctx, size_t* released_bytes) {
   return NIDO_OK;
 }
 
+extern "C" int nido_check_bounded_wait(nido_ctx ctx, int32_t* gave_up, int32_t* waited_ms) {
+  if (!ctx) return nido_set_error(NIDO_E_INVALID, "null context");
+  NIDO_CUDA_TRY(cudaSetDevice(ctx->device));
+  return nido::check_bounded_wait(ctx, gave_up, waited_ms);
+}
+
 extern "C" int nido_ctx_sync(nido_ctx ctx) {
   if (!ctx) return nido_set_error(NIDO_E_INVALID, "null context");
   NIDO_CUDA_TRY(cudaStreamSynchronize(ctx->stream));
@@ -1119,7 +1125,9 @@ extern "C" int nido_run(nido_graph g, const nido_params* p, int64_t* out_comm, n
   int64_t nerr = 0;
   NIDO_CUDA_TRY(cudaMemcpyAsync(&nerr, g->dcount + 1, sizeof(int64_t), cudaMemcpyDeviceToHost, s));
   NIDO_CUDA_TRY(cudaStreamSynchronize(s));
-  if (nerr) return nido_set_error(NIDO_E_CUDA, "hash table overflow in %lld probes", (long long)nerr);
+  if (nerr)
+    return nido_set_error(NIDO_E_CUDA, "a move kernel gave up %lld times (hash-table probe limit or bounded wait)",
+                          (long long)nerr);
   lap(1);
   if (out_comm) NIDO_TRY(nido_get_clustering(g, out_comm));
   lap(5);

@@ -288,6 +288,7 @@ int color_current_graph(nido_graph_s* g, uint64_t seed, int32_t* colors, int64_t
 // ev_start / ev_end (may be null) are recorded around the tier kernels
 int launch_move(nido_graph_s* g, int batch, int tie, cudaEvent_t ev_start, cudaEvent_t ev_end);
 int launch_move_tiers(nido_graph_s* g, int batch, int tie);  // enqueue only (capturable)
+int check_bounded_wait(nido_ctx_s* ctx, int32_t* gave_up, int32_t* waited_ms);  // move.cu
 int plan_hubs(nido_graph_s* g);          // per phase, after the tier lists
 int move_init_attributes();              // once per device
 // times `sweeps` move sweeps (no commit) for candidate tier configurations

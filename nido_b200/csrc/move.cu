@@ -801,13 +801,38 @@ __device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned 
   return ok != 0;
 }
 
-// bounded wait: gives up (false) after kMbarTries attempts instead of spinning
-// forever; the caller counts the failure in p.err
+__device__ __forceinline__ unsigned long long gtimer_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// bounded wait: gives up (false) after kMbarTries attempts or about a second,
+// whichever comes first, instead of spinning forever; the caller counts the
+// failure in p.err
 constexpr int kMbarTries = 1 << 20;
+constexpr unsigned long long kMbarWaitNs = 1000000000ull;
 __device__ __forceinline__ bool mbar_wait(unsigned long long* bar, unsigned parity) {
-  for (int i = 0; i < kMbarTries; ++i)
+  const unsigned long long t0 = gtimer_ns();
+  for (int i = 0; i < kMbarTries; ++i) {
     if (mbar_try_wait(bar, parity)) return true;
+    if ((i & 255) == 255 && gtimer_ns() - t0 > kMbarWaitNs) return false;
+  }
   return false;
+}
+
+// Self-check of the bounded waits: one thread waits on an mbarrier that
+// expects an arrival nobody makes.  The wait must give up and the kernel
+// report it (out[0] = 1, out[1] = milliseconds waited), leaving the context
+// usable.
+__global__ void k_check_bounded_wait(int32_t* out) {
+  __shared__ unsigned long long bar;
+  if (threadIdx.x != 0) return;
+  mbar_init(&bar, 1);
+  const unsigned long long t0 = gtimer_ns();
+  const bool done = mbar_wait(&bar, 0);
+  out[0] = done ? 0 : 1;
+  out[1] = (int32_t)min((gtimer_ns() - t0) / 1000000ull, 1ull << 30);
 }
 
 __device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes, unsigned long long* bar) {
@@ -1858,6 +1883,22 @@ int launch_move_tiers(nido_graph_s* g, int batch, int tie) {
   if (batch < 0 || batch >= g->nbatches)
     return nido_set_error(NIDO_E_INVALID, "louvain_update: batch %d out of range [0,%d)", batch, g->nbatches);
   return tiers_direct(g, batch, tie, move_args(g, tie));
+}
+
+int check_bounded_wait(nido_ctx_s* ctx, int32_t* gave_up, int32_t* waited_ms) {
+  int32_t* d = nullptr;
+  NIDO_CUDA_TRY(cudaMalloc((void**)&d, 2 * sizeof(int32_t)));
+  int32_t h[2] = {0, 0};
+  k_check_bounded_wait<<<1, 32, 0, ctx->stream>>>(d);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(h, d, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  cudaFree(d);
+  if (e != cudaSuccess) return nido_set_error(NIDO_E_CUDA, "bounded-wait check: %s", cudaGetErrorString(e));
+  nido_count_launches(1);
+  if (gave_up) *gave_up = h[0];
+  if (waited_ms) *waited_ms = h[1];
+  return NIDO_OK;
 }
 
 int launch_move(nido_graph_s* g, int batch, int tie, cudaEvent_t ev_start, cudaEvent_t ev_end) {
