@@ -53,6 +53,7 @@ struct MoveArgs {
   // FP64 one is several times slower) and every partial sum is exact, so
   // the e_vc read back are the FP64 sums bit for bit
   int ints;
+  int64_t nv;  // vertices of the current graph (all graphs in many-graph mode)
 };
 
 // The mass of v's graph (kernels are instantiated per mode, so the
@@ -177,8 +178,17 @@ __global__ void __launch_bounds__(256, 6) k_move_group(const int32_t* __restrict
       c = p.comm[u];
       wt = (u == v) ? 0. : p.w[s + gl];
     }
-    const unsigned long long mkey = ((unsigned long long)(unsigned)gid << 32) | (unsigned)c;
-    const unsigned peers = __match_any_sync(NIDO_FULL_MASK, mkey);
+    // lanes of one vertex with equal communities: a 32-bit match where the
+    // group index fits above the ids (invalid lanes, c = -1, may match across
+    // groups; they add nothing), else a 64-bit one
+    unsigned peers;
+    if constexpr (G == 32) {
+      peers = __match_any_sync(NIDO_FULL_MASK, (unsigned)c);
+    } else if (p.nv <= (int64_t)1 << 29) {
+      peers = __match_any_sync(NIDO_FULL_MASK, (unsigned)c | ((unsigned)gid << 29));
+    } else {
+      peers = __match_any_sync(NIDO_FULL_MASK, ((unsigned long long)(unsigned)gid << 32) | (unsigned)c);
+    }
     const int leader = __ffs(peers) - 1;
     const bool lead = ok && lane == leader;
     double e;
@@ -1867,7 +1877,7 @@ int move_init_attributes() {
 namespace {
 MoveArgs move_args(nido_graph_s* g, int tie) {
   return MoveArgs{g->off, g->adj, g->w, g->comm, g->k, g->a, g->newc, g->m, tie,
-                  reinterpret_cast<unsigned long long*>(g->dcount + 1), g->gid, g->mg, g->int_weights ? 1 : 0};
+                  reinterpret_cast<unsigned long long*>(g->dcount + 1), g->gid, g->mg, g->int_weights ? 1 : 0, g->nv};
 }
 
 int tiers_direct(nido_graph_s* g, int batch, int tie, const MoveArgs& p) {
