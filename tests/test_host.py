@@ -126,6 +126,16 @@ def test_cli_options():
     assert r.returncode != 0
 
 
+def test_package_cli_options():
+    """python -m nido_b200: one of --file / --workload / --many is required, and
+    the batched many-graph run is offered."""
+    import sys
+    r = subprocess.run([sys.executable, "-m", "nido_b200", "--help"], capture_output=True, text=True, cwd=ROOT)
+    assert r.returncode == 0 and "--many" in r.stdout and "--many-edges" in r.stdout
+    r = subprocess.run([sys.executable, "-m", "nido_b200"], capture_output=True, text=True, cwd=ROOT)
+    assert r.returncode != 0 and "one of the arguments" in r.stderr
+
+
 def _free_port():
     s = socket.socket()
     s.bind(("127.0.0.1", 0))
